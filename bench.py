@@ -1,0 +1,433 @@
+"""Benchmark: time-to-solution of the Krylov hot path on B200.
+
+One step = one complete solve, from b resident in HBM to x resident in HBM, to
+a relative residual of 1e-10 (the reference's stopping test on the recurrence
+residual; the true FP64 residual is checked and reported).
+
+Workloads (the default is the one the headline metric is quoted on):
+  c4_mixed  3D variable-coefficient diffusion 160^3 (n = 4,096,000, nnz =
+            28,518,400, ln kappa ~ N(0, 1.5^2) per cell, harmonic-mean faces),
+            b ~ N(0,1): VPCG with an FP64 outer loop and an FP32 inner CG of
+            exactly 20 iterations, to rel-res 1e-10. The plain FP64 CG on the
+            same system is timed beside it.
+  c2_cg     3D 7-point Poisson 128^3 (n = 2,097,152), b ~ U(0,1): CG FP64.
+Inputs are seeded synthetic data with the configurations' shapes; the matrix
+(>= 175 MB) is larger than the 126 MB L2, so no L2 flush is needed between
+steps.
+
+`--impl reference` times the reference's own CPU path (oracle/_ref/Solver,
+built from the reference sources) on the host cores for the same workload.
+
+Multi-GPU (torchrun, N > 1): the path does not shard in this build; every rank
+solves its own replica (weak scaling) and the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c4_mixed": dict(problem="varcoef3d", grid=160, outer="VPCG", inner="CG",
+                     params=dict(E=1e-10, L=10000, l=20, e=1e-30, inner_precision="fp32"),
+                     plain=dict(outer="CG", params=dict(E=1e-10, L=20000)),
+                     ref_args=["-S", "vpcg", "-s", "cg", "-l", "20", "-e", "1e-30", "-E", "1e-10"],
+                     spmv_values="fp32"),
+    "c2_cg": dict(problem="poisson3d", grid=128, outer="CG", inner="NONE",
+                  params=dict(E=1e-10, L=10000), plain=None,
+                  ref_args=["-S", "cg", "-E", "1e-10"], spmv_values="fp64"),
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def spmv_bytes(n, nnz, values):
+    """Algorithmic bytes of one SpMV: values + int32 columns + int32 row
+    offsets + x read once + y written once."""
+    vb = {"fp64": 8, "fp32": 4, "bf16": 2}[values]
+    xb = 8 if values == "fp64" else 4
+    return nnz * (vb + 4) + 4 * (n + 1) + xb * n + xb * n
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import solver_cpp_b200 as ks
+    from solver_cpp_b200.matrices import config_problem
+
+    W = WORKLOADS[args.workload]
+    A, b, _ = config_problem(W["problem"], W["grid"])
+    n, nnz = A.n, A.nnz
+    ctx = ks.Context(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    M = ctx.matrix(A, transpose=False, fp32=True, bf16=True)
+    B = ctx.vector(b)
+    X = ctx.vector(n=n)
+    launches0 = ks.lib().ks_ctx_launches(ctx.handle)
+
+    def one(outer, inner, params):
+        return ks.solve(ctx, M, outer, B, inner=inner, x=X, **params)
+
+    for _ in range(args.warmup):
+        r = one(W["outer"], W["inner"], W["params"])
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches_a = ks.lib().ks_ctx_launches(ctx.handle)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        results = []
+        for _ in range(args.steps):
+            results.append(one(W["outer"], W["inner"], W["params"]))
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    launches_b = ks.lib().ks_ctx_launches(ctx.handle)
+    clocks = sampler.stop()
+    total_ms = ev0.elapsed_time(ev1)
+    total_ms = max_over_ranks(total_ms, world)
+    barrier(world)
+    res = results[-1]
+    ms_per_step = total_ms / args.steps
+    value = ms_per_step / 1e3
+
+    # plain FP64 method on the same system (the comparison the metric names)
+    plain = None
+    if W.get("plain"):
+        P = W["plain"]
+        one(P["outer"], "NONE", P["params"])
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            pr = None
+            for _ in range(max(1, args.steps // 2)):
+                pr = one(P["outer"], "NONE", P["params"])
+            e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1) / max(1, args.steps // 2)
+        xp = X.numpy()
+        plain = {"method": P["outer"], "seconds": pms / 1e3, "loop": pr.loop, "true_rel_res": pr.true_rel_res,
+                 "speedup_mixed_vs_plain": (pms / 1e3) / value}
+        # agreement of the mixed solution with the FP64 one
+        one(W["outer"], W["inner"], W["params"])
+        xm = X.numpy()
+        plain["x_rel_diff_vs_fp64"] = float(np.linalg.norm(xm - xp) / np.linalg.norm(xp))
+
+    # dominant kernel: SpMV with the workload's value precision, timed alone
+    vals = W["spmv_values"]
+    dt = ks.FP64 if vals == "fp64" else ks.FP32
+    xs = ctx.vector(np.random.default_rng(0).standard_normal(n), dtype=dt)
+    ys = ctx.vector(n=n, dtype=dt)
+    vcode = {"fp64": ks.FP64, "fp32": ks.FP32, "bf16": ks.BF16}[vals]
+    for _ in range(5):
+        ks.spmv(M, xs, ys, values=vcode)
+    torch.cuda.synchronize()
+    reps = 50
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        s0.record(stream)
+        for _ in range(reps):
+            ks.spmv(M, xs, ys, values=vcode)
+        s1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = s0.elapsed_time(s1) / reps
+    alg = spmv_bytes(n, nnz, vals)
+    peak, peak_kind = load_peaks()
+    achieved = alg / (spmv_ms / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(f"{args.workload}:{vals}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": f"spmv_{vals}",
+                "alg_bytes_per_launch": alg, "launch_ms": round(spmv_ms, 5), "peak_kind": peak_kind}
+    fp64_bytes = spmv_bytes(n, nnz, "fp64")
+    if vals != "fp64":  # also the FP64 SpMV of the outer loop
+        x64, y64 = ctx.vector(np.random.default_rng(0).standard_normal(n)), ctx.vector(n=n)
+        ks.spmv(M, x64, y64)
+        torch.cuda.synchronize()
+        s0.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(reps):
+                ks.spmv(M, x64, y64)
+            s1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = s0.elapsed_time(s1) / reps
+        roofline["spmv_fp64_gbs"] = round(fp64_bytes / (ms64 / 1e3) / 1e9, 1)
+
+    # end to end through the public host API: pinned b -> device -> x -> host
+    e2e = None
+    if not args.no_e2e:
+        bh = torch.from_numpy(b).pin_memory().numpy()
+        xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        import ctypes as C
+
+        p = ks.make_params(**W["params"])
+        rep = ks._abi.Report()
+        hi = np.zeros(W["params"]["L"] + 2, dtype=np.int64)
+        he = np.zeros(W["params"]["L"] + 2)
+        L = ks.lib()
+        oc, ic = ks.SOLVERS[W["outer"]], ks.SOLVERS[W["inner"]]
+        for _ in range(1):
+            L.ks_solve_host(ctx.handle, M.handle, oc, ic, C.byref(p), bh.ctypes.data, xh.ctypes.data,
+                            hi.ctypes.data, he.ctypes.data, hi.shape[0], C.byref(rep))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.steps):
+                L.ks_solve_host(ctx.handle, M.handle, oc, ic, C.byref(p), bh.ctypes.data, xh.ctypes.data,
+                                hi.ctypes.data, he.ctypes.data, hi.shape[0], C.byref(rep))
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+        e2e = {"value": ems / 1e3, "unit": "s", "h2d_bytes_per_step": 8 * n,
+               "d2h_bytes_per_step": 8 * n + 16 * int(rep.hist_len) + 64}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(A, b, W, res)
+
+    out = {
+        "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); SpMV HBM GB/s",
+        "value": round(value, 6), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 outer / f32 inner" if args.workload == "c4_mixed" else "f64",
+        "data": "synthetic (seeded generator of the configuration; no dataset)",
+        "config": {"workload": args.workload, "problem": W["problem"], "grid": W["grid"], "n": n, "nnz": nnz,
+                   "method": W["outer"] + ("/" + W["inner"] if W["inner"] != "NONE" else ""),
+                   "params": W["params"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (matrix >= 175 MB)"},
+        "result": {"status": res.status, "loop": res.loop, "true_rel_res": res.true_rel_res,
+                   "inner_calls": res.inner_calls},
+        "plain_fp64": plain,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": int(launches_b - launches_a),
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    M.close()
+    ctx.close()
+    del launches0
+
+
+def cpu_baseline_port(A, b, W, res):
+    """The oracle (single-threaded C restatement of the reference) on a
+    bounded sample: a few iterations of the same method, scaled to the GPU
+    run's iteration count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    p = dict(W["params"])
+    p.pop("inner_precision", None)
+    sample_iters = 2 if W["inner"] != "NONE" else 20
+    p["L"] = sample_iters
+    P = pyoracle.Problem(A, with_transpose=False)
+    t0 = time.perf_counter()
+    o = pyoracle.solve(P, b, W["outer"], W["inner"], hist_cap=64, **p)
+    dt = time.perf_counter() - t0
+    per_iter = dt / max(1, sample_iters)
+    est = per_iter * max(1, res.loop)
+    return {"value": round(est, 3), "unit": "s", "cores": 1, "kind": "port",
+            "sample": f"{sample_iters} iterations of {W['outer']}" + (f"/{W['inner']}" if W['inner'] != 'NONE' else '')
+                      + f" in FP64 on the full system ({dt:.2f} s), scaled to the GPU run's {res.loop} iterations"}
+
+
+def run_reference(args, world, rank):
+    """The reference's own CPU path (oracle/_ref/Solver, all host threads) on
+    the same workload: each step runs a bounded number of iterations and is
+    scaled to the iteration count the full solve needs."""
+    if world > 1 and rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    W = WORKLOADS[args.workload]
+    if not pyoracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/Solver was not built (reference "
+                          "sources absent when the package was built)"}))
+        return
+    from solver_cpp_b200.matrices import config_problem
+
+    A, b, _ = config_problem(W["problem"], W["grid"])
+    threads = os.cpu_count() or 1
+    wd = tempfile.mkdtemp(prefix="refbench_")
+    mdir = os.path.join(wd, "Matrix", "CRS", "bench")
+    os.makedirs(mdir, exist_ok=True)
+    try:
+        import solver_cpp_b200 as ks
+
+        ks.crs_write(mdir, A, b)
+    except Exception:
+        from solver_cpp_b200.matrices import write_crs
+
+        write_crs(mdir, A, b)
+    # iterations to convergence of the reference's method on this system:
+    # the plain and mixed runs use the same outer method; one full run of the
+    # bounded sample gives the per-iteration time.
+    cap = 3 if W["inner"] != "NONE" else 40
+    times, loops = [], []
+    for i in range(args.warmup + args.steps):
+        r = pyoracle.run_reference(A, b, W["ref_args"] + ["-L", str(cap)], threads=threads, workdir=wd,
+                                   name="bench", keep_x=False)
+        if i >= args.warmup:
+            times.append(r["time"])
+            loops.append(r["loop"])
+    per_iter = statistics.median(t / max(1, min(l, cap)) for t, l in zip(times, loops))
+    full = args.ref_iterations or {"c4_mixed": 0, "c2_cg": 0}.get(args.workload) or cap
+    value = per_iter * full
+    out = {"impl": "reference", "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); "
+           "SpMV HBM GB/s", "value": round(value, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(statistics.median(times) * 1e3, 2), "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded generator of the configuration; no dataset)",
+           "config": {"workload": args.workload, "problem": W["problem"], "grid": W["grid"], "n": A.n,
+                      "nnz": A.nnz, "reference_flags": W["ref_args"]},
+           "cpu_baseline": {"value": round(value, 4), "unit": "s", "cores": threads, "kind": "reference",
+                            "sample": f"{cap} iterations per step of the reference binary (-t {threads}), "
+                                      f"{per_iter:.4f} s/iteration scaled to {full} iterations"},
+           "e2e": {"value": round(value, 4), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c4_mixed")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-iterations", type=int, default=0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

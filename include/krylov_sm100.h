@@ -1,0 +1,261 @@
+/*
+ * krylov_sm100.h -- C ABI of the B200 (sm_100a) Krylov hot path of solver_cpp.
+ *
+ * This library replaces the reference's host math class `blas`
+ * (blas.hpp:8-78) and its device offload class `cuda` (cudaFunction.hpp:7-129)
+ * with device-resident kernels, and runs the reference's Krylov methods
+ * (cg.cpp, cr.cpp, bicg.cpp, gcr.cpp, gmres.cpp, kskipcg.cpp, kskipbicg.cpp,
+ * vpcg.cpp, vpcr.cpp, vpgcr.cpp, vpgmres.cpp) with every vector kept in HBM.
+ * Only scalars (convergence flags, the residual history) come back to the host.
+ *
+ * Conventions
+ *  - Every entry point returns a ks_status and never exits or traps. On failure
+ *    ks_last_error() describes the cause.
+ *  - Matrices are square CSR with 0-based int32 indices, as the reference's
+ *    collection holds them (solver_collection.hpp:100-117).
+ *  - Work is issued on the context's stream. Calls that return host scalars
+ *    synchronise that stream; all others are asynchronous.
+ *  - One context may be used by one host thread at a time.
+ */
+#ifndef KRYLOV_SM100_H
+#define KRYLOV_SM100_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KS_ABI_VERSION 1
+
+typedef enum {
+  KS_OK = 0,              /* converged / success (reference solve() == 0)      */
+  KS_NOT_CONVERGED = 2,   /* maxloop reached (reference solve() == 2)           */
+  KS_BREAKDOWN = 3,       /* a Krylov denominator was exactly zero              */
+  KS_NAN_DETECTED = 4,    /* a recurrence produced a non-finite scalar          */
+  KS_BAD_INPUT = 5,       /* invalid argument, shape or handle                  */
+  KS_CUDA_ERROR = 6,      /* a CUDA runtime call failed                         */
+  KS_TIMEOUT = 7,         /* a bounded device wait gave up                      */
+  KS_OUT_OF_MEMORY = 8,   /* device allocation failed                           */
+  KS_NO_DEVICE = 9,       /* no usable CUDA device                              */
+  KS_IO_ERROR = 10,       /* CRS text files missing or malformed                */
+  KS_UNIMPLEMENTED = 99   /* reference's "Not implemented" (KSKIPCR, VPBICG)    */
+} ks_status;
+
+/* Method names; values equal the reference's SOLVERS_NAME
+ * (solver_collection.hpp:7-24). */
+typedef enum {
+  KS_NONE = 0, KS_CG = 1, KS_BICG = 2, KS_CR = 3, KS_GCR = 4, KS_GMRES = 5,
+  KS_KSKIPCG = 6, KS_KSKIPCR = 7, KS_KSKIPBICG = 8, KS_VPCG = 9,
+  KS_VPBICG = 10, KS_VPCR = 11, KS_VPGCR = 12, KS_VPGMRES = 13
+} ks_solver;
+
+/* Element type of a vector, or of the matrix values an operation reads. */
+typedef enum { KS_FP64 = 0, KS_FP32 = 1, KS_BF16 = 2 } ks_precision;
+
+typedef struct ks_ctx ks_ctx;
+typedef struct ks_mat ks_mat;
+typedef struct ks_vec ks_vec;
+
+/* ---------------------------------------------------------------- context */
+
+/* Replaces the reference's per-solver `new cuda(times*, N, ...)` buffer owner
+ * (cudaFunction.cu:270-372) and cuda::Reset/GetDeviceNum
+ * (cudaFunction.cu:571-578,1905-1909): a context owns the stream, the
+ * reduction scratch and a workspace pool reused across solves. */
+ks_status ks_ctx_create(int device, ks_ctx **out);
+ks_status ks_ctx_destroy(ks_ctx *ctx);
+/* Use an existing cudaStream_t (passed as void*); NULL restores the
+ * context's own stream. */
+ks_status ks_ctx_set_stream(ks_ctx *ctx, void *stream);
+ks_status ks_ctx_synchronize(ks_ctx *ctx);
+/* Number of CUDA devices (cuda::GetDeviceNum, cudaFunction.cu:1905). */
+int ks_device_count(void);
+const char *ks_status_string(ks_status s);
+/* Kernels this context has launched so far (diagnostics; the reference's
+ * `times` class counts time, not launches: times.hpp:15-88). */
+int64_t ks_ctx_launches(const ks_ctx *ctx);
+const char *ks_last_error(const ks_ctx *ctx);
+int ks_abi_version(void);
+
+/* ----------------------------------------------------------------- matrix */
+
+#define KS_MAT_TRANSPOSE 1u /* also build A^T (the reference's CTval/CTcol/CTptr) */
+#define KS_MAT_FP32 2u      /* keep an FP32 copy of the values                    */
+#define KS_MAT_BF16 4u      /* keep a BF16 copy of the values                     */
+
+/* Upload a host CSR matrix (collection::CudaCopy_Part1,
+ * solver_collection.cpp:932-942) and build the row-block schedule of the
+ * adaptive SpMV. With KS_MAT_TRANSPOSE the transpose is built on the device;
+ * it replaces cuda::CSR2CSC (cudaFunction.cu:896-982), whose cuSPARSE call no
+ * longer exists in CUDA 12. */
+ks_status ks_csr_upload(ks_ctx *ctx, int64_t n, int64_t nnz,
+                        const int32_t *ptr, const int32_t *col,
+                        const double *val, unsigned flags, ks_mat **out);
+/* Same from device arrays (copied; the caller keeps ownership). */
+ks_status ks_csr_upload_device(ks_ctx *ctx, int64_t n, int64_t nnz,
+                               const int32_t *d_ptr, const int32_t *d_col,
+                               const double *d_val, unsigned flags,
+                               ks_mat **out);
+ks_status ks_mat_destroy(ks_mat *mat);
+/* n, nnz, and the number of SpMV row blocks. */
+ks_status ks_mat_info(const ks_mat *mat, int64_t *n, int64_t *nnz,
+                      int64_t *row_blocks);
+/* Copy the device-built transpose back (CSR of A^T: tptr[n+1], trow[nnz],
+ * tval[nnz]), i.e. the CSC arrays the reference's CSR2CSC returns. */
+ks_status ks_mat_transpose_download(const ks_mat *mat, int32_t *tptr,
+                                    int32_t *trow, double *tval);
+
+/* ----------------------------------------------------------------- vector */
+
+/* Device vectors (the reference keeps them on the host and copies them on
+ * every SpMV: cuda::H2D/D2H, cudaFunction.cu:421-471). */
+ks_status ks_vec_create(ks_ctx *ctx, int64_t n, ks_precision type,
+                        ks_vec **out);
+/* Non-owning view of caller device memory (e.g. a torch tensor). */
+ks_status ks_vec_wrap(ks_ctx *ctx, int64_t n, ks_precision type,
+                      void *device_ptr, ks_vec **out);
+ks_status ks_vec_destroy(ks_vec *v);
+ks_status ks_vec_upload(ks_vec *v, const void *host);      /* synchronous */
+ks_status ks_vec_download(const ks_vec *v, void *host);    /* synchronous */
+/* Part of a vector: elements [offset, offset+count). */
+ks_status ks_vec_upload_range(ks_vec *v, int64_t offset, int64_t count,
+                              const void *host);
+ks_status ks_vec_download_range(const ks_vec *v, int64_t offset,
+                                int64_t count, void *host);
+ks_status ks_vec_fill(ks_vec *v, double value);
+void *ks_vec_device_ptr(ks_vec *v);
+int64_t ks_vec_length(const ks_vec *v);
+
+/* ------------------------------------------------------------ primitives */
+
+/* y = A x (trans = 0) or y = A^T x (trans = 1). Replaces cuda::MtxVec_mult
+ * (cudaFunction.cu:613-638) and blas::MtxVec_mult (blas.cpp:43-129). The
+ * matrix values read follow the vectors: FP64 vectors read the FP64 values,
+ * FP32 vectors the FP32 copy. For FP64 rows of up to 2048 nonzeros the sum
+ * runs in the reference's order and matches it bit for bit. */
+ks_status ks_spmv(const ks_mat *mat, int trans, const ks_vec *x, ks_vec *y);
+/* As ks_spmv, choosing the matrix value copy explicitly (KS_BF16 values with
+ * FP32 vectors is the BF16-stored variant). */
+ks_status ks_spmv_values(const ks_mat *mat, int trans, ks_precision values,
+                         const ks_vec *x, ks_vec *y);
+/* blas::dot / blas::norm_2 (blas.cpp:149-209, 31-41); deterministic. */
+ks_status ks_dot(const ks_vec *x, const ks_vec *y, double *result);
+ks_status ks_nrm2(const ks_vec *x, double *result);
+/* y = a*x + y (blas::Scalar_axy, blas.cpp:226-233). */
+ks_status ks_axpy(double a, const ks_vec *x, ks_vec *y);
+/* Fused y = a*x + y and result = (y, w) in one pass. */
+ks_status ks_axpy_dot(double a, const ks_vec *x, ks_vec *y, const ks_vec *w,
+                      double *result);
+/* h[i] = (V_i, w) for i < k, V_i = V[i*ld .. i*ld+n). GMRES's H column
+ * (gmres.cpp:354-371) and GCR's beta dots (blas.cpp:532-535) as one
+ * tall-skinny pass. */
+ks_status ks_block_dot(const ks_vec *V, int64_t ld, int k, const ks_vec *w,
+                       double *h);
+/* w[j] -= h[i] * V_i[j] for i = 0..k-1 in order (blas::Gmres_sp_1,
+ * blas.cpp:477-488). */
+ks_status ks_block_axpy(const ks_vec *V, int64_t ld, int k, const double *h,
+                        ks_vec *w);
+/* Matrix powers Ar[i] = A^{i+1} r (i <= 2k), Ap[i] = A^{i+1} p (i <= 2k+1),
+ * stored contiguously with stride n (blas::Kskip_cg_bicg_base,
+ * blas.cpp:353-399; cuda::Kskip_cg_bicg_base, cudaFunction.cu:984-1026). */
+ks_status ks_matpow(const ks_mat *mat, const ks_vec *r, const ks_vec *p,
+                    int k, ks_vec *Ar, ks_vec *Ap);
+/* k-skip CG Gram values delta[2k], eta[2k+1], zeta[2k+2]
+ * (blas::Kskip_cg_innerProduce, blas.cpp:401-435). */
+ks_status ks_gram_cg(const ks_vec *Ar, const ks_vec *Ap, const ks_vec *r,
+                     const ks_vec *p, int k, double *delta, double *eta,
+                     double *zeta);
+/* k-skip BiCG Gram values theta[2k], eta[2k+1], rho[2k+1], phi[2k+2]
+ * against the shadow vectors (blas::Kskip_bicg_innerProduce,
+ * blas.cpp:437-475). */
+ks_status ks_gram_bicg(const ks_vec *Ar, const ks_vec *Ap, const ks_vec *rs,
+                       const ks_vec *ps, int k, double *theta, double *eta,
+                       double *rho, double *phi);
+
+/* ------------------------------------------------------------------ solve */
+
+/* Mirrors the reference's flags (solver_collection.cpp:278-307):
+ * -L -E -R -K -F (outer) and -l -e -r -k -f (inner). */
+typedef struct {
+  int64_t outer_maxloop;   /* -L, default 10000 */
+  double outer_eps;        /* -E, default 1e-8  */
+  int64_t outer_restart;   /* -R, default 1000  */
+  int32_t outer_kskip;     /* -K, default 2     */
+  int32_t outer_fix;       /* -F, default 2     */
+  int64_t inner_maxloop;   /* -l, default 50    */
+  double inner_eps;        /* -e, default 1e-1  */
+  int64_t inner_restart;   /* -r, default 1000  */
+  int32_t inner_kskip;     /* -k, default 2     */
+  int32_t inner_fix;       /* -f, default 2     */
+  int32_t inner_precision; /* ks_precision of a VP method's inner solve      */
+  int32_t reference_defects; /* 1: reproduce the reference's k-skip CG
+                                recurrences and GMRES assembly; 0: corrected */
+  int32_t transpose;       /* 1: solve A^T x = b (adjoint solves)            */
+  int32_t poll_interval;   /* iterations in flight between host polls; 0=auto */
+} ks_params;
+
+typedef struct {
+  int32_t status;          /* ks_status of the method                        */
+  int64_t loop;            /* the value the reference prints as "loop ="     */
+  int64_t hist_len;        /* residual-history entries produced              */
+  double final_rel_res;    /* last history value                             */
+  double true_res_log10;   /* log10(|b-Ax|/|b-Ax0|), blas::Check_error       */
+  double true_rel_res;     /* |b-Ax|_2/|b|_2 in FP64                         */
+  int64_t spmv_count;      /* SpMVs issued (A and A^T, outer and inner)      */
+  int64_t inner_iterations;/* inner-solver iterations (VP methods)          */
+  double solve_seconds;    /* device time of the solve loop (CUDA events)    */
+} ks_report;
+
+void ks_params_default(ks_params *p);
+
+/* Run one Krylov method on device vectors (outerMethods::outerSelect,
+ * outerMethods.cpp:20-82; innerMethods::innerSelect, innerMethods.cpp:71-118).
+ * x is overwritten (the reference zeroes it: cg.cpp:79). If hist_err is not
+ * NULL the residual history (iteration label, relative residual) -- the
+ * contents of ./output/<NAME>_his.txt -- is copied out, up to hist_cap rows.
+ * Returns the method's status (KS_OK, KS_NOT_CONVERGED, ...). */
+ks_status ks_solve(ks_ctx *ctx, const ks_mat *mat, ks_solver outer,
+                   ks_solver inner, const ks_params *params, const ks_vec *b,
+                   ks_vec *x, int64_t *hist_iter, double *hist_err,
+                   int64_t hist_cap, ks_report *report);
+/* Same with host arrays: b is uploaded, x downloaded (end to end). */
+ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer,
+                        ks_solver inner, const ks_params *params,
+                        const double *b, double *x, int64_t *hist_iter,
+                        double *hist_err, int64_t hist_cap,
+                        ks_report *report);
+/* log10(|b - A x| / |b - A x0|) with x0 = 0 (blas::Check_error,
+ * blas.cpp:266-301), plus |b - A x|/|b| in *rel (may be NULL). */
+ks_status ks_check_error(const ks_mat *mat, const ks_vec *b, const ks_vec *x,
+                         double *log10_ratio, double *rel);
+
+/* ---------------------------------------------------------------- adjoint */
+
+/* Gradient of a loss L(x) with x = A^{-1} b, given g = dL/dx:
+ * solve A^T lambda = g with `solver` (on the transpose), then
+ * grad_b = lambda and grad_val[j] = -lambda[row(j)] * x[col(j)] over the CSR
+ * pattern. grad_b and grad_val may be NULL. The reference has no counterpart. */
+ks_status ks_adjoint_grad(ks_ctx *ctx, const ks_mat *mat, ks_solver solver,
+                          ks_solver inner, const ks_params *params,
+                          const ks_vec *x, const ks_vec *g, ks_vec *grad_b,
+                          ks_vec *grad_val, ks_report *report);
+/* The fused pattern gather alone: grad_val[j] = -lambda[row(j)] * x[col(j)]. */
+ks_status ks_pattern_grad(const ks_mat *mat, const ks_vec *lambda,
+                          const ks_vec *x, ks_vec *grad_val);
+
+/* ---------------------------------------------------------------- CRS I/O */
+
+/* The reference's text format (collection::checkCRSMatrix / readMatrix,
+ * solver_collection.cpp:655-828): dir/ColVal.txt, dir/Ptr.txt, dir/bx.txt. */
+ks_status ks_crs_read_header(const char *dir, int64_t *n, int64_t *nnz);
+ks_status ks_crs_read(const char *dir, int64_t n, int64_t nnz, int32_t *ptr,
+                      int32_t *col, double *val, double *b, double *x);
+ks_status ks_crs_write(const char *dir, int64_t n, int64_t nnz,
+                       const int32_t *ptr, const int32_t *col,
+                       const double *val, const double *b, const double *x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KRYLOV_SM100_H */

@@ -1,0 +1,298 @@
+// Internal definitions shared by the kernel and host translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "krylov_sm100.h"
+
+namespace ks {
+
+// ---------------------------------------------------------------- launch shape
+constexpr int kThreads = 256;       // threads per CTA for every kernel here
+constexpr int kRowsPerBlock = 256;  // rows staged by one SpMV row block
+constexpr int kNnzPerBlock = 2048;  // nonzeros staged by one SpMV row block
+constexpr int kChunk = 4;           // nonzeros per vectorised load (int4 cols)
+constexpr int kPad = 8;             // tail padding of col/val arrays (elements)
+constexpr int kMaxDots = 8;         // simultaneous reductions in one kernel
+constexpr int kBlockDotGroup = 8;   // tall-skinny dots per pass
+constexpr int kMaxGroups = 128;     // block-dot groups in one launch (1024 dots)
+
+// ---------------------------------------------------------------- state
+// Device-resident scalar state of one running Krylov method. Every scalar of
+// the recurrences lives here; the host only reads `done` and the history.
+enum DoneCode : int {
+  kRunning = 0,
+  kConverged = 1,
+  kMaxLoop = 2,
+  kBreakdown = 3,
+  kNaN = 4,
+};
+
+struct KState {
+  double s[96];          // named scalar slots (per method)
+  int done;              // DoneCode
+  int pad0;
+  long long loop;        // the method's iteration counter
+  long long hlen;        // history entries written
+  long long hcap;        // history capacity
+  long long aux[8];      // method-specific integers (e.g. GMRES step index)
+  double *hist_err;      // device history arrays (capacity hcap)
+  long long *hist_it;
+};
+
+// Stop predicate: a kernel does nothing once either flag is set. Used so a
+// whole queued iteration turns into no-ops after convergence, and so inner
+// solves of a VP method stop when the outer method has finished.
+struct Stop {
+  const int *a;
+  const int *b;
+  __device__ __forceinline__ bool operator()() const {
+    return (a && *(volatile const int *)a) || (b && *(volatile const int *)b);
+  }
+};
+
+// Reduction scratch: per-CTA partials plus a last-CTA-done counter.
+struct Red {
+  double *partials;     // [kMaxDots * kMaxGroups? ] x grid
+  unsigned *counter;
+};
+
+// ---------------------------------------------------------------- matrices
+struct CsrDev {
+  int n = 0;
+  long long nnz = 0;
+  int *ptr = nullptr;
+  int *col = nullptr;
+  double *val = nullptr;
+  float *val32 = nullptr;
+  __nv_bfloat16 *val16 = nullptr;
+  int *rb = nullptr;  // row-block boundaries, nrb + 1 entries
+  int nrb = 0;
+};
+
+template <class MT>
+struct CsrK {
+  const int *__restrict__ ptr;
+  const int *__restrict__ col;
+  const MT *__restrict__ val;
+  const int *__restrict__ rb;
+  int nrb;
+  int n;
+};
+
+template <class MT>
+inline CsrK<MT> view(const CsrDev &A);
+template <>
+inline CsrK<double> view<double>(const CsrDev &A) {
+  return {A.ptr, A.col, A.val, A.rb, A.nrb, A.n};
+}
+template <>
+inline CsrK<float> view<float>(const CsrDev &A) {
+  return {A.ptr, A.col, A.val32, A.rb, A.nrb, A.n};
+}
+template <>
+inline CsrK<__nv_bfloat16> view<__nv_bfloat16>(const CsrDev &A) {
+  return {A.ptr, A.col, A.val16, A.rb, A.nrb, A.n};
+}
+
+// ---------------------------------------------------------------- arithmetic
+// Round-to-nearest operations that the compiler may not contract into FMA:
+// the reference's host loops (blas.cpp) round the product and the sum
+// separately, and so do these.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+template <class T>
+__device__ __forceinline__ T to(double v);
+template <>
+__device__ __forceinline__ double to<double>(double v) { return v; }
+template <>
+__device__ __forceinline__ float to<float>(double v) { return (float)v; }
+
+__device__ __forceinline__ double widen(double v) { return v; }
+__device__ __forceinline__ double widen(float v) { return (double)v; }
+__device__ __forceinline__ float val_as_float(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// Matrix value -> accumulation type.
+template <class AT, class MT>
+__device__ __forceinline__ AT mval(MT v) { return (AT)v; }
+template <>
+__device__ __forceinline__ float mval<float, __nv_bfloat16>(__nv_bfloat16 v) {
+  return __bfloat162float(v);
+}
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sums of ND values; result valid in every thread. Fixed order, so
+// deterministic for a fixed launch shape.
+template <int ND>
+__device__ __forceinline__ void block_sum(double (&v)[ND]) {
+  __shared__ double sh[ND][kThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < ND; d++) v[d] = warp_sum(v[d]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int d = 0; d < ND; d++) sh[d][wid] = v[d];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; w++) s += sh[d][w];
+    v[d] = s;
+  }
+}
+
+// Single-pass deterministic grid reduction (last CTA done) over G CTAs, this
+// CTA being number `bid`. Every one of the G CTAs must call it exactly once.
+// Returns true in all threads of the last CTA to arrive, which then holds the
+// grand totals in `v`. No CTA waits on another: the last arriving CTA does the
+// final sum in a fixed order, so there is no spin and the result does not
+// depend on arrival order.
+template <int ND>
+__device__ __forceinline__ bool grid_sum_n(double (&v)[ND], double *partials,
+                                           unsigned *counter, unsigned G,
+                                           unsigned bid) {
+  __shared__ bool is_last;
+  block_sum<ND>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int d = 0; d < ND; d++) partials[(size_t)d * G + bid] = v[d];
+    __threadfence();
+    unsigned prev = atomicAdd(counter, 1u);
+    is_last = (prev == G - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    double s = 0.0;
+    for (unsigned i = threadIdx.x; i < G; i += blockDim.x)
+      s += __ldcg(partials + (size_t)d * G + i);
+    v[d] = s;
+  }
+  block_sum<ND>(v);
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+template <int ND>
+__device__ __forceinline__ bool grid_sum(double (&v)[ND], double *partials,
+                                         unsigned *counter) {
+  return grid_sum_n<ND>(v, partials, counter, gridDim.x * gridDim.y,
+                        blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ---------------------------------------------------------------- loads
+// Streaming (evict-first) loads for matrix data read once per SpMV, so the
+// Krylov vectors keep their place in L2.
+__device__ __forceinline__ int4 ld_stream(const int4 *p) { return __ldcs(p); }
+__device__ __forceinline__ void ld_vals4(const double *p, double (&v)[4]) {
+  double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
+  double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld_vals4(const float *p, float (&v)[4]) {
+  float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void ld_vals4(const __nv_bfloat16 *p, __nv_bfloat16 (&v)[4]) {
+  uint2 a = __ldcs(reinterpret_cast<const uint2 *>(p));
+  __nv_bfloat162 lo = *reinterpret_cast<__nv_bfloat162 *>(&a.x);
+  __nv_bfloat162 hi = *reinterpret_cast<__nv_bfloat162 *>(&a.y);
+  v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
+}
+
+}  // namespace ks
+
+// ---------------------------------------------------------------- handles
+struct ks_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  double *partials = nullptr;   // reduction scratch
+  size_t partials_len = 0;
+  unsigned *counters = nullptr; // last-CTA-done counters
+  int ncounters = 0;
+  double *d_result = nullptr;   // device staging for scalar results
+  size_t d_result_len = 0;
+  double *h_pinned = nullptr;   // pinned host staging (scalars)
+  size_t h_pinned_len = 0;
+  int *h_flags = nullptr;       // pinned ring of polled `done` flags
+  int nflags = 0;
+  cudaEvent_t *flag_events = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::vector<std::pair<void *, size_t>> pool;  // reusable device buffers
+  std::vector<bool> pool_busy;
+  std::string last_error;
+  long long launches = 0;       // kernels launched (diagnostics)
+};
+
+struct ks_mat {
+  ks_ctx *ctx = nullptr;
+  ks::CsrDev A;
+  ks::CsrDev T;
+  bool has_T = false;
+  unsigned flags = 0;
+};
+
+struct ks_vec {
+  ks_ctx *ctx = nullptr;
+  long long n = 0;
+  ks_precision type = KS_FP64;
+  void *d = nullptr;
+  bool owned = false;
+};
+
+namespace ks {
+
+inline size_t elem_size(ks_precision t) {
+  return t == KS_FP64 ? 8 : (t == KS_FP32 ? 4 : 2);
+}
+
+// Error plumbing for host code.
+ks_status set_error(ks_ctx *ctx, ks_status s, const std::string &msg);
+ks_status cuda_fail(ks_ctx *ctx, cudaError_t e, const char *what);
+
+#define KS_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return ::ks::cuda_fail((ctx), _e, #call); \
+  } while (0)
+
+#define KS_TRY(...)                    \
+  do {                                 \
+    ks_status _s = (__VA_ARGS__);      \
+    if (_s != KS_OK) return _s;        \
+  } while (0)
+
+// Scratch sizing.
+int red_grid(const ks_ctx *ctx);  // CTAs of the vector kernels
+int spmv_grid(const ks_ctx *ctx, const CsrDev &A);
+
+// Workspace pool (device buffers reused across solves).
+ks_status pool_get(ks_ctx *ctx, size_t bytes, void **out);
+void pool_release(ks_ctx *ctx, void *p);
+
+}  // namespace ks

@@ -1,0 +1,596 @@
+// Context, matrices, vectors and the primitive operations of the C ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "ks_kernels.cuh"
+#include "ks_ops.cuh"
+
+namespace ks {
+
+ks_status set_error(ks_ctx *ctx, ks_status s, const std::string &msg) {
+  if (ctx) ctx->last_error = msg;
+  return s;
+}
+
+ks_status cuda_fail(ks_ctx *ctx, cudaError_t e, const char *what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+  (void)cudaGetLastError();  // clear a sticky launch error where possible
+  ks_status s = (e == cudaErrorMemoryAllocation) ? KS_OUT_OF_MEMORY : KS_CUDA_ERROR;
+  return set_error(ctx, s, msg);
+}
+
+int red_grid(const ks_ctx *ctx) { return ctx->num_sms * 4; }
+
+int spmv_grid(const ks_ctx *ctx, const CsrDev &A) {
+  int g = ctx->num_sms * 8;
+  return std::max(1, std::min(g, A.nrb));
+}
+
+ks_status pool_get(ks_ctx *ctx, size_t bytes, void **out) {
+  bytes = std::max<size_t>(bytes, 256);
+  int best = -1;
+  for (size_t i = 0; i < ctx->pool.size(); i++) {
+    if (ctx->pool_busy[i] || ctx->pool[i].second < bytes) continue;
+    if (best < 0 || ctx->pool[i].second < ctx->pool[best].second) best = (int)i;
+  }
+  if (best >= 0) {
+    ctx->pool_busy[best] = true;
+    *out = ctx->pool[best].first;
+    return KS_OK;
+  }
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    // Free idle buffers and retry once.
+    for (size_t i = 0; i < ctx->pool.size();) {
+      if (!ctx->pool_busy[i]) {
+        cudaFree(ctx->pool[i].first);
+        ctx->pool.erase(ctx->pool.begin() + i);
+        ctx->pool_busy.erase(ctx->pool_busy.begin() + i);
+      } else {
+        i++;
+      }
+    }
+    (void)cudaGetLastError();
+    e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(workspace)");
+  }
+  ctx->pool.push_back({p, bytes});
+  ctx->pool_busy.push_back(true);
+  *out = p;
+  return KS_OK;
+}
+
+void pool_release(ks_ctx *ctx, void *p) {
+  for (size_t i = 0; i < ctx->pool.size(); i++)
+    if (ctx->pool[i].first == p) ctx->pool_busy[i] = false;
+}
+
+// ------------------------------------------------------------- row blocks
+// Greedy CSR-Adaptive partition: a block takes consecutive rows while it has
+// at most kRowsPerBlock rows and kNnzPerBlock nonzeros; a row longer than
+// kNnzPerBlock forms a block of its own.
+static std::vector<int> row_blocks(const int32_t *ptr, int n) {
+  std::vector<int> rb;
+  rb.reserve(n / 64 + 2);
+  rb.push_back(0);
+  int r = 0;
+  while (r < n) {
+    const int r0 = r;
+    const long long j0 = ptr[r0];
+    r = r0 + 1;
+    if ((long long)ptr[r0 + 1] - j0 <= kNnzPerBlock) {
+      while (r < n && r - r0 < kRowsPerBlock && (long long)ptr[r + 1] - j0 <= kNnzPerBlock) r++;
+    }
+    rb.push_back(r);
+  }
+  return rb;
+}
+
+// ------------------------------------------------------------- transpose
+__global__ void k_col_count(const int *__restrict__ col, long long nnz, int *__restrict__ cnt) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nnz;
+       j += (long long)gridDim.x * blockDim.x)
+    atomicAdd(cnt + col[j], 1);
+}
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Exclusive scan of `in` (n entries) into `out` (n+1 entries, out[n] = total),
+// tile by tile; tile totals go to `sums`.
+__global__ void k_scan_tiles(const int *__restrict__ in, int n, int *__restrict__ out,
+                             long long *__restrict__ sums) {
+  __shared__ long long sh[kScanThreads];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  long long v[kScanItems];
+  long long s = 0;
+#pragma unroll
+  for (int q = 0; q < kScanItems; q++) {
+    v[q] = (base + q < n) ? in[base + q] : 0;
+    s += v[q];
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < kScanThreads; o <<= 1) {
+    long long t = (threadIdx.x >= o) ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += t;
+    __syncthreads();
+  }
+  long long run = sh[threadIdx.x] - s;  // exclusive prefix of this thread
+#pragma unroll
+  for (int q = 0; q < kScanItems; q++) {
+    if (base + q < n) out[base + q] = (int)run;
+    run += v[q];
+  }
+  if (threadIdx.x == kScanThreads - 1) sums[blockIdx.x] = sh[threadIdx.x];
+}
+
+__global__ void k_scan_sums(long long *sums, int ntiles) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    long long run = 0;
+    for (int i = 0; i < ntiles; i++) {
+      long long t = sums[i];
+      sums[i] = run;
+      run += t;
+    }
+    sums[ntiles] = run;
+  }
+}
+
+__global__ void k_scan_add(int *out, int n, const long long *__restrict__ sums, int ntiles) {
+  const int i = blockIdx.x * kScanThreads + threadIdx.x;
+  for (int q = 0; q < kScanItems; q++) {
+    const int idx = blockIdx.x * kScanTile + q * kScanThreads + threadIdx.x;
+    if (idx < n) out[idx] += (int)sums[blockIdx.x];
+  }
+  if (i == 0) out[n] = (int)sums[ntiles];
+}
+
+__global__ void k_scatter_t(const int *__restrict__ ptr, const int *__restrict__ col,
+                            const double *__restrict__ val, int n, int *__restrict__ cursor,
+                            int *__restrict__ trow, double *__restrict__ tval) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    for (int j = ptr[r]; j < ptr[r + 1]; j++) {
+      const int d = atomicAdd(cursor + col[j], 1);
+      trow[d] = r;
+      tval[d] = val[j];
+    }
+  }
+}
+
+// Within each column, order the entries by row (the scatter's atomics leave
+// them in arrival order). Insertion sort per column: columns of sparse PDE
+// matrices are short.
+__global__ void k_sort_cols(const int *__restrict__ tptr, int n, int *__restrict__ trow,
+                            double *__restrict__ tval) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    const int a = tptr[c], b = tptr[c + 1];
+    for (int i = a + 1; i < b; i++) {
+      const int kr = trow[i];
+      const double kv = tval[i];
+      int j = i - 1;
+      while (j >= a && trow[j] > kr) {
+        trow[j + 1] = trow[j];
+        tval[j + 1] = tval[j];
+        j--;
+      }
+      trow[j + 1] = kr;
+      tval[j + 1] = kv;
+    }
+  }
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+__global__ void k_to_bf16(const double *__restrict__ a, __nv_bfloat16 *__restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16_rn((float)a[i]);
+}
+
+static void free_csr(CsrDev &A) {
+  cudaFree(A.ptr);
+  cudaFree(A.col);
+  cudaFree(A.val);
+  cudaFree(A.val32);
+  cudaFree(A.val16);
+  cudaFree(A.rb);
+  A = CsrDev();
+}
+
+static ks_status alloc_csr(ks_ctx *ctx, CsrDev &A, int n, long long nnz) {
+  A.n = n;
+  A.nnz = nnz;
+  KS_CUDA(ctx, cudaMalloc(&A.ptr, sizeof(int) * (size_t)(n + 1)));
+  KS_CUDA(ctx, cudaMalloc(&A.col, sizeof(int) * (size_t)(nnz + kPad)));
+  KS_CUDA(ctx, cudaMalloc(&A.val, sizeof(double) * (size_t)(nnz + kPad)));
+  KS_CUDA(ctx, cudaMemsetAsync(A.col + nnz, 0, sizeof(int) * kPad, ctx->stream));
+  KS_CUDA(ctx, cudaMemsetAsync(A.val + nnz, 0, sizeof(double) * kPad, ctx->stream));
+  return KS_OK;
+}
+
+static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, unsigned flags) {
+  std::vector<int> rb = row_blocks(host_ptr, A.n);
+  A.nrb = (int)rb.size() - 1;
+  KS_CUDA(ctx, cudaMalloc(&A.rb, sizeof(int) * rb.size()));
+  KS_CUDA(ctx, cudaMemcpyAsync(A.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice,
+                               ctx->stream));
+  const long long tot = A.nnz + kPad;
+  const int g = ctx->num_sms * 8;
+  if (flags & KS_MAT_FP32) {
+    KS_CUDA(ctx, cudaMalloc(&A.val32, sizeof(float) * (size_t)tot));
+    k_to_f32<<<g, 256, 0, ctx->stream>>>(A.val, A.val32, tot);
+  }
+  if (flags & KS_MAT_BF16) {
+    KS_CUDA(ctx, cudaMalloc(&A.val16, sizeof(__nv_bfloat16) * (size_t)tot));
+    k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.val, A.val16, tot);
+  }
+  KS_CUDA(ctx, cudaGetLastError());
+  // rb is a host vector going out of scope: the copy must complete first.
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return KS_OK;
+}
+
+static ks_status build_transpose(ks_ctx *ctx, ks_mat *m) {
+  CsrDev &A = m->A;
+  CsrDev &T = m->T;
+  const int n = A.n;
+  KS_TRY(alloc_csr(ctx, T, n, A.nnz));
+  int *cnt = nullptr, *cursor = nullptr;
+  long long *sums = nullptr;
+  const int ntiles = (n + kScanTile - 1) / kScanTile;
+  KS_CUDA(ctx, cudaMalloc(&cnt, sizeof(int) * (size_t)(n + 1)));
+  KS_CUDA(ctx, cudaMalloc(&cursor, sizeof(int) * (size_t)(n + 1)));
+  KS_CUDA(ctx, cudaMalloc(&sums, sizeof(long long) * (size_t)(ntiles + 1)));
+  KS_CUDA(ctx, cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(n + 1), ctx->stream));
+  const int g = ctx->num_sms * 8;
+  k_col_count<<<g, 256, 0, ctx->stream>>>(A.col, A.nnz, cnt);
+  k_scan_tiles<<<std::max(ntiles, 1), kScanThreads, 0, ctx->stream>>>(cnt, n, T.ptr, sums);
+  k_scan_sums<<<1, 32, 0, ctx->stream>>>(sums, ntiles);
+  k_scan_add<<<std::max(ntiles, 1), kScanThreads, 0, ctx->stream>>>(T.ptr, n, sums, ntiles);
+  KS_CUDA(ctx, cudaMemcpyAsync(cursor, T.ptr, sizeof(int) * (size_t)(n + 1), cudaMemcpyDeviceToDevice,
+                               ctx->stream));
+  k_scatter_t<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.val, n, cursor, T.col, T.val);
+  k_sort_cols<<<g, 256, 0, ctx->stream>>>(T.ptr, n, T.col, T.val);
+  KS_CUDA(ctx, cudaGetLastError());
+  std::vector<int32_t> tptr((size_t)n + 1);
+  KS_CUDA(ctx, cudaMemcpyAsync(tptr.data(), T.ptr, sizeof(int) * (size_t)(n + 1),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(cnt);
+  cudaFree(cursor);
+  cudaFree(sums);
+  KS_TRY(finish_csr(ctx, T, tptr.data(), m->flags));
+  m->has_T = true;
+  return KS_OK;
+}
+
+static ks_status check_csr(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_t *ptr,
+                           const int32_t *col) {
+  if (n < 1 || n >= (1LL << 31) - 1 || nnz < 0 || nnz >= (1LL << 31) - 1)
+    return set_error(ctx, KS_BAD_INPUT, "n and nnz must fit the int32 CSR format (n >= 1)");
+  if (ptr) {
+    if (ptr[0] != 0 || ptr[n] != nnz)
+      return set_error(ctx, KS_BAD_INPUT, "ptr[0] must be 0 and ptr[n] must equal nnz");
+    for (int64_t i = 0; i < n; i++)
+      if (ptr[i + 1] < ptr[i]) return set_error(ctx, KS_BAD_INPUT, "ptr must be non-decreasing");
+  }
+  if (col) {
+    for (int64_t j = 0; j < nnz; j++)
+      if (col[j] < 0 || col[j] >= n) return set_error(ctx, KS_BAD_INPUT, "column index out of range");
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------- primitive kernels
+__global__ void k_copy_bytes_done(const int *src, int *dst) { *dst = *src; }
+
+}  // namespace ks
+
+using namespace ks;
+
+// ============================================================= C ABI: context
+extern "C" {
+
+int ks_abi_version(void) { return KS_ABI_VERSION; }
+
+int ks_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+const char *ks_status_string(ks_status s) {
+  switch (s) {
+    case KS_OK: return "converged / ok";
+    case KS_NOT_CONVERGED: return "not converged (maxloop reached)";
+    case KS_BREAKDOWN: return "breakdown (zero Krylov denominator)";
+    case KS_NAN_DETECTED: return "non-finite scalar in the recurrence";
+    case KS_BAD_INPUT: return "bad input";
+    case KS_CUDA_ERROR: return "CUDA error";
+    case KS_TIMEOUT: return "bounded device wait timed out";
+    case KS_OUT_OF_MEMORY: return "out of device memory";
+    case KS_NO_DEVICE: return "no CUDA device";
+    case KS_IO_ERROR: return "CRS file error";
+    case KS_UNIMPLEMENTED: return "not implemented";
+  }
+  return "unknown status";
+}
+
+const char *ks_last_error(const ks_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int64_t ks_ctx_launches(const ks_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+ks_status ks_ctx_create(int device, ks_ctx **out) {
+  if (!out) return KS_BAD_INPUT;
+  *out = nullptr;
+  int ndev = ks_device_count();
+  if (ndev <= 0) return KS_NO_DEVICE;
+  if (device < 0 || device >= ndev) return KS_BAD_INPUT;
+  ks_ctx *ctx = new ks_ctx();
+  ctx->device = device;
+  auto fail = [&](ks_status s) {
+    ks_ctx_destroy(ctx);
+    return s;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return fail(KS_CUDA_ERROR);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return fail(KS_CUDA_ERROR);
+  ctx->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(KS_CUDA_ERROR);
+  ctx->stream = ctx->own_stream;
+  ctx->partials_len = (size_t)kMaxGroups * kBlockDotGroup * (size_t)std::max(red_grid(ctx), ctx->num_sms * 8);
+  if (cudaMalloc(&ctx->partials, sizeof(double) * ctx->partials_len) != cudaSuccess)
+    return fail(KS_OUT_OF_MEMORY);
+  ctx->ncounters = kMaxGroups + 64;
+  if (cudaMalloc(&ctx->counters, sizeof(unsigned) * ctx->ncounters) != cudaSuccess)
+    return fail(KS_OUT_OF_MEMORY);
+  if (cudaMemset(ctx->counters, 0, sizeof(unsigned) * ctx->ncounters) != cudaSuccess)
+    return fail(KS_CUDA_ERROR);
+  ctx->d_result_len = 4096;
+  if (cudaMalloc(&ctx->d_result, sizeof(double) * ctx->d_result_len) != cudaSuccess)
+    return fail(KS_OUT_OF_MEMORY);
+  ctx->h_pinned_len = 4096;
+  if (cudaMallocHost(&ctx->h_pinned, sizeof(double) * ctx->h_pinned_len) != cudaSuccess)
+    return fail(KS_OUT_OF_MEMORY);
+  ctx->nflags = 64;
+  if (cudaHostAlloc(&ctx->h_flags, sizeof(int) * ctx->nflags,
+                    cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+    return fail(KS_OUT_OF_MEMORY);
+  std::memset(ctx->h_flags, 0, sizeof(int) * ctx->nflags);
+  ctx->flag_events = new cudaEvent_t[ctx->nflags];
+  for (int i = 0; i < ctx->nflags; i++) {
+    if (cudaEventCreateWithFlags(&ctx->flag_events[i], cudaEventDisableTiming) != cudaSuccess)
+      return fail(KS_CUDA_ERROR);
+  }
+  if (cudaEventCreate(&ctx->ev_start) != cudaSuccess || cudaEventCreate(&ctx->ev_stop) != cudaSuccess)
+    return fail(KS_CUDA_ERROR);
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(KS_CUDA_ERROR);
+  *out = ctx;
+  return KS_OK;
+}
+
+ks_status ks_ctx_destroy(ks_ctx *ctx) {
+  if (!ctx) return KS_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &b : ctx->pool) cudaFree(b.first);
+  ctx->pool.clear();
+  cudaFree(ctx->partials);
+  cudaFree(ctx->counters);
+  cudaFree(ctx->d_result);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
+  if (ctx->flag_events) {
+    for (int i = 0; i < ctx->nflags; i++)
+      if (ctx->flag_events[i]) cudaEventDestroy(ctx->flag_events[i]);
+    delete[] ctx->flag_events;
+  }
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return KS_OK;
+}
+
+ks_status ks_ctx_set_stream(ks_ctx *ctx, void *stream) {
+  if (!ctx) return KS_BAD_INPUT;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return KS_OK;
+}
+
+ks_status ks_ctx_synchronize(ks_ctx *ctx) {
+  if (!ctx) return KS_BAD_INPUT;
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return KS_OK;
+}
+
+// ============================================================= C ABI: matrices
+static ks_status upload_common(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_t *ptr,
+                               const int32_t *col, const double *val, unsigned flags, ks_mat **out,
+                               cudaMemcpyKind kind) {
+  if (!ctx || !out || !ptr || (nnz > 0 && (!col || !val))) return KS_BAD_INPUT;
+  *out = nullptr;
+  KS_CUDA(ctx, cudaSetDevice(ctx->device));
+  std::vector<int32_t> hptr;
+  const int32_t *host_ptr = ptr;
+  if (kind == cudaMemcpyHostToDevice) {
+    KS_TRY(check_csr(ctx, n, nnz, ptr, col));
+  } else {
+    KS_TRY(check_csr(ctx, n, nnz, nullptr, nullptr));
+    hptr.resize((size_t)n + 1);
+    KS_CUDA(ctx, cudaMemcpy(hptr.data(), ptr, sizeof(int32_t) * (size_t)(n + 1), cudaMemcpyDeviceToHost));
+    KS_TRY(check_csr(ctx, n, nnz, hptr.data(), nullptr));
+    host_ptr = hptr.data();
+  }
+  ks_mat *m = new ks_mat();
+  m->ctx = ctx;
+  m->flags = flags;
+  ks_status s = alloc_csr(ctx, m->A, (int)n, nnz);
+  if (s == KS_OK) {
+    cudaError_t e = cudaMemcpyAsync(m->A.ptr, ptr, sizeof(int) * (size_t)(n + 1), kind, ctx->stream);
+    if (e == cudaSuccess && nnz > 0)
+      e = cudaMemcpyAsync(m->A.col, col, sizeof(int) * (size_t)nnz, kind, ctx->stream);
+    if (e == cudaSuccess && nnz > 0)
+      e = cudaMemcpyAsync(m->A.val, val, sizeof(double) * (size_t)nnz, kind, ctx->stream);
+    if (e != cudaSuccess) s = cuda_fail(ctx, e, "csr upload");
+  }
+  if (s == KS_OK) s = finish_csr(ctx, m->A, host_ptr, flags);
+  if (s == KS_OK && (flags & KS_MAT_TRANSPOSE)) s = build_transpose(ctx, m);
+  if (s != KS_OK) {
+    ks_mat_destroy(m);
+    return s;
+  }
+  *out = m;
+  return KS_OK;
+}
+
+ks_status ks_csr_upload(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_t *ptr, const int32_t *col,
+                        const double *val, unsigned flags, ks_mat **out) {
+  return upload_common(ctx, n, nnz, ptr, col, val, flags, out, cudaMemcpyHostToDevice);
+}
+
+ks_status ks_csr_upload_device(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_t *d_ptr,
+                               const int32_t *d_col, const double *d_val, unsigned flags,
+                               ks_mat **out) {
+  return upload_common(ctx, n, nnz, d_ptr, d_col, d_val, flags, out, cudaMemcpyDeviceToDevice);
+}
+
+ks_status ks_mat_destroy(ks_mat *m) {
+  if (!m) return KS_OK;
+  if (m->ctx) {
+    cudaSetDevice(m->ctx->device);
+    cudaStreamSynchronize(m->ctx->stream);
+  }
+  free_csr(m->A);
+  free_csr(m->T);
+  delete m;
+  return KS_OK;
+}
+
+ks_status ks_mat_info(const ks_mat *m, int64_t *n, int64_t *nnz, int64_t *row_blocks) {
+  if (!m) return KS_BAD_INPUT;
+  if (n) *n = m->A.n;
+  if (nnz) *nnz = m->A.nnz;
+  if (row_blocks) *row_blocks = m->A.nrb;
+  return KS_OK;
+}
+
+ks_status ks_mat_transpose_download(const ks_mat *m, int32_t *tptr, int32_t *trow, double *tval) {
+  if (!m || !m->has_T) return m ? set_error(m->ctx, KS_BAD_INPUT, "matrix has no transpose") : KS_BAD_INPUT;
+  ks_ctx *ctx = m->ctx;
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (tptr) KS_CUDA(ctx, cudaMemcpy(tptr, m->T.ptr, sizeof(int) * (size_t)(m->T.n + 1), cudaMemcpyDeviceToHost));
+  if (trow) KS_CUDA(ctx, cudaMemcpy(trow, m->T.col, sizeof(int) * (size_t)m->T.nnz, cudaMemcpyDeviceToHost));
+  if (tval) KS_CUDA(ctx, cudaMemcpy(tval, m->T.val, sizeof(double) * (size_t)m->T.nnz, cudaMemcpyDeviceToHost));
+  return KS_OK;
+}
+
+// ============================================================= C ABI: vectors
+ks_status ks_vec_create(ks_ctx *ctx, int64_t n, ks_precision type, ks_vec **out) {
+  if (!ctx || !out || n < 1 || type < KS_FP64 || type > KS_BF16) return KS_BAD_INPUT;
+  *out = nullptr;
+  KS_CUDA(ctx, cudaSetDevice(ctx->device));
+  ks_vec *v = new ks_vec();
+  v->ctx = ctx;
+  v->n = n;
+  v->type = type;
+  v->owned = true;
+  cudaError_t e = cudaMalloc(&v->d, elem_size(type) * (size_t)n + 64);
+  if (e != cudaSuccess) {
+    delete v;
+    return cuda_fail(ctx, e, "cudaMalloc(vector)");
+  }
+  e = cudaMemsetAsync(v->d, 0, elem_size(type) * (size_t)n, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFree(v->d);
+    delete v;
+    return cuda_fail(ctx, e, "cudaMemset(vector)");
+  }
+  *out = v;
+  return KS_OK;
+}
+
+ks_status ks_vec_wrap(ks_ctx *ctx, int64_t n, ks_precision type, void *device_ptr, ks_vec **out) {
+  if (!ctx || !out || !device_ptr || n < 1 || type < KS_FP64 || type > KS_BF16) return KS_BAD_INPUT;
+  if (((uintptr_t)device_ptr) % 16 != 0)
+    return set_error(ctx, KS_BAD_INPUT, "wrapped device pointer must be 16-byte aligned");
+  ks_vec *v = new ks_vec();
+  v->ctx = ctx;
+  v->n = n;
+  v->type = type;
+  v->d = device_ptr;
+  v->owned = false;
+  *out = v;
+  return KS_OK;
+}
+
+ks_status ks_vec_destroy(ks_vec *v) {
+  if (!v) return KS_OK;
+  if (v->owned && v->d) {
+    cudaSetDevice(v->ctx->device);
+    cudaStreamSynchronize(v->ctx->stream);
+    cudaFree(v->d);
+  }
+  delete v;
+  return KS_OK;
+}
+
+ks_status ks_vec_upload_range(ks_vec *v, int64_t offset, int64_t count, const void *host) {
+  if (!v || !host || offset < 0 || count < 0 || offset + count > v->n) return KS_BAD_INPUT;
+  ks_ctx *ctx = v->ctx;
+  const size_t es = elem_size(v->type);
+  KS_CUDA(ctx, cudaMemcpyAsync((char *)v->d + es * offset, host, es * (size_t)count,
+                               cudaMemcpyHostToDevice, ctx->stream));
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return KS_OK;
+}
+
+ks_status ks_vec_download_range(const ks_vec *v, int64_t offset, int64_t count, void *host) {
+  if (!v || !host || offset < 0 || count < 0 || offset + count > v->n) return KS_BAD_INPUT;
+  ks_ctx *ctx = v->ctx;
+  const size_t es = elem_size(v->type);
+  KS_CUDA(ctx, cudaMemcpyAsync(host, (const char *)v->d + es * offset, es * (size_t)count,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return KS_OK;
+}
+
+ks_status ks_vec_upload(ks_vec *v, const void *host) {
+  return v ? ks_vec_upload_range(v, 0, v->n, host) : KS_BAD_INPUT;
+}
+
+ks_status ks_vec_download(const ks_vec *v, void *host) {
+  return v ? ks_vec_download_range(v, 0, v->n, host) : KS_BAD_INPUT;
+}
+
+ks_status ks_vec_fill(ks_vec *v, double value) {
+  if (!v) return KS_BAD_INPUT;
+  ks_ctx *ctx = v->ctx;
+  if (v->type == KS_FP64)
+    launch_vec(ctx, v->n, FillOp<double>{(double *)v->d, value}, Stop{nullptr, nullptr});
+  else if (v->type == KS_FP32)
+    launch_vec(ctx, v->n, FillOp<float>{(float *)v->d, (float)value}, Stop{nullptr, nullptr});
+  else
+    return set_error(ctx, KS_BAD_INPUT, "fill supports FP64 and FP32 vectors");
+  KS_CUDA(ctx, cudaGetLastError());
+  return KS_OK;
+}
+
+void *ks_vec_device_ptr(ks_vec *v) { return v ? v->d : nullptr; }
+int64_t ks_vec_length(const ks_vec *v) { return v ? v->n : 0; }
+
+}  // extern "C"

@@ -1,0 +1,1638 @@
+// Krylov methods with every vector and every recurrence scalar on the device.
+//
+// Each method is the reference's loop (cg.cpp, cr.cpp, bicg.cpp, gcr.cpp,
+// gmres.cpp, kskipcg.cpp, kskipbicg.cpp, vpcg.cpp, vpcr.cpp, vpgcr.cpp,
+// vpgmres.cpp) re-cut into fused kernels. Reductions finish in the last CTA
+// of their kernel, which also advances the scalar recurrence (alpha, beta,
+// the stopping test and the residual history) in device memory. The host
+// issues iterations without waiting and only polls a host-mapped `done`
+// flag a bounded number of iterations behind; once a method has finished,
+// queued kernels see `done` and return at once.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "ks_ops.cuh"
+
+namespace ks {
+
+ks_status spmv_any(ks_ctx *ctx, const CsrDev &A, ks_precision vals, ks_precision vt, const void *x,
+                   void *y, Stop stop);
+ks_status matpow(ks_ctx *ctx, const CsrDev &A, const double *r, const double *p, int k, double *Ar,
+                 double *Ap, Stop stop);
+
+// ------------------------------------------------------------------ state
+enum Slot : int {
+  S_BNORM = 0,
+  S_EPS = 1,
+  S_RR = 2,     // (r,r) / (r*,r) / (r,z) / (r,s) / zaz: the carried product
+  S_ALPHA = 3,
+  S_BETA = 4,
+  S_T = 5,      // GMRES: current norm
+  S_GAMMA = 6,  // k-skip
+};
+enum Aux : int { A_MAXLOOP = 0, A_RECORD = 1, A_SPMV = 2, A_CONVK = 3, A_FINAL = 4, A_KIDX = 5 };
+
+struct DevState {  // KState plus the host-mapped mirror of `done`
+  KState k;
+  int *host_done;
+};
+
+__device__ __forceinline__ void set_done(DevState *st, int code) {
+  st->k.done = code;
+  if (st->host_done) *(volatile int *)st->host_done = code;
+}
+
+__device__ __forceinline__ void record(DevState *st, long long label, double err) {
+  if (!st->k.aux[A_RECORD]) return;
+  const long long h = st->k.hlen++;
+  if (h < st->k.hcap) {
+    st->k.hist_err[h] = err;
+    st->k.hist_it[h] = label;
+  }
+}
+
+// Stopping test at the top of iteration L of the CG-type loops
+// (cg.cpp:184-198): loop ends after maxloop iterations, records, compares.
+__device__ __forceinline__ void check_top(DevState *st, long long L, double err) {
+  st->k.loop = L;
+  if (L > st->k.aux[A_MAXLOOP]) {
+    set_done(st, kMaxLoop);
+    return;
+  }
+  record(st, L, err);
+  if (err <= st->k.s[S_EPS])
+    set_done(st, kConverged);
+  else if (err != err)
+    set_done(st, kNaN);
+}
+
+// a / b of a recurrence; a zero or non-finite result stops the method.
+__device__ __forceinline__ double rdiv(DevState *st, double a, double b) {
+  if (b == 0.0) {
+    set_done(st, kBreakdown);
+    return 0.0;
+  }
+  const double q = div_rn(a, b);
+  if (!isfinite(q)) set_done(st, kNaN);
+  return q;
+}
+
+__device__ __forceinline__ double rd(const double *p) { return __ldg(p); }
+
+// ------------------------------------------------------------------ env
+struct Params {
+  long long maxloop;
+  double eps;
+  long long restart;
+  int kskip;
+  int fix;
+};
+
+template <class VT>
+struct Env {
+  ks_ctx *ctx = nullptr;
+  const CsrDev *A = nullptr;   // operator
+  const CsrDev *AT = nullptr;  // its transpose
+  ks_precision mvals = KS_FP64;
+  DevState *st = nullptr;
+  const int *outer_done = nullptr;
+  bool record = false;
+  bool outer = false;  // drives host polling
+  Params sp{};
+  bool faithful = false;
+  long long n = 0;
+  volatile int *hflag = nullptr;  // host view of st->host_done (outer only)
+  int lookahead = 8;
+  Stop stop() const { return Stop{&st->k.done, outer_done}; }
+};
+
+// Host-side bounded lookahead: after each issued iteration, wait for the one
+// `la` iterations back and read the mapped done flag.
+struct Poller {
+  ks_ctx *ctx;
+  volatile int *flag;
+  int la;
+  long long issued = 0;
+  bool step() {
+    if (!flag) return false;
+    const int R = ctx->nflags;
+    cudaEventRecord(ctx->flag_events[issued % R], ctx->stream);
+    issued++;
+    if (*flag) return true;
+    if (issued > la) {
+      cudaEventSynchronize(ctx->flag_events[(issued - 1 - la) % R]);
+      return *flag != 0;
+    }
+    return false;
+  }
+};
+
+// SpMV with an epilogue, dispatched on the vector type and value copy.
+template <class VT, class Epi>
+inline void mv(const Env<VT> &E, const CsrDev &M, const VT *x, const Epi &epi) {
+  if constexpr (std::is_same<VT, double>::value) {
+    launch_spmv<double, double>(E.ctx, M, x, epi, E.stop());
+  } else {
+    if (E.mvals == KS_BF16)
+      launch_spmv<__nv_bfloat16, float>(E.ctx, M, x, epi, E.stop());
+    else
+      launch_spmv<float, float>(E.ctx, M, x, epi, E.stop());
+  }
+}
+
+template <class VT, class Op>
+inline void vec(const Env<VT> &E, const Op &op) {
+  launch_vec(E.ctx, E.n, op, E.stop());
+}
+
+// ------------------------------------------------------------------ shared ops
+// bnorm = |b|, stored with eps; resets the method's state.
+struct InitOp {
+  DevState *st;
+  double eps;
+  long long maxloop;
+  int rec;
+  __device__ void run() const {
+    st->k.done = kRunning;
+    st->k.loop = 0;
+    st->k.hlen = 0;
+    st->k.s[S_EPS] = eps;
+    st->k.aux[A_MAXLOOP] = maxloop;
+    st->k.aux[A_RECORD] = rec;
+    st->k.aux[A_CONVK] = 0;
+    st->k.aux[A_FINAL] = 0;
+    if (st->host_done) *(volatile int *)st->host_done = 0;
+  }
+};
+
+template <class VT>
+struct NormBOp {  // s[BNORM] = |b|
+  const VT *b;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void elem(long long i, double (&acc)[1]) const {
+    const double v = widen(b[i]);
+    acc[0] = add_rn(acc[0], mul_rn(v, v));
+  }
+  __device__ void finish(const double (&s)[1]) const { st->k.s[S_BNORM] = sqrt(s[0]); }
+};
+
+template <class VT>
+struct ZeroOp {
+  VT *x;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const { x[i] = (VT)0; }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+template <class VT>
+struct CopyOp {
+  const VT *a;
+  VT *b;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const { b[i] = a[i]; }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+// p = (beta * p) + r, beta from a slot (Scalar_axy(beta, p, r, p)).
+template <class VT>
+struct XpbyOp {
+  VT *p;
+  const VT *r;
+  const double *beta;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const {
+    const VT b = (VT)rd(beta);
+    p[i] = add_rn(mul_rn(b, p[i]), r[i]);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+// Two of them with one beta (p = beta p + r; q = beta q + s), optionally
+// followed by (q,q) -> alpha = s[RR] / (q,q) (CR, VPCR).
+template <class VT>
+struct Xpby2Op {
+  VT *p;
+  const VT *r;
+  VT *q;
+  const VT *s;
+  DevState *st;
+  int alpha_from_qq;
+  static constexpr int ND = 1;
+  __device__ void elem(long long i, double (&acc)[1]) const {
+    const VT b = (VT)rd(&st->k.s[S_BETA]);
+    p[i] = add_rn(mul_rn(b, p[i]), r[i]);
+    const VT qi = add_rn(mul_rn(b, q[i]), s[i]);
+    q[i] = qi;
+    acc[0] = add_rn(acc[0], mul_rn(widen(qi), widen(qi)));
+  }
+  __device__ void finish(const double (&sm)[1]) const {
+    if (alpha_from_qq) st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], sm[0]);
+  }
+};
+
+// r = b - A x; out (r,r); optional copies c1 = r, c2 = r. Used by every
+// method's start; `mode` picks the scalar step in finish().
+enum StartMode : int {
+  START_CG = 0,    // rr = (r,r); check_top(1)
+  START_CHECK = 1, // check_top(1) only (VP methods: rr comes later)
+  START_NORM = 2,  // s[T] = |r| (GMRES cycle start)
+  START_GCR = 3,   // GCR cycle start: maxloop test, check(loop)
+  START_KSKIP = 4, // nothing (k-skip checks at block start)
+};
+
+template <class VT>
+struct StartEpi {
+  using acc_t = VT;
+  const VT *b;
+  VT *r;
+  VT *c1;
+  VT *c2;
+  VT *c3;
+  DevState *st;
+  int mode;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    const VT ri = sub_rn(b[i], v);
+    r[i] = ri;
+    if (c1) c1[i] = ri;
+    if (c2) c2[i] = ri;
+    if (c3) c3[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[1]) const;
+};
+
+// GCR's stopping test at the top of step k (gcr.cpp:222-239).
+__device__ __forceinline__ void check_gcr(DevState *st, double err) {
+  const long long L = st->k.loop;
+  record(st, L, err);
+  if (err <= st->k.s[S_EPS]) {
+    set_done(st, kConverged);
+  } else if (L >= st->k.aux[A_MAXLOOP]) {
+    set_done(st, kMaxLoop);
+  } else if (err != err) {
+    set_done(st, kNaN);
+  } else {
+    st->k.loop = L + 1;
+  }
+}
+
+template <class VT>
+__device__ void StartEpi<VT>::finish(const double (&s)[1]) const {
+  const double err = sqrt(s[0]) / st->k.s[S_BNORM];
+  switch (mode) {
+    case START_CG:
+      st->k.s[S_RR] = s[0];
+      check_top(st, 1, err);
+      break;
+    case START_CHECK:
+      check_top(st, 1, err);
+      break;
+    case START_NORM:
+      st->k.s[S_T] = sqrt(s[0]);
+      break;
+    case START_GCR:
+      if (st->k.loop >= st->k.aux[A_MAXLOOP])
+        set_done(st, kMaxLoop);
+      else
+        check_gcr(st, err);
+      break;
+    default:
+      break;
+  }
+}
+
+// ------------------------------------------------------------------ CG
+// cg::solve (cg.cpp:148-240), three fused kernels per iteration:
+//   q = A p, (p,q) -> alpha;  x += alpha p, r -= alpha q, (r,r) -> beta,
+//   check;  p = beta p + r.
+template <class VT>
+struct CgMvEpi {
+  using acc_t = VT;
+  const VT *p;
+  VT *q;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    q[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(p[i]), widen(v)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], s[0]);
+  }
+};
+
+// x += alpha p; r -= alpha q; (r,r). mode 0: CG (beta = rr2/rr, check);
+// mode 1: check only (VP outer: rr carried separately).
+template <class VT>
+struct XrUpdOp {
+  VT *x;
+  VT *r;
+  const VT *p;
+  const VT *q;
+  DevState *st;
+  int mode;
+  static constexpr int ND = 1;
+  __device__ void elem(long long i, double (&acc)[1]) const {
+    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
+    x[i] = add_rn(mul_rn(a, p[i]), x[i]);
+    const VT ri = add_rn(mul_rn((VT)(-a), q[i]), r[i]);
+    r[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    const long long L = st->k.loop;
+    if (mode == 0) {
+      st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
+      st->k.s[S_RR] = s[0];
+    }
+    check_top(st, L + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
+  }
+};
+
+template <class VT>
+struct Ws {  // carve n-length vectors out of one workspace block
+  VT *base;
+  long long n;
+  int used = 0;
+  VT *take(int count = 1) {
+    VT *p = base + (long long)used * n;
+    used += count;
+    return p;
+  }
+};
+
+template <class VT>
+ks_status init_state(const Env<VT> &E, const VT *b) {
+  launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  launch_vec(E.ctx, E.n, NormBOp<VT>{b, E.st}, Stop{nullptr, E.outer_done});
+  return KS_OK;
+}
+
+inline int cg_vectors() { return 3; }
+
+template <class VT>
+ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
+  Ws<VT> W{ws, E.n};
+  VT *r = W.take(), *p = W.take(), *q = W.take();
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CG});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  for (long long L = 1; L <= E.sp.maxloop; L++) {
+    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
+    vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 0});
+    vec(E, XpbyOp<VT>{p, r, &E.st->k.s[S_BETA]});
+    if (E.outer && P.step()) break;
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ CR
+// cr::solve (cr.cpp:152-263): x/r update with check; s = A r, (r,s) -> beta;
+// p = beta p + r, q = beta q + s with (q,q) -> next alpha.
+template <class VT>
+struct CrStartMvEpi {  // q = A p; s = q; rs = (r,s); alpha = rs/(q,q)
+  using acc_t = VT;
+  const VT *r;
+  VT *q;
+  VT *s;
+  DevState *st;
+  static constexpr int ND = 2;
+  __device__ void row(int i, VT v, double (&acc)[2]) const {
+    q[i] = v;
+    s[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(r[i]), widen(v)));
+    acc[1] = add_rn(acc[1], mul_rn(widen(v), widen(v)));
+  }
+  __device__ void finish(const double (&sm)[2]) const {
+    st->k.s[S_RR] = sm[0];
+    st->k.s[S_ALPHA] = rdiv(st, sm[0], sm[1]);
+  }
+};
+
+template <class VT>
+struct CrMvEpi {  // s = A r; rs2 = (r,s); beta = rs2/rs; rs = rs2
+  using acc_t = VT;
+  const VT *r;
+  VT *s;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    s[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(r[i]), widen(v)));
+  }
+  __device__ void finish(const double (&sm)[1]) const {
+    st->k.s[S_BETA] = rdiv(st, sm[0], st->k.s[S_RR]);
+    st->k.s[S_RR] = sm[0];
+  }
+};
+
+inline int cr_vectors() { return 4; }
+
+template <class VT>
+ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
+  Ws<VT> W{ws, E.n};
+  VT *r = W.take(), *p = W.take(), *q = W.take(), *s = W.take();
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CHECK});
+  mv(E, *E.A, (const VT *)p, CrStartMvEpi<VT>{r, q, s, E.st});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  for (long long L = 1; L <= E.sp.maxloop; L++) {
+    vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 1});
+    mv(E, *E.A, (const VT *)r, CrMvEpi<VT>{r, s, E.st});
+    vec(E, Xpby2Op<VT>{p, r, q, s, E.st, 1});
+    if (E.outer && P.step()) break;
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ BiCG
+// bicg::solve (bicg.cpp:162-277).
+template <class VT>
+struct BicgMvTEpi {  // r* = -alpha (A^T p*) + r*; rr2 = (r*, r) -> beta
+  using acc_t = VT;
+  VT *rs;
+  const VT *r;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
+    const VT ri = add_rn(mul_rn((VT)(-a), v), rs[i]);
+    rs[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(r[i])));
+  }
+  __device__ void finish(const double (&sm)[1]) const {
+    st->k.s[S_BETA] = rdiv(st, sm[0], st->k.s[S_RR]);
+    st->k.s[S_RR] = sm[0];
+  }
+};
+
+template <class VT>
+struct Xpby2PlainOp {  // p = beta p + r; ps = beta ps + rs
+  VT *p;
+  const VT *r;
+  VT *ps;
+  const VT *rs;
+  const double *beta;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const {
+    const VT b = (VT)rd(beta);
+    p[i] = add_rn(mul_rn(b, p[i]), r[i]);
+    ps[i] = add_rn(mul_rn(b, ps[i]), rs[i]);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+inline int bicg_vectors() { return 5; }
+
+template <class VT>
+ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
+  Ws<VT> W{ws, E.n};
+  VT *r = W.take(), *rs = W.take(), *p = W.take(), *ps = W.take(), *mvv = W.take();
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  // (r*, r) = (r, r) at the start
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, rs, p, ps, E.st, START_CG});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  for (long long L = 1; L <= E.sp.maxloop; L++) {
+    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
+    vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
+    mv(E, *E.AT, (const VT *)ps, BicgMvTEpi<VT>{rs, r, E.st});
+    vec(E, Xpby2PlainOp<VT>{p, r, ps, rs, &E.st->k.s[S_BETA]});
+    if (E.outer && P.step()) break;
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ GCR
+// gcr::solve (gcr.cpp:178-317). Device arrays: qq[m], beta[m].
+template <class VT>
+struct GcrQ0Epi {  // Q0 = A P0; qq[0] = (Q0,Q0); rq = (r,Q0) -> alpha
+  using acc_t = VT;
+  const VT *r;
+  VT *q0;
+  double *qq;
+  DevState *st;
+  static constexpr int ND = 2;
+  __device__ void row(int i, VT v, double (&acc)[2]) const {
+    q0[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(v), widen(v)));
+    acc[1] = add_rn(acc[1], mul_rn(widen(r[i]), widen(v)));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    qq[0] = s[0];
+    st->k.s[S_ALPHA] = rdiv(st, s[1], s[0]);
+  }
+};
+
+// x += alpha P_k; if (!last) { r -= alpha Q_k; (r,r) -> check }.
+template <class VT>
+struct GcrXrOp {
+  VT *x;
+  VT *r;
+  const VT *pk;
+  const VT *qk;
+  DevState *st;
+  int last;
+  static constexpr int ND = 1;
+  __device__ void elem(long long i, double (&acc)[1]) const {
+    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
+    x[i] = add_rn(mul_rn(a, pk[i]), x[i]);
+    if (!last) {
+      const VT ri = add_rn(mul_rn((VT)(-a), qk[i]), r[i]);
+      r[i] = ri;
+      acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+    }
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    if (!last) check_gcr(st, sqrt(s[0]) / st->k.s[S_BNORM]);
+  }
+};
+
+struct GcrBetaPut {  // beta[i] = -(Av, Q_i) / qq[i]   (blas::Gcr_sp_1)
+  double *beta;
+  const double *qq;
+  DevState *st;
+  __device__ void put(int, int i, double v) const { beta[i] = rdiv(st, -v, qq[i]); }
+};
+
+// P_{k+1} = z + sum_i beta_i P_i, Q_{k+1} = Av + sum_i beta_i Q_i, the sums
+// accumulated from zero in index order (gcr.cpp:277-308); then
+// qq[k+1] = (Q_{k+1},Q_{k+1}) and alpha = (r, Q_{k+1}) / qq[k+1].
+template <class VT>
+struct GcrPQOp {
+  const VT *P;
+  const VT *Q;
+  long long n;
+  int k1;  // number of terms (k+1)
+  const double *beta;
+  const VT *z;
+  const VT *Av;
+  const VT *r;
+  VT *pn;
+  VT *qn;
+  double *qq_next;
+  DevState *st;
+  static constexpr int ND = 2;
+  __device__ void elem(long long j, double (&acc)[2]) const {
+    VT pa = (VT)0, qa = (VT)0;
+    for (int i = 0; i < k1; i++) {
+      const VT bi = (VT)rd(beta + i);
+      pa = add_rn(mul_rn(bi, P[(long long)i * n + j]), pa);
+      qa = add_rn(mul_rn(bi, Q[(long long)i * n + j]), qa);
+    }
+    pn[j] = add_rn(z[j], pa);
+    const VT qv = add_rn(Av[j], qa);
+    qn[j] = qv;
+    acc[0] = add_rn(acc[0], mul_rn(widen(qv), widen(qv)));
+    acc[1] = add_rn(acc[1], mul_rn(widen(r[j]), widen(qv)));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    *qq_next = s[0];
+    st->k.s[S_ALPHA] = rdiv(st, s[1], s[0]);
+  }
+};
+
+template <class VT>
+struct InnerRunner;  // VP inner solves (defined below)
+
+struct SetLoopOp {
+  DevState *st;
+  long long v;
+  __device__ void run() const { st->k.loop = v; }
+};
+
+struct SqrtTOp {  // s[T] = sqrt(s[T])
+  DevState *st;
+  __device__ void run() const { st->k.s[S_T] = sqrt(st->k.s[S_T]); }
+};
+
+// Shared GCR / VPGCR body. With `inner` set, each new direction is the inner
+// solver's approximation of A^{-1} r (vpgcr.cpp:693-846).
+template <class VT>
+ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws,
+                       InnerRunner<VT> *inner) {
+  const long long n = E.n;
+  const int m = (int)E.sp.restart;
+  Ws<VT> W{ws, n};
+  VT *r = W.take(), *Av = W.take(), *z = W.take();
+  VT *P = W.take(m), *Q = W.take(m);
+  double *qq = dws, *beta = dws + m;
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  launch_scalar(E.ctx, SetLoopOp{E.st, 1}, E.stop());  // loop = 1 (gcr.cpp:41)
+  Poller P_{E.ctx, E.hflag, E.lookahead};
+  long long issued_steps = 0;
+  bool stop_host = false;
+  while (!stop_host) {
+    // cycle start: r = b - A x, then the first direction
+    if (inner) {
+      mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_GCR});
+      inner->solve(r, P);  // P_0 = M(r)
+    } else {
+      mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, P, nullptr, nullptr, E.st, START_GCR});
+    }
+    mv(E, *E.A, (const VT *)P, GcrQ0Epi<VT>{r, Q, qq, E.st});
+    for (int k = 0; k < m; k++) {
+      const bool last = (k == m - 1);
+      vec(E, GcrXrOp<VT>{x, r, P + (long long)k * n, Q + (long long)k * n, E.st, last ? 1 : 0});
+      issued_steps++;
+      if (last) break;
+      const VT *znew = r;
+      if (inner) {
+        inner->solve(r, z);
+        znew = z;
+      }
+      mv(E, *E.A, znew, StoreEpi<VT, VT>{Av});
+      KS_TRY(launch_block_dot<1, VT>(E.ctx, Q, n, k + 1, Av, nullptr, n, GcrBetaPut{beta, qq, E.st},
+                                     E.stop()));
+      vec(E, GcrPQOp<VT>{P, Q, n, k + 1, beta, znew, Av, r, P + (long long)(k + 1) * n,
+                         Q + (long long)(k + 1) * n, qq + k + 1, E.st});
+      // Each step is one check of the loop counter, so the method has
+      // stopped on the device after at most maxloop steps.
+      if ((E.outer && P_.step()) || issued_steps >= E.sp.maxloop) {
+        stop_host = true;
+        break;
+      }
+    }
+    if (stop_host || (E.outer && P_.step()) || issued_steps >= E.sp.maxloop) break;
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ GMRES
+// gmres::solve (gmres.cpp:232-422) / vpgmres::solve (vpgmres.cpp:746-944).
+// Device arrays: H (m+1) x m row-major, cs[m], sn[m], e[m+1], y[m].
+struct GmArrays {
+  double *H, *cs, *sn, *e, *y;
+  int m;
+};
+
+template <class VT>
+struct ScaleOp {  // out = a / t, t from slot (Scalar_x_div_a)
+  const VT *a;
+  VT *out;
+  const double *t;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const {
+    out[i] = div_rn(a[i], (VT)rd(t));
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+// Cycle start scalars: e = 0, e[0] = t; done checks happen per step.
+struct GmCycleOp {
+  GmArrays g;
+  DevState *st;
+  __device__ void run() const {
+    for (int i = 0; i < g.m; i++) g.e[i] = 0.0;
+    g.e[0] = st->k.s[S_T];
+    st->k.aux[A_KIDX] = 0;
+  }
+};
+
+// Stopping test of step k (gmres.cpp:270-324): record (count+1, |e_k|/|b|);
+// maxloop first, then eps. The device remembers k for the final assembly.
+struct GmCheckOp {
+  GmArrays g;
+  DevState *st;
+  int k;
+  __device__ void run() const {
+    const long long count = st->k.loop;
+    const double err = fabs(g.e[k]) / st->k.s[S_BNORM];
+    record(st, count + 1, err);
+    st->k.aux[A_CONVK] = k;
+    if (count + 1 >= st->k.aux[A_MAXLOOP])
+      set_done(st, kMaxLoop);
+    else if (err <= st->k.s[S_EPS])
+      set_done(st, kConverged);
+    else if (err != err)
+      set_done(st, kNaN);
+  }
+};
+
+struct GmPutH {  // H[i][k] = (w, V_i)
+  double *H;
+  int m, k;
+  __device__ void put(int, int i, double v) const { H[(long long)i * m + k] = v; }
+};
+
+// H[k+1][k] = |w| arrives in s[T] from the block AXPY; then the Givens
+// rotations of column k (gmres.cpp:384-399) and count++.
+struct GmGivensOp {
+  GmArrays g;
+  DevState *st;
+  int k;
+  __device__ void run() const {
+    const int m = g.m;
+    double *H = g.H;
+    H[(long long)(k + 1) * m + k] = st->k.s[S_T];
+    for (int i = 0; i <= k - 1; i++) {
+      const double t1 = H[(long long)i * m + k], t2 = H[(long long)(i + 1) * m + k];
+      H[(long long)i * m + k] = g.cs[i] * t1 - g.sn[i] * t2;
+      H[(long long)(i + 1) * m + k] = g.sn[i] * t1 + g.cs[i] * t2;
+    }
+    const double hkk = H[(long long)k * m + k], hk1 = H[(long long)(k + 1) * m + k];
+    const double a = sqrt(hkk * hkk + hk1 * hk1);
+    g.cs[k] = hkk / a;
+    g.sn[k] = -hk1 / a;
+    g.e[k + 1] = g.sn[k] * g.e[k];
+    g.e[k] = g.cs[k] * g.e[k];
+    H[(long long)k * m + k] = g.cs[k] * H[(long long)k * m + k] - g.sn[k] * H[(long long)(k + 1) * m + k];
+    H[(long long)(k + 1) * m + k] = 0.0;
+    st->k.loop += 1;
+  }
+};
+
+// Back substitution y = H^{-1} e on the leading size x size block
+// (blas::Hye, blas.cpp:303-314). size < 0: take size from the stop step.
+struct GmHyeOp {
+  GmArrays g;
+  DevState *st;
+  int size;
+  int final_mode;  // 1: run only when the method has stopped and not yet assembled
+  __device__ void run() const {
+    if (final_mode) {
+      const int d = st->k.done;
+      if (!(d == kConverged || d == kMaxLoop) || st->k.aux[A_FINAL]) return;
+    }
+    const int sz = size >= 0 ? size : (int)st->k.aux[A_CONVK];
+    for (int i = 0; i < g.m; i++) g.y[i] = 0.0;
+    for (int i = sz - 1; i >= 0; i--) {
+      double t = 0.0;
+      for (int j = i + 1; j < sz; j++) t += g.y[j] * g.H[(long long)i * g.m + j];
+      g.y[i] = (g.e[i] - t) / g.H[(long long)i * g.m + i];
+    }
+  }
+};
+
+// x = x + sum_i y_i B_i, the sum accumulated from zero in index order
+// (gmres.cpp:409-419). With `final_mode` the count comes from the stop step;
+// `overwrite` reproduces the reference's Scalar_ax assembly
+// (gmres.cpp:290-297): only the last term survives.
+template <class VT>
+struct GmUpdateOp {
+  const VT *B;
+  long long n;
+  int cnt;
+  const double *y;
+  VT *x;
+  const DevState *st;
+  int final_mode;
+  int overwrite;
+  static constexpr int ND = 0;
+  __device__ void elem(long long j, double (&)[1]) const {
+    int c = cnt;
+    if (final_mode) c = (int)st->k.aux[A_CONVK];
+    VT t = (VT)0;
+    if (overwrite) {
+      if (c > 0) t = mul_rn((VT)rd(y + c - 1), B[(long long)(c - 1) * n + j]);
+    } else {
+      for (int i = 0; i < c; i++) t = add_rn(t, mul_rn((VT)rd(y + i), B[(long long)i * n + j]));
+    }
+    x[j] = add_rn(x[j], t);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+// Final assembly runs in a kernel that is not gated by `done`; it checks the
+// stop reason itself and marks the state assembled.
+template <class VT>
+__global__ void gm_final_kernel(GmUpdateOp<VT> op, DevState *st, const int *outer_done) {
+  if (outer_done && *(volatile const int *)outer_done) return;
+  const int d = st->k.done;
+  if (!(d == kConverged || d == kMaxLoop) || st->k.aux[A_FINAL]) return;
+  double acc[1];
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < op.n;
+       j += (long long)gridDim.x * blockDim.x)
+    op.elem(j, acc);
+}
+
+struct GmMarkFinal {
+  DevState *st;
+  __device__ void run() const {
+    const int d = st->k.done;
+    if ((d == kConverged || d == kMaxLoop) && !st->k.aux[A_FINAL]) st->k.aux[A_FINAL] = 1;
+  }
+};
+
+template <class VT>
+ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws,
+                         InnerRunner<VT> *inner) {
+  const long long n = E.n;
+  const int m = (int)E.sp.restart;
+  if (m < 2) return set_error(E.ctx, KS_BAD_INPUT, "GMRES needs restart >= 2");
+  Ws<VT> W{ws, n};
+  VT *r = W.take(), *w = W.take(), *z = W.take();
+  VT *V = W.take(m + 1);
+  VT *Z = inner ? W.take(m) : nullptr;
+  GmArrays g{dws, dws + (long long)(m + 1) * m, dws + (long long)(m + 1) * m + m,
+             dws + (long long)(m + 1) * m + 2 * m, dws + (long long)(m + 1) * m + 3 * m + 1, m};
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  long long issued = 0;
+  bool stop_host = false;
+  const VT *B = inner ? Z : V;
+  while (!stop_host) {
+    mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_NORM});
+    vec(E, ScaleOp<VT>{r, V, &E.st->k.s[S_T]});
+    launch_scalar(E.ctx, GmCycleOp{g, E.st}, E.stop());
+    for (int k = 0; k < m - 1; k++) {
+      launch_scalar(E.ctx, GmCheckOp{g, E.st, k}, E.stop());
+      const VT *vk = V + (long long)k * n;
+      if (inner) {
+        inner->solve(vk, Z + (long long)k * n);
+        mv(E, *E.A, (const VT *)(Z + (long long)k * n), StoreEpi<VT, VT>{w});
+      } else {
+        mv(E, *E.A, vk, StoreEpi<VT, VT>{w});
+      }
+      KS_TRY(launch_block_dot<1, VT>(E.ctx, V, n, k + 1, w, nullptr, n, GmPutH{g.H, m, k}, E.stop()));
+      vec(E, BlockAxpyOp<VT>{V, n, k + 1, g.H + k, m, w, &E.st->k.s[S_T]});
+      launch_scalar(E.ctx, SqrtTOp{E.st}, E.stop());
+      vec(E, ScaleOp<VT>{w, V + (long long)(k + 1) * n, &E.st->k.s[S_T]});
+      launch_scalar(E.ctx, GmGivensOp{g, E.st, k}, E.stop());
+      issued++;
+      if (E.outer && P.step()) {
+        stop_host = true;
+        break;
+      }
+      if (issued >= E.sp.maxloop) {
+        stop_host = true;
+        break;
+      }
+    }
+    if (stop_host) break;
+    // end of cycle (gmres.cpp:409-421)
+    launch_scalar(E.ctx, GmHyeOp{g, E.st, m - 1, 0}, E.stop());
+    vec(E, GmUpdateOp<VT>{B, n, m - 1, g.y, x, E.st, 0, 0});
+    if (E.outer && P.step()) break;
+  }
+  // The step that stopped the method (converged or maxloop) assembles x.
+  launch_scalar(E.ctx, GmHyeOp{g, E.st, -1, 1}, Stop{nullptr, E.outer_done});
+  {
+    GmUpdateOp<VT> op{B, n, 0, g.y, x, E.st, 1, E.faithful ? 1 : 0};
+    int grid = red_grid(E.ctx);
+    E.ctx->launches++;
+    gm_final_kernel<VT><<<grid, kThreads, 0, E.ctx->stream>>>(op, E.st, E.outer_done);
+  }
+  launch_scalar(E.ctx, GmMarkFinal{E.st}, Stop{nullptr, E.outer_done});
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ k-skip CG
+// kskipcg::solve (kskipcg.cpp:187-310). Per block of k+1 iterations: the
+// matrix powers (4k+3 SpMVs in 2k+2 shared passes), one Gram pass, the scalar
+// recurrence for all k+1 steps on the device, then k+1 x (SpMV + update).
+// Device arrays: G = [delta(2k) | eta(2k+2) | zeta(2k+2)], coef = [alpha | beta](k+1).
+struct KsCheckOp {  // gamma = (r,r) arrives in s[GAMMA]; check (nloop+1)
+  DevState *st;
+  long long nloop;
+  __device__ void run() const {
+    st->k.loop = nloop;
+    const double g = st->k.s[S_GAMMA];
+    const double err = sqrt(g) / st->k.s[S_BNORM];
+    record(st, nloop + 1, err);
+    if (err <= st->k.s[S_EPS])
+      set_done(st, kConverged);
+    else if (err != err)
+      set_done(st, kNaN);
+  }
+};
+
+struct KsCgRecOp {
+  DevState *st;
+  double *G;  // delta | eta | zeta
+  double *coef;
+  int k, fix, fixed;
+  __device__ void run() const {
+    double *delta = G, *eta = G + 2 * k, *zeta = G + 4 * k + 2;
+    double gamma = st->k.s[S_GAMMA];
+    for (int i = 0; i <= k; i++) {
+      const double alpha = gamma / zeta[0];
+      const double beta = alpha * zeta[1] / zeta[0] - 1.0;
+      if (fix == 1) {
+        gamma = beta * gamma;
+      } else if (fix == 2) {
+        const double t0 = gamma - alpha * eta[0];
+        const double t1 = eta[0] - alpha * zeta[1];
+        gamma = t0 - alpha * t1;
+      }
+      const int cnt = 2 * k - 2 * i;
+      for (int j = 0; j < cnt; j++) {
+        if (!fixed) {
+          delta[j] = delta[j] - 2 * alpha * eta[j + 1] + alpha * alpha * eta[j + 2];
+          const double eta_old = eta[j];
+          eta[j] = delta[j] + beta * zeta[j + 1] - alpha * beta * zeta[j + 1];
+          zeta[j] = eta[j + 1] + beta * eta_old + beta * beta * zeta[j] - alpha * beta * zeta[j + 1];
+        } else {
+          const double d = delta[j] - 2 * alpha * eta[j + 1] + alpha * alpha * zeta[j + 2];
+          const double rp = eta[j] - alpha * zeta[j + 1];
+          const double e = d + beta * rp;
+          const double z = e + beta * rp + beta * beta * zeta[j];
+          delta[j] = d;
+          eta[j] = e;
+          zeta[j] = z;
+        }
+      }
+      coef[i] = alpha;
+      coef[k + 1 + i] = beta;
+    }
+  }
+};
+
+// x += a p; r -= a Av; p = b p + r (kskipcg.cpp:292-305).
+template <class VT>
+struct KsUpdOp {
+  VT *x;
+  VT *r;
+  VT *p;
+  const VT *Av;
+  const double *a;
+  const double *bt;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const {
+    const VT al = (VT)rd(a), be = (VT)rd(bt);
+    const VT pi = p[i];
+    x[i] = add_rn(mul_rn(al, pi), x[i]);
+    const VT ri = add_rn(mul_rn((VT)(-al), Av[i]), r[i]);
+    r[i] = ri;
+    p[i] = add_rn(mul_rn(be, pi), ri);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+template <class VT>
+struct GammaOp {  // s[GAMMA] = (u, v)
+  const VT *u;
+  const VT *v;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void elem(long long i, double (&acc)[1]) const {
+    acc[0] = add_rn(acc[0], mul_rn(widen(u[i]), widen(v[i])));
+  }
+  __device__ void finish(const double (&s)[1]) const { st->k.s[S_GAMMA] = s[0]; }
+};
+
+template <class VT>
+struct Store2 {
+  using acc_t = VT;
+  VT *y0, *y1;
+  static constexpr int ND = 0;
+  __device__ void row(int r, VT a, VT b, double (&)[1]) const {
+    y0[r] = a;
+    y1[r] = b;
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+template <class VT>
+void matpow_t(const Env<VT> &E, const VT *r, const VT *p, int k, VT *Ar, VT *Ap) {
+  const long long n = E.n;
+  auto mv2 = [&](const VT *a, const VT *b2, VT *o0, VT *o1) {
+    if constexpr (std::is_same<VT, double>::value) {
+      launch_spmv2<double, double>(E.ctx, *E.A, a, b2, Store2<VT>{o0, o1}, E.stop());
+    } else {
+      if (E.mvals == KS_BF16)
+        launch_spmv2<__nv_bfloat16, float>(E.ctx, *E.A, a, b2, Store2<VT>{o0, o1}, E.stop());
+      else
+        launch_spmv2<float, float>(E.ctx, *E.A, a, b2, Store2<VT>{o0, o1}, E.stop());
+    }
+  };
+  mv2(r, p, Ar, Ap);
+  for (int i = 1; i < 2 * k + 1; i++)
+    mv2(Ar + (long long)(i - 1) * n, Ap + (long long)(i - 1) * n, Ar + (long long)i * n,
+        Ap + (long long)i * n);
+  mv(E, *E.A, (const VT *)(Ap + (long long)(2 * k) * n), StoreEpi<VT, VT>{Ap + (long long)(2 * k + 1) * n});
+}
+
+template <class VT>
+ks_status run_kskipcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
+  const long long n = E.n;
+  const int k = E.sp.kskip;
+  if (k < 0) return set_error(E.ctx, KS_BAD_INPUT, "kskip must be >= 0");
+  Ws<VT> W{ws, n};
+  VT *r = W.take(), *p = W.take(), *Av = W.take();
+  VT *Ar = W.take(2 * k + 1), *Ap = W.take(2 * k + 2);
+  double *G = dws, *coef = dws + 6 * k + 4;
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_KSKIP});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  long long nloop = 0;
+  for (nloop = 0; nloop < E.sp.maxloop; nloop += k + 1) {
+    vec(E, GammaOp<VT>{r, r, E.st});
+    launch_scalar(E.ctx, KsCheckOp{E.st, nloop}, E.stop());
+    matpow_t(E, r, p, k, Ar, Ap);
+    if (k > 0)
+      KS_TRY(launch_block_dot<1, VT>(E.ctx, Ar, n, 2 * k, r, nullptr, n, PutArray{G, 0, 1}, E.stop()));
+    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ap, n, 2 * k + 2, r, p, n,
+                                   PutArray{G + 2 * k, 2 * k + 2, 1}, E.stop()));
+    launch_scalar(E.ctx, KsCgRecOp{E.st, G, coef, k, E.sp.fix, E.faithful ? 0 : 1}, E.stop());
+    for (int i = 0; i <= k; i++) {
+      mv(E, *E.A, (const VT *)p, StoreEpi<VT, VT>{Av});
+      vec(E, KsUpdOp<VT>{x, r, p, Av, coef + i, coef + k + 1 + i});
+    }
+    if (E.outer && P.step()) break;
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ k-skip BiCG
+// kskipBicg::solve (kskipbicg.cpp:207-352).
+// G = [theta(2k+1) | rho(2k+1) | eta(2k+2) | phi(2k+2)].
+struct KsBicgRecOp {
+  DevState *st;
+  double *G;
+  double *coef;
+  int k;
+  __device__ void run() const {
+    double *theta = G, *rho = G + 2 * k + 1, *eta = G + 4 * k + 2, *phi = G + 6 * k + 4;
+    double gamma = st->k.s[S_GAMMA];
+    for (int i = 0; i <= k; i++) {
+      const double alpha = gamma / phi[0];
+      const double beta = 1.0 - (eta[0] + rho[0] - alpha * phi[1]) / phi[0];
+      gamma = gamma * beta;
+      const int cnt = 2 * k - 2 * i;
+      for (int j = 0; j < cnt; j++) {
+        theta[j] = theta[j] - alpha * eta[j + 1] - alpha * rho[j + 1] + alpha * alpha * phi[j + 2];
+        const double t = theta[j] - alpha * beta * phi[j + 1];
+        eta[j] = t + beta * eta[j];
+        rho[j] = t + beta * rho[j];
+        phi[j] = eta[j] + rho[j] - theta[j] + beta * beta * phi[j];
+      }
+      coef[i] = alpha;
+      coef[k + 1 + i] = beta;
+    }
+  }
+};
+
+template <class VT>
+struct KsXrOp {  // x += a p; r -= a Av
+  VT *x;
+  VT *r;
+  const VT *p;
+  const VT *Av;
+  const double *a;
+  static constexpr int ND = 0;
+  __device__ void elem(long long i, double (&)[1]) const {
+    const VT al = (VT)rd(a);
+    x[i] = add_rn(mul_rn(al, p[i]), x[i]);
+    r[i] = add_rn(mul_rn((VT)(-al), Av[i]), r[i]);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+template <class VT>
+struct KsRsEpi {  // r* = -a (A^T p*) + r*
+  using acc_t = VT;
+  VT *rs;
+  const double *a;
+  static constexpr int ND = 0;
+  __device__ void row(int i, VT v, double (&)[1]) const {
+    rs[i] = add_rn(mul_rn((VT)(-rd(a)), v), rs[i]);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+template <class VT>
+ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
+  const long long n = E.n;
+  const int k = E.sp.kskip;
+  if (k < 0) return set_error(E.ctx, KS_BAD_INPUT, "kskip must be >= 0");
+  Ws<VT> W{ws, n};
+  VT *r = W.take(), *p = W.take(), *rs = W.take(), *ps = W.take(), *Av = W.take();
+  VT *Ar = W.take(2 * k + 1), *Ap = W.take(2 * k + 2);
+  double *G = dws, *coef = dws + 8 * k + 6;
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, rs, ps, E.st, START_KSKIP});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  for (long long nloop = 0; nloop < E.sp.maxloop; nloop += k + 1) {
+    // the check uses |r|; gamma = (r*, r) comes right after
+    vec(E, GammaOp<VT>{r, r, E.st});
+    launch_scalar(E.ctx, KsCheckOp{E.st, nloop}, E.stop());
+    matpow_t(E, r, p, k, Ar, Ap);
+    vec(E, GammaOp<VT>{rs, r, E.st});
+    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ar, n, 2 * k + 1, rs, ps, n, PutArray{G, 2 * k + 1, 1},
+                                   E.stop()));
+    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ap, n, 2 * k + 2, rs, ps, n,
+                                   PutArray{G + 4 * k + 2, 2 * k + 2, 1}, E.stop()));
+    launch_scalar(E.ctx, KsBicgRecOp{E.st, G, coef, k}, E.stop());
+    for (int i = 0; i <= k; i++) {
+      mv(E, *E.A, (const VT *)p, StoreEpi<VT, VT>{Av});
+      vec(E, KsXrOp<VT>{x, r, p, Av, coef + i});
+      mv(E, *E.AT, (const VT *)ps, KsRsEpi<VT>{rs, coef + i});
+      vec(E, Xpby2PlainOp<VT>{p, r, ps, rs, coef + k + 1 + i});
+    }
+    if (E.outer && P.step()) break;
+  }
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ sizes
+inline long long vec_count(int method, const Params &sp) {
+  const long long m = sp.restart, k = sp.kskip;
+  switch (method) {
+    case KS_CG: return 3;
+    case KS_CR: return 4;
+    case KS_BICG: return 5;
+    case KS_GCR: case KS_VPGCR: return 3 + 2 * m;
+    case KS_GMRES: return 3 + (m + 1);
+    case KS_VPGMRES: return 3 + (m + 1) + m;
+    case KS_KSKIPCG: return 3 + (2 * k + 1) + (2 * k + 2);
+    case KS_KSKIPBICG: return 5 + (2 * k + 1) + (2 * k + 2);
+    case KS_VPCG: return 4;
+    case KS_VPCR: return 5;
+  }
+  return 0;
+}
+
+inline long long dws_count(int method, const Params &sp) {
+  const long long m = sp.restart, k = sp.kskip;
+  switch (method) {
+    case KS_GCR: case KS_VPGCR: return 2 * m + 2;
+    case KS_GMRES: case KS_VPGMRES: return (m + 1) * m + 4 * m + 4;
+    case KS_KSKIPCG: return 6 * k + 4 + 2 * (k + 1) + 4;
+    case KS_KSKIPBICG: return 8 * k + 6 + 2 * (k + 1) + 4;
+  }
+  return 4;
+}
+
+// ------------------------------------------------------------------ inner solves
+// A VP method's inner solve z ~ A^{-1} r (innerMethods::innerSelect,
+// innerMethods.cpp:71-118): a fresh run of the inner method with the inner
+// parameters, zero start, no history. In FP32/BF16 mode the right-hand side
+// is rounded to FP32 on entry and z widened back to FP64 on exit.
+template <class IT>
+ks_status run_method(int method, const Env<IT> &E, const IT *b, IT *x, IT *ws, double *dws,
+                     InnerRunner<IT> *inner);
+
+template <class VT>
+struct InnerRunner {
+  // Outer-precision view (VT) and the inner environment.
+  ks_ctx *ctx = nullptr;
+  int method = KS_NONE;
+  ks_precision iprec = KS_FP64;
+  long long n = 0;
+  Env<double> E64;
+  Env<float> E32;
+  double *ws64 = nullptr;
+  float *ws32 = nullptr;
+  double *dws = nullptr;
+  float *b32 = nullptr, *z32 = nullptr;
+  long long calls = 0;
+  ks_status status = KS_OK;
+  void solve(const VT *b, VT *z);
+};
+
+template <class VT>
+void InnerRunner<VT>::solve(const VT *b, VT *z) {
+  calls++;
+  if (status != KS_OK) return;
+  if constexpr (std::is_same<VT, double>::value) {
+    if (iprec == KS_FP64) {
+      status = run_method<double>(method, E64, b, z, ws64, dws, nullptr);
+    } else {
+      launch_vec(ctx, n, ConvertOp<double, float>{b, b32}, Stop{nullptr, E32.outer_done});
+      status = run_method<float>(method, E32, b32, z32, ws32, dws, nullptr);
+      launch_vec(ctx, n, ConvertOp<float, double>{z32, z}, Stop{nullptr, E32.outer_done});
+    }
+  } else {
+    status = KS_UNIMPLEMENTED;  // VP methods run their outer loop in FP64
+  }
+}
+
+// ------------------------------------------------------------------ VPCG / VPCR
+template <class VT>
+struct RzOp {  // rr2 = (r, z); beta = rr2 / rr; rr = rr2   (vpcg.cpp:733-745)
+  const VT *r;
+  const VT *z;
+  DevState *st;
+  int init;  // 1: just rr = (r,z)
+  static constexpr int ND = 1;
+  __device__ void elem(long long i, double (&acc)[1]) const {
+    acc[0] = add_rn(acc[0], mul_rn(widen(r[i]), widen(z[i])));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    if (!init) st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
+    st->k.s[S_RR] = s[0];
+  }
+};
+
+template <class VT>
+ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT> *inner) {
+  Ws<VT> W{ws, E.n};
+  VT *r = W.take(), *p = W.take(), *z = W.take(), *mvv = W.take();
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
+  inner->solve(r, z);
+  vec(E, CopyOp<VT>{z, p});
+  vec(E, RzOp<VT>{r, z, E.st, 1});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  for (long long L = 1; L <= E.sp.maxloop; L++) {
+    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, mvv, E.st});
+    vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
+    inner->solve(r, z);
+    vec(E, RzOp<VT>{r, z, E.st, 0});
+    vec(E, XpbyOp<VT>{p, z, &E.st->k.s[S_BETA]});
+    if (P.step()) break;
+  }
+  return KS_OK;
+}
+
+template <class VT>
+struct VpcrMvEpi {  // Av = A z; zaz(2) = (z, Av); init: Ap = Av, alpha from (Ap,Ap)
+  using acc_t = VT;
+  const VT *z;
+  VT *Av;
+  VT *Ap;  // set on init
+  DevState *st;
+  int init;
+  static constexpr int ND = 2;
+  __device__ void row(int i, VT v, double (&acc)[2]) const {
+    Av[i] = v;
+    if (init) Ap[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(z[i]), widen(v)));
+    acc[1] = add_rn(acc[1], mul_rn(widen(v), widen(v)));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    if (init) {
+      st->k.s[S_RR] = s[0];
+      st->k.s[S_ALPHA] = rdiv(st, s[0], s[1]);
+    } else {
+      st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
+      st->k.s[S_RR] = s[0];
+    }
+  }
+};
+
+template <class VT>
+ks_status run_vpcr(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT> *inner) {
+  Ws<VT> W{ws, E.n};
+  VT *r = W.take(), *p = W.take(), *z = W.take(), *Av = W.take(), *Ap = W.take();
+  init_state(E, b);
+  vec(E, ZeroOp<VT>{x});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
+  inner->solve(r, z);
+  vec(E, CopyOp<VT>{z, p});
+  mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, Ap, E.st, 1});
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  for (long long L = 1; L <= E.sp.maxloop; L++) {
+    vec(E, XrUpdOp<VT>{x, r, p, Ap, E.st, 1});
+    inner->solve(r, z);
+    mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, nullptr, E.st, 0});
+    vec(E, Xpby2Op<VT>{p, z, Ap, Av, E.st, 1});
+    if (P.step()) break;
+  }
+  return KS_OK;
+}
+
+template <class IT>
+ks_status run_method(int method, const Env<IT> &E, const IT *b, IT *x, IT *ws, double *dws,
+                     InnerRunner<IT> *inner) {
+  switch (method) {
+    case KS_CG: return run_cg(E, b, x, ws);
+    case KS_CR: return run_cr(E, b, x, ws);
+    case KS_BICG: return run_bicg(E, b, x, ws);
+    case KS_GCR: return run_gcr_core(E, b, x, ws, dws, (InnerRunner<IT> *)nullptr);
+    case KS_GMRES: return run_gmres_core(E, b, x, ws, dws, (InnerRunner<IT> *)nullptr);
+    case KS_KSKIPCG: return run_kskipcg(E, b, x, ws, dws);
+    case KS_KSKIPBICG: return run_kskipbicg(E, b, x, ws, dws);
+  }
+  if constexpr (std::is_same<IT, double>::value) {
+    switch (method) {
+      case KS_VPCG: return run_vpcg(E, b, x, ws, inner);
+      case KS_VPCR: return run_vpcr(E, b, x, ws, inner);
+      case KS_VPGCR: return run_gcr_core(E, b, x, ws, dws, inner);
+      case KS_VPGMRES: return run_gmres_core(E, b, x, ws, dws, inner);
+    }
+  }
+  return set_error(E.ctx, KS_UNIMPLEMENTED, "method not implemented");
+}
+
+static bool is_vp(int m) { return m == KS_VPCG || m == KS_VPCR || m == KS_VPGCR || m == KS_VPGMRES; }
+static bool is_inner_ok(int m) {
+  return m == KS_CG || m == KS_CR || m == KS_GCR || m == KS_BICG || m == KS_GMRES || m == KS_KSKIPCG ||
+         m == KS_KSKIPBICG;
+}
+static bool needs_T(int m) { return m == KS_BICG || m == KS_KSKIPBICG; }
+
+struct Alloc {  // RAII for pool buffers
+  ks_ctx *ctx;
+  std::vector<void *> bufs;
+  ~Alloc() {
+    for (void *p : bufs) pool_release(ctx, p);
+  }
+  template <class T>
+  ks_status get(size_t count, T **out) {
+    void *p = nullptr;
+    KS_TRY(pool_get(ctx, sizeof(T) * std::max<size_t>(count, 1) + 256, &p));
+    bufs.push_back(p);
+    *out = (T *)p;
+    return KS_OK;
+  }
+};
+
+__global__ void k_copy_state(const DevState *st, long long *out) {
+  out[0] = st->k.done;
+  out[1] = st->k.loop;
+  out[2] = st->k.hlen;
+  out[3] = st->k.aux[A_CONVK];
+}
+
+}  // namespace ks
+
+using namespace ks;
+
+static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                            const ks_params *prm, const double *b, double *x, int64_t *hist_iter,
+                            double *hist_err, int64_t hist_cap, ks_report *rep) {
+  if (outer == KS_KSKIPCR || outer == KS_VPBICG)
+    return set_error(ctx, KS_UNIMPLEMENTED, "Not implemented (as in the reference)");
+  const bool vp = is_vp(outer);
+  if (!vp && !is_inner_ok(outer)) return set_error(ctx, KS_BAD_INPUT, "unknown outer solver");
+  if (vp && !is_inner_ok(inner))
+    return set_error(ctx, KS_BAD_INPUT, "VP methods need an inner solver (cg cr gcr bicg gmres kskipcg kskipbicg)");
+  const bool trans = prm->transpose != 0;
+  const bool need_T = needs_T(outer) || (vp && needs_T(inner)) || trans;
+  if (need_T && !mat->has_T)
+    return set_error(ctx, KS_BAD_INPUT, "this method needs the transpose (upload with KS_MAT_TRANSPOSE)");
+  const CsrDev *A = trans ? &mat->T : &mat->A;
+  const CsrDev *AT = trans ? &mat->A : (mat->has_T ? &mat->T : &mat->A);
+  const ks_precision ip = vp ? (ks_precision)prm->inner_precision : KS_FP64;
+  if (ip == KS_FP32 && !A->val32) return set_error(ctx, KS_BAD_INPUT, "FP32 inner solve needs KS_MAT_FP32");
+  if (ip == KS_BF16 && !A->val16) return set_error(ctx, KS_BAD_INPUT, "BF16 inner solve needs KS_MAT_BF16");
+  if (ip != KS_FP64 && needs_T(inner) && !(ip == KS_FP32 ? (const void *)AT->val32 : (const void *)AT->val16))
+    return set_error(ctx, KS_BAD_INPUT, "low-precision inner BiCG needs the transpose's value copy");
+
+  Params outer_sp{prm->outer_maxloop, prm->outer_eps, prm->outer_restart, prm->outer_kskip, prm->outer_fix};
+  Params inner_sp{prm->inner_maxloop, prm->inner_eps, prm->inner_restart, prm->inner_kskip, prm->inner_fix};
+  if ((outer == KS_GCR || outer == KS_GMRES || outer == KS_VPGCR || outer == KS_VPGMRES) &&
+      (outer_sp.restart < 1 || outer_sp.restart > 1024))
+    return set_error(ctx, KS_BAD_INPUT, "restart must be in [1, 1024]");
+  if (vp && (inner == KS_GCR || inner == KS_GMRES) && (inner_sp.restart < 1 || inner_sp.restart > 1024))
+    return set_error(ctx, KS_BAD_INPUT, "inner restart must be in [1, 1024]");
+  if (outer_sp.kskip < 0 || outer_sp.kskip > 100 || inner_sp.kskip < 0 || inner_sp.kskip > 100)
+    return set_error(ctx, KS_BAD_INPUT, "kskip must be in [0, 100]");
+
+  KS_CUDA(ctx, cudaSetDevice(ctx->device));
+  const long long n = A->n;
+  Alloc al{ctx, {}};
+  // device state (outer, inner) and history
+  DevState *st = nullptr, *ist = nullptr;
+  KS_TRY(al.get(2, &st));
+  ist = st + 1;
+  const long long hcap = std::max<long long>(1, std::min<long long>(outer_sp.maxloop + 2, 1LL << 26));
+  double *d_hist = nullptr;
+  long long *d_hit = nullptr;
+  KS_TRY(al.get(hcap, &d_hist));
+  KS_TRY(al.get(hcap, &d_hit));
+  {
+    DevState h[2];
+    std::memset(h, 0, sizeof(h));
+    h[0].k.hist_err = d_hist;
+    h[0].k.hist_it = d_hit;
+    h[0].k.hcap = hcap;
+    h[0].host_done = nullptr;
+    int *mapped = nullptr;
+    if (cudaHostGetDevicePointer((void **)&mapped, ctx->h_flags, 0) == cudaSuccess) h[0].host_done = mapped;
+    else (void)cudaGetLastError();
+    KS_CUDA(ctx, cudaMemcpyAsync(st, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->h_flags[0] = 0;
+
+  // workspaces
+  double *ws = nullptr, *dws = nullptr;
+  KS_TRY(al.get((size_t)(vec_count(outer, outer_sp) * n), &ws));
+  KS_TRY(al.get((size_t)dws_count(outer, outer_sp), &dws));
+
+  Env<double> E;
+  E.ctx = ctx;
+  E.A = A;
+  E.AT = AT;
+  E.mvals = KS_FP64;
+  E.st = st;
+  E.record = true;
+  E.outer = true;
+  E.sp = outer_sp;
+  E.faithful = prm->reference_defects != 0;
+  E.n = n;
+  E.hflag = (volatile int *)ctx->h_flags;
+  E.lookahead = prm->poll_interval > 0 ? prm->poll_interval : (vp ? 2 : 8);
+  E.lookahead = std::min(E.lookahead, ctx->nflags - 1);  // event ring size
+  if (!ctx->h_flags || !st) return KS_CUDA_ERROR;
+
+  InnerRunner<double> IR;
+  if (vp) {
+    IR.ctx = ctx;
+    IR.method = inner;
+    IR.iprec = ip;
+    IR.n = n;
+    KS_TRY(al.get((size_t)dws_count(inner, inner_sp), &IR.dws));
+    if (ip == KS_FP64) {
+      Env<double> &I = IR.E64;
+      I = E;
+      I.st = ist;
+      I.outer_done = &st->k.done;
+      I.record = false;
+      I.outer = false;
+      I.sp = inner_sp;
+      I.hflag = nullptr;
+      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp) * n), &IR.ws64));
+    } else {
+      Env<float> &I = IR.E32;
+      I.ctx = ctx;
+      I.A = A;
+      I.AT = AT;
+      I.mvals = ip;
+      I.st = ist;
+      I.outer_done = &st->k.done;
+      I.record = false;
+      I.outer = false;
+      I.sp = inner_sp;
+      I.faithful = E.faithful;
+      I.n = n;
+      I.hflag = nullptr;
+      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp) * n), &IR.ws32));
+      KS_TRY(al.get((size_t)n, &IR.b32));
+      KS_TRY(al.get((size_t)n, &IR.z32));
+    }
+  }
+
+  KS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  ks_status s = run_method<double>(outer, E, b, x, ws, dws, vp ? &IR : nullptr);
+  if (s == KS_OK && vp) s = IR.status;
+  KS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  if (s != KS_OK) {
+    cudaStreamSynchronize(ctx->stream);
+    return s;
+  }
+  KS_CUDA(ctx, cudaGetLastError());
+  long long *d_out = nullptr;
+  KS_TRY(al.get(4, &d_out));
+  k_copy_state<<<1, 1, 0, ctx->stream>>>(st, d_out);
+  long long hs[4];
+  KS_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, d_out, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(hs, ctx->h_pinned, sizeof(hs));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  const int done = (int)hs[0];
+  ks_status st_code = KS_NOT_CONVERGED;
+  if (done == kConverged) st_code = KS_OK;
+  else if (done == kBreakdown) st_code = KS_BREAKDOWN;
+  else if (done == kNaN) st_code = KS_NAN_DETECTED;
+  long long loop = hs[1];
+  // reported "loop =" values (cg.cpp:246, gmres.cpp:427, kskipcg.cpp:314, kskipbicg.cpp:356)
+  const int kk = outer_sp.kskip;
+  if (outer == KS_GMRES || outer == KS_VPGMRES) {
+    loop = loop + 1;
+  } else if (outer == KS_KSKIPCG || outer == KS_KSKIPBICG) {
+    long long nl = loop;
+    if (done != kConverged) {  // ran out: nloop is the first multiple of k+1 >= maxloop
+      nl = ((outer_sp.maxloop + kk) / (kk + 1)) * (kk + 1);
+      if (outer_sp.maxloop <= 0) nl = 0;
+    }
+    loop = (outer == KS_KSKIPCG) ? nl - kk + 1 : nl + 1;
+  } else if (outer == KS_GCR || outer == KS_VPGCR) {
+    // loop as the device left it
+  } else if (done == kMaxLoop || done == kRunning) {
+    loop = outer_sp.maxloop + 1;
+  }
+  const long long hlen = hs[2];
+  if (hist_err && hist_cap > 0) {
+    const long long cnt = std::min<long long>(std::min<long long>(hlen, hcap), hist_cap);
+    if (cnt > 0) {
+      KS_CUDA(ctx, cudaMemcpy(hist_err, d_hist, sizeof(double) * cnt, cudaMemcpyDeviceToHost));
+      if (hist_iter) KS_CUDA(ctx, cudaMemcpy(hist_iter, d_hit, sizeof(long long) * cnt, cudaMemcpyDeviceToHost));
+    }
+  }
+  if (rep) {
+    rep->status = st_code;
+    rep->loop = loop;
+    rep->hist_len = hlen;
+    rep->final_rel_res = 0.0;
+    if (hlen > 0 && hlen <= hcap) {
+      double last = 0.0;
+      KS_CUDA(ctx, cudaMemcpy(&last, d_hist + hlen - 1, sizeof(double), cudaMemcpyDeviceToHost));
+      rep->final_rel_res = last;
+    }
+    rep->solve_seconds = ms * 1e-3;
+    rep->inner_iterations = vp ? IR.calls : 0;
+    rep->spmv_count = 0;
+    rep->true_res_log10 = 0.0;
+    rep->true_rel_res = 0.0;
+  }
+  return st_code;
+}
+
+extern "C" {
+
+void ks_params_default(ks_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->outer_maxloop = 10000;
+  p->outer_eps = 1e-8;
+  p->outer_restart = 1000;
+  p->outer_kskip = 2;
+  p->outer_fix = 2;
+  p->inner_maxloop = 50;
+  p->inner_eps = 1e-1;
+  p->inner_restart = 1000;
+  p->inner_kskip = 2;
+  p->inner_fix = 2;
+  p->inner_precision = KS_FP64;
+  p->reference_defects = 0;
+  p->transpose = 0;
+  p->poll_interval = 0;
+}
+
+ks_status ks_solve(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                   const ks_params *params, const ks_vec *b, ks_vec *x, int64_t *hist_iter,
+                   double *hist_err, int64_t hist_cap, ks_report *report) {
+  if (!ctx || !mat || !b || !x || mat->ctx != ctx || b->ctx != ctx || x->ctx != ctx) return KS_BAD_INPUT;
+  if (b->type != KS_FP64 || x->type != KS_FP64 || b->n != mat->A.n || x->n != mat->A.n)
+    return set_error(ctx, KS_BAD_INPUT, "ks_solve: b and x must be FP64 vectors of length n");
+  ks_params def;
+  if (!params) {
+    ks_params_default(&def);
+    params = &def;
+  }
+  ks_status s = solve_impl(ctx, mat, outer, inner, params, (const double *)b->d, (double *)x->d, hist_iter,
+                           hist_err, hist_cap, report);
+  if (report && (s == KS_OK || s == KS_NOT_CONVERGED || s == KS_BREAKDOWN || s == KS_NAN_DETECTED)) {
+    double lg = 0, rel = 0;
+    const ks_mat *m = mat;
+    if (params->transpose) {
+      // residual of A^T x = b
+      launch_spmv<double, double>(ctx, m->T, (const double *)x->d,
+                                  ResidEpi<double>{(const double *)b->d, nullptr, ctx->d_result},
+                                  Stop{nullptr, nullptr});
+      double sc[2];
+      KS_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_result, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+      KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      rel = std::sqrt(ctx->h_pinned[0]) / std::sqrt(ctx->h_pinned[1]);
+      lg = std::log10(rel);
+    } else {
+      ks_status c = ks_check_error(m, b, x, &lg, &rel);
+      if (c != KS_OK) return c;
+    }
+    report->true_res_log10 = lg;
+    report->true_rel_res = rel;
+  }
+  return s;
+}
+
+ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                        const ks_params *params, const double *b, double *x, int64_t *hist_iter,
+                        double *hist_err, int64_t hist_cap, ks_report *report) {
+  if (!ctx || !mat || !b || !x) return KS_BAD_INPUT;
+  ks_vec *vb = nullptr, *vx = nullptr;
+  KS_TRY(ks_vec_create(ctx, mat->A.n, KS_FP64, &vb));
+  ks_status s = ks_vec_create(ctx, mat->A.n, KS_FP64, &vx);
+  if (s == KS_OK) s = ks_vec_upload(vb, b);
+  ks_status r = s;
+  if (s == KS_OK) {
+    r = ks_solve(ctx, mat, outer, inner, params, vb, vx, hist_iter, hist_err, hist_cap, report);
+    if (r == KS_OK || r == KS_NOT_CONVERGED || r == KS_BREAKDOWN || r == KS_NAN_DETECTED) {
+      ks_status d = ks_vec_download(vx, x);
+      if (d != KS_OK) r = d;
+    }
+  }
+  ks_vec_destroy(vb);
+  ks_vec_destroy(vx);
+  return r;
+}
+
+ks_status ks_adjoint_grad(ks_ctx *ctx, const ks_mat *mat, ks_solver solver, ks_solver inner,
+                          const ks_params *params, const ks_vec *x, const ks_vec *g, ks_vec *grad_b,
+                          ks_vec *grad_val, ks_report *report) {
+  if (!ctx || !mat || !x || !g || x->type != KS_FP64 || g->type != KS_FP64) return KS_BAD_INPUT;
+  ks_params p;
+  if (params) p = *params;
+  else ks_params_default(&p);
+  p.transpose = 1;
+  ks_vec *lam = grad_b;
+  ks_vec *own = nullptr;
+  if (!lam) {
+    KS_TRY(ks_vec_create(ctx, mat->A.n, KS_FP64, &own));
+    lam = own;
+  }
+  ks_status s = ks_solve(ctx, mat, solver, inner, &p, g, lam, nullptr, nullptr, 0, report);
+  if ((s == KS_OK || s == KS_NOT_CONVERGED) && grad_val) {
+    ks_status q = ks_pattern_grad(mat, lam, x, grad_val);
+    if (q != KS_OK) s = q;
+  }
+  if (own) ks_vec_destroy(own);
+  return s;
+}
+
+}  // extern "C"

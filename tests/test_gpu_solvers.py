@@ -1,0 +1,123 @@
+"""GPU: every Krylov method reproduces the reference's own run.
+
+Against the golden fixtures (the reference's CPU path, -t 1): the residual
+history to 1e-8 relative per iteration, the iteration count within +-1 %
+(at least +-1), the same verdict and the same printed true residual. The GPU
+sums its dot products in a different (fixed) order than the host loop, so the
+histories are not bitwise equal; SpMV and every element-wise update are.
+Methods with reference defects are run with reference_defects=1 here; the
+corrected forms are checked against the corrected oracle below.
+"""
+import numpy as np
+import pytest
+
+from golden_cases import index, load, rel_close
+from solver_cpp_b200.matrices import config_problem
+
+pytestmark = pytest.mark.gpu
+
+HIST_RTOL = 1e-8
+DIVERGING = {"p2_kskipcg", "p2_vpcr_cg", "p2_vpcg_kskipcg", "p2_vpcg_gmres", "cd2_vpgmres_gmres"}
+
+
+def _mat(ctx, A):
+    return ctx.matrix(A, transpose=True, fp32=True, bf16=True)
+
+
+@pytest.mark.parametrize("cid", sorted(index().keys()))
+def test_history_matches_reference(ks, ctx, cid):
+    meta, g = load(cid)
+    A, b, _ = config_problem(meta["problem"], meta["grid"])
+    M = _mat(ctx, A)
+    r = ks.solve(ctx, M, meta["outer"], b, inner=meta["inner"], reference_defects=1, **meta["params"])
+    ref_err, ref_it = g["hist_err"], g["hist_iter"]
+    if cid in DIVERGING:
+        m = min(8, len(ref_err))
+        assert np.array_equal(r.hist_iter[:m], ref_it[:m])
+        assert np.all(rel_close(r.hist_err[:m], ref_err[:m], 1e-6))
+        assert r.converged == meta["converged"]
+        return
+    assert r.converged == meta["converged"]
+    tol = max(1, int(0.01 * meta["loop"]))
+    assert abs(r.loop - meta["loop"]) <= tol
+    m = min(len(ref_err), len(r.hist_err))
+    assert m >= len(ref_err) - tol
+    assert np.array_equal(r.hist_iter[:m], ref_it[:m])
+    bad = ~rel_close(r.hist_err[:m], ref_err[:m], HIST_RTOL)
+    assert not bad.any(), f"first deviating entry {np.argmax(bad)} of {m}"
+    assert round(r.true_res_log10, 1) == pytest.approx(meta["true_res_log10"], abs=0.11)
+
+
+@pytest.mark.parametrize("k", [1, 2, 4])
+def test_corrected_kskipcg_matches_corrected_oracle(ks, ctx, oracle, k):
+    A, b, _ = config_problem("poisson3d", 16)
+    M = _mat(ctx, A)
+    r = ks.solve(ctx, M, "KSKIPCG", b, E=1e-10, K=k)
+    o = oracle.solve(A, b, "KSKIPCG", E=1e-10, K=k, fix_kskipcg=1)
+    assert r.converged and o["status"] == 0
+    assert r.loop == o["loop"]
+    np.testing.assert_allclose(r.hist_err, o["hist_err"], rtol=1e-8)
+    assert r.true_res_log10 < -9.5
+
+
+@pytest.mark.parametrize("outer,inner", [("GMRES", "NONE"), ("VPGMRES", "CG")])
+def test_corrected_gmres_assembly(ks, ctx, oracle, outer, inner):
+    A, b, _ = config_problem("convdiff2d", 32)
+    M = _mat(ctx, A)
+    kw = dict(E=1e-10, R=30, l=10, e=0.1)
+    r = ks.solve(ctx, M, outer, b, inner=inner, **kw)
+    o = oracle.solve(A, b, outer, inner, fix_gmres_assembly=1, **kw)
+    assert r.converged == (o["status"] == 0)
+    assert abs(r.loop - o["loop"]) <= 1
+    np.testing.assert_allclose(r.hist_err[:len(o["hist_err"]) - 1], o["hist_err"][:-1], rtol=1e-8)
+    if r.converged:
+        assert r.true_res_log10 < -9.5
+
+
+def test_not_implemented_methods(ks, ctx):
+    A, b, _ = config_problem("poisson2d", 8)
+    M = _mat(ctx, A)
+    for name in ("KSKIPCR", "VPBICG"):
+        with pytest.raises(ks.KrylovError) as e:
+            ks.solve(ctx, M, name, b, inner="CG")
+        assert e.value.status == 99
+
+
+def test_maxloop_and_loop_reporting(ks, ctx, oracle):
+    A, b, _ = config_problem("poisson2d", 32)
+    M = _mat(ctx, A)
+    for name, kw in (("CG", {}), ("CR", {}), ("BICG", {}), ("GCR", {"R": 5}), ("GMRES", {"R": 5}),
+                     ("KSKIPBICG", {"K": 2})):
+        r = ks.solve(ctx, M, name, b, L=7, E=1e-14, **kw)
+        o = oracle.solve(A, b, name, L=7, E=1e-14, **kw)
+        assert r.status == 2 and o["status"] == 2
+        assert r.loop == o["loop"], name
+        assert np.array_equal(r.hist_iter, o["hist_iter"]), name
+
+
+def test_breakdown_and_nan_paths(ks, ctx):
+    """b = 0: |b| = 0 gives a NaN residual ratio; the reference loops to maxloop
+    on NaNs, the library stops at once with KS_NAN_DETECTED."""
+    A, _, _ = config_problem("poisson2d", 8)
+    M = _mat(ctx, A)
+    r = ks.solve(ctx, M, "CG", np.zeros(A.n), L=50)
+    assert r.status == 4
+    assert r.loop <= 2
+
+
+def test_repeat_solves_are_deterministic(ks, ctx):
+    A, b, _ = config_problem("convdiff3d", 14)
+    M = _mat(ctx, A)
+    r1 = ks.solve(ctx, M, "BICG", b, E=1e-10)
+    r2 = ks.solve(ctx, M, "BICG", b, E=1e-10)
+    assert np.array_equal(r1.hist_err, r2.hist_err) and np.array_equal(r1.x, r2.x)
+
+
+def test_device_vectors_path(ks, ctx):
+    A, b, _ = config_problem("poisson3d", 12)
+    M = _mat(ctx, A)
+    B = ctx.vector(b)
+    X = ctx.vector(n=A.n)
+    r = ks.solve(ctx, M, "CG", B, x=X, E=1e-10)
+    h = ks.solve(ctx, M, "CG", b, E=1e-10)
+    assert r.converged and np.array_equal(X.numpy(), h.x)
