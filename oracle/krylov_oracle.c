@@ -35,8 +35,37 @@ void oracle_spmv_t(const or_mat *A, const double *x, double *y) {
   csr_mv(A->n, A->tptr, A->tcol, A->tval, x, y);
 }
 
-/* blas::dot (blas.cpp:149-162). */
+/* Number of partial sums of dot/norm_2 for the solve in progress (see
+ * or_params.sum_chunks). The oracle is single-threaded test code. */
+static int g_sum_chunks = 1;
+
+/* blas::dot (blas.cpp:149-162). With g_sum_chunks = T > 1 the index range is
+ * split as OpenMP schedule(static) splits it over T threads (the first n % T
+ * threads take one extra element), each part summed from 0.0 in order and
+ * the parts added in thread order. */
 double oracle_dot(long n, const double *x, const double *y) {
+  if (g_sum_chunks <= 1) {
+    double t = 0.0;
+    for (long i = 0; i < n; i++) t += x[i] * y[i];
+    return t;
+  }
+  const long T = g_sum_chunks, q = n / T, rem = n % T;
+  double total = 0.0;
+  long s = 0;
+  for (long c = 0; c < T; c++) {
+    const long len = q + (c < rem ? 1 : 0);
+    double t = 0.0;
+    for (long i = s; i < s + len; i++) t += x[i] * y[i];
+    total += t;
+    s += len;
+  }
+  return total;
+}
+
+/* A dot product the reference always sums sequentially: the ones inside
+ * Gcr_sp_1's parallel loop (blas.cpp:529-535) run as nested, one-thread
+ * regions. */
+static double seq_dot(long n, const double *x, const double *y) {
   double t = 0.0;
   for (long i = 0; i < n; i++) t += x[i] * y[i];
   return t;
@@ -44,9 +73,7 @@ double oracle_dot(long n, const double *x, const double *y) {
 
 /* blas::norm_2 (blas.cpp:31-41). */
 double oracle_norm2(long n, const double *x) {
-  double t = 0.0;
-  for (long i = 0; i < n; i++) t += x[i] * x[i];
-  return sqrt(t);
+  return sqrt(oracle_dot(n, x, x));
 }
 
 /* Scalar_axy (blas.cpp:226-233): out = (a*x) + y. */
@@ -432,7 +459,7 @@ static res_t solve_gcr(ctx_t *c, const double *b, double *x, int inner,
       memset(pk1, 0, sizeof(double) * (size_t)n);
       memset(qk1, 0, sizeof(double) * (size_t)n);
       for (long i = 0; i <= k; i++)
-        beta[i] = -(oracle_dot(n, Av, Q + i * n)) / qq[i];
+        beta[i] = -(seq_dot(n, Av, Q + i * n)) / qq[i];
       for (long i = 0; i <= k; i++) {
         axy(n, beta[i], P + i * n, pk1, pk1);
         axy(n, beta[i], Q + i * n, qk1, qk1);
@@ -885,7 +912,7 @@ static res_t solve_vpgcr(ctx_t *c, const double *b, double *x, hist_t *h) {
       memset(pk1, 0, sizeof(double) * (size_t)n);
       memset(qk1, 0, sizeof(double) * (size_t)n);
       for (long i = 0; i <= k; i++)
-        beta[i] = -(oracle_dot(n, Av, Q + i * n)) / qq[i];
+        beta[i] = -(seq_dot(n, Av, Q + i * n)) / qq[i];
       for (long i = 0; i <= k; i++) {
         axy(n, beta[i], P + i * n, pk1, pk1);
         axy(n, beta[i], Q + i * n, qk1, qk1);
@@ -926,6 +953,7 @@ void oracle_default_params(or_params *p) {
   p->inner_fix = 2;
   p->fix_kskipcg = 0;
   p->fix_gmres_assembly = 0;
+  p->sum_chunks = 1;
 }
 
 /* outerMethods::outerSelect (outerMethods.cpp:20-82). */
@@ -933,6 +961,7 @@ int oracle_solve(const or_mat *A, const or_params *p, const double *b,
                  double *x, long *hist_iter, double *hist_err, long hist_cap,
                  or_report *rep) {
   ctx_t c = {A, p, 0, p->inner != OR_NONE};
+  g_sum_chunks = p->sum_chunks > 1 ? p->sum_chunks : 1;
   hist_t h = {hist_iter, hist_err, hist_iter && hist_err ? hist_cap : 0, 0};
   res_t res = {99, 0};
   long n = A->n;
@@ -962,5 +991,6 @@ int oracle_solve(const or_mat *A, const or_params *p, const double *b,
       free(x0);
     }
   }
+  g_sum_chunks = 1;
   return res.status;
 }

@@ -52,6 +52,10 @@ typedef struct {
   int inner_fix;          /* -f */
   int fix_kskipcg;        /* 1: corrected recurrences */
   int fix_gmres_assembly; /* 1: accumulate the correction */
+  int sum_chunks;         /* >1: dot products and norms summed as that many
+                             contiguous partial sums added in order, the way
+                             an OpenMP static reduction with that many
+                             threads does; 0/1: one sequential sum (-t 1) */
 } or_params;
 
 typedef struct {

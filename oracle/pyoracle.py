@@ -46,7 +46,7 @@ class _Params(C.Structure):
         ("outer_kskip", C.c_int), ("outer_fix", C.c_int),
         ("inner_maxloop", C.c_long), ("inner_eps", C.c_double), ("inner_restart", C.c_long),
         ("inner_kskip", C.c_int), ("inner_fix", C.c_int),
-        ("fix_kskipcg", C.c_int), ("fix_gmres_assembly", C.c_int),
+        ("fix_kskipcg", C.c_int), ("fix_gmres_assembly", C.c_int), ("sum_chunks", C.c_int),
     ]
 
 

@@ -73,6 +73,9 @@ CASES = [
 ]
 
 
+THREADS = (2, 3, 4, 8)
+
+
 def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
@@ -106,15 +109,34 @@ def main():
         if res["returncode"] != 0:
             raise SystemExit(f"{cid}: reference failed\n{res['stderr']}")
         outer, inner, kw = flags_to_params(args)
+        # The reference's own sensitivity to summation order: rerun it with
+        # more OpenMP threads (its dot products and norms then add partial
+        # sums) and record, per history entry, the largest relative departure
+        # from the -t 1 run, plus the spread of iteration counts.
+        h1 = res["hist_err"]
+        env = np.zeros_like(h1)
+        loops = [res["loop"]]
+        verdicts = [bool(res["converged"])]
+        for t in THREADS:
+            rt = pyoracle.run_reference(A, b, args, threads=t, keep_x=False)
+            loops.append(rt["loop"])
+            verdicts.append(bool(rt["converged"]))
+            m = min(len(h1), len(rt["hist_err"]))
+            dev = np.abs(rt["hist_err"][:m] - h1[:m]) / np.maximum(np.abs(h1[:m]), 1e-300)
+            env[:m] = np.maximum(env[:m], dev)
+            if m < len(h1):  # a shorter run departs completely beyond its end
+                env[m:] = np.inf
         np.savez_compressed(
             os.path.join(HERE, f"{cid}.npz"),
-            hist_iter=res["hist_iter"], hist_err=res["hist_err"], x=res.get("x", np.zeros(0)),
+            hist_iter=res["hist_iter"], hist_err=h1, x=res.get("x", np.zeros(0)), envelope=env,
         )
         index[cid] = {
             "problem": prob, "grid": grid, "args": args, "outer": outer, "inner": inner, "params": kw,
             "loop": res["loop"], "converged": bool(res["converged"]),
             "true_res_log10": res["true_res_log10"], "n": A.n, "nnz": A.nnz,
             "sha_val": digest(A.val), "sha_b": digest(b),
+            "threads_checked": [1] + list(THREADS), "loop_range": [min(loops), max(loops)],
+            "verdicts_agree": len(set(verdicts)) == 1,
         }
         print(f"{cid:22s} loop={res['loop']:6d} conv={res['converged']!s:5s} "
               f"true={res['true_res_log10']} hist={len(res['hist_err'])}")

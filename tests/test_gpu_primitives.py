@@ -168,5 +168,6 @@ def test_check_error_matches_reference(ks, ctx, oracle):
     P = oracle.Problem(A)
     import ctypes as C
 
-    ref = oracle.lib().oracle_check_error(C.byref(P.mat), b.ctypes.data, x.ctypes.data, np.zeros(A.n).ctypes.data)
+    x0 = np.zeros(A.n)
+    ref = oracle.lib().oracle_check_error(C.byref(P.mat), b.ctypes.data, x.ctypes.data, x0.ctypes.data)
     assert lg == pytest.approx(ref, rel=1e-13)

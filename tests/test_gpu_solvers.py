@@ -1,23 +1,22 @@
 """GPU: every Krylov method reproduces the reference's own run.
 
 Against the golden fixtures (the reference's CPU path, -t 1): the residual
-history to 1e-8 relative per iteration, the iteration count within +-1 %
-(at least +-1), the same verdict and the same printed true residual. The GPU
-sums its dot products in a different (fixed) order than the host loop, so the
-histories are not bitwise equal; SpMV and every element-wise update are.
-Methods with reference defects are run with reference_defects=1 here; the
-corrected forms are checked against the corrected oracle below.
+history to 1e-8 relative per entry up to the point where the reference
+departs from itself under a change of OpenMP thread count, within 10x that
+self-departure afterwards, the iteration count within the reference's own
+spread +-1 %, the same verdict and the same printed true residual
+(golden_cases.check_history). SpMV and every element-wise update match the
+reference bit for bit; only the order of the terms of each dot product
+differs. Methods with reference defects run with reference_defects=1 here;
+the corrected forms are checked against the corrected oracle below.
 """
 import numpy as np
 import pytest
 
-from golden_cases import index, load, rel_close
+from golden_cases import check_history, index, load, oracle_envelope
 from solver_cpp_b200.matrices import config_problem
 
 pytestmark = pytest.mark.gpu
-
-HIST_RTOL = 1e-8
-DIVERGING = {"p2_kskipcg", "p2_vpcr_cg", "p2_vpcg_kskipcg", "p2_vpcg_gmres", "cd2_vpgmres_gmres"}
 
 
 def _mat(ctx, A):
@@ -30,22 +29,11 @@ def test_history_matches_reference(ks, ctx, cid):
     A, b, _ = config_problem(meta["problem"], meta["grid"])
     M = _mat(ctx, A)
     r = ks.solve(ctx, M, meta["outer"], b, inner=meta["inner"], reference_defects=1, **meta["params"])
-    ref_err, ref_it = g["hist_err"], g["hist_iter"]
-    if cid in DIVERGING:
-        m = min(8, len(ref_err))
-        assert np.array_equal(r.hist_iter[:m], ref_it[:m])
-        assert np.all(rel_close(r.hist_err[:m], ref_err[:m], 1e-6))
-        assert r.converged == meta["converged"]
-        return
     assert r.converged == meta["converged"]
-    tol = max(1, int(0.01 * meta["loop"]))
-    assert abs(r.loop - meta["loop"]) <= tol
-    m = min(len(ref_err), len(r.hist_err))
-    assert m >= len(ref_err) - tol
-    assert np.array_equal(r.hist_iter[:m], ref_it[:m])
-    bad = ~rel_close(r.hist_err[:m], ref_err[:m], HIST_RTOL)
-    assert not bad.any(), f"first deviating entry {np.argmax(bad)} of {m}"
-    assert round(r.true_res_log10, 1) == pytest.approx(meta["true_res_log10"], abs=0.11)
+    check_history(r.hist_iter, r.hist_err, g["hist_iter"], g["hist_err"], g["envelope"], r.loop, meta["loop"],
+                  meta["loop_range"])
+    if meta["converged"] or meta["true_res_log10"] < 0:
+        assert round(r.true_res_log10, 1) == pytest.approx(meta["true_res_log10"], abs=0.21)
 
 
 @pytest.mark.parametrize("k", [1, 2, 4])
@@ -53,10 +41,9 @@ def test_corrected_kskipcg_matches_corrected_oracle(ks, ctx, oracle, k):
     A, b, _ = config_problem("poisson3d", 16)
     M = _mat(ctx, A)
     r = ks.solve(ctx, M, "KSKIPCG", b, E=1e-10, K=k)
-    o = oracle.solve(A, b, "KSKIPCG", E=1e-10, K=k, fix_kskipcg=1)
+    o, env, lr = oracle_envelope(oracle, A, b, "KSKIPCG", E=1e-10, K=k, fix_kskipcg=1)
     assert r.converged and o["status"] == 0
-    assert r.loop == o["loop"]
-    np.testing.assert_allclose(r.hist_err, o["hist_err"], rtol=1e-8)
+    check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
     assert r.true_res_log10 < -9.5
 
 
@@ -66,10 +53,9 @@ def test_corrected_gmres_assembly(ks, ctx, oracle, outer, inner):
     M = _mat(ctx, A)
     kw = dict(E=1e-10, R=30, l=10, e=0.1)
     r = ks.solve(ctx, M, outer, b, inner=inner, **kw)
-    o = oracle.solve(A, b, outer, inner, fix_gmres_assembly=1, **kw)
+    o, env, lr = oracle_envelope(oracle, A, b, outer, inner, fix_gmres_assembly=1, **kw)
     assert r.converged == (o["status"] == 0)
-    assert abs(r.loop - o["loop"]) <= 1
-    np.testing.assert_allclose(r.hist_err[:len(o["hist_err"]) - 1], o["hist_err"][:-1], rtol=1e-8)
+    check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
     if r.converged:
         assert r.true_res_log10 < -9.5
 

@@ -39,6 +39,20 @@ def test_oracle_matches_reference_golden(oracle, cid):
         assert np.all(np.abs(r["x"] - g["x"]) <= PRINT_RTOL * np.abs(g["x"]) + 1e-300)
 
 
+@pytest.mark.parametrize("cid", ["cd2_bicg", "cd2_gmres", "vc3_cg", "vc3_vpcg_cg", "cd3_kskipbicg"])
+def test_parity_criterion_accepts_a_reordered_sum(oracle, cid):
+    """The history criterion used for the GPU accepts the oracle run with its
+    dot products summed in 3 or 5 parts (another legitimate summation order)."""
+    from golden_cases import check_history
+
+    meta, g = load(cid)
+    A, b, _ = config_problem(meta["problem"], meta["grid"])
+    for chunks in (3, 5):
+        r = oracle.solve(A, b, meta["outer"], meta["inner"], sum_chunks=chunks, **meta["params"])
+        check_history(r["hist_iter"], r["hist_err"], g["hist_iter"], g["hist_err"], g["envelope"], r["loop"],
+                      meta["loop"], meta["loop_range"])
+
+
 def test_c1_configuration(oracle):
     """CG on the 64x64 Poisson problem, tol 1e-10, 202 iterations."""
     meta, g = load("c1_cg")
