@@ -72,6 +72,7 @@ struct CsrDev {
   float *val32 = nullptr;
   __nv_bfloat16 *val16 = nullptr;
   int *rb = nullptr;  // row-block boundaries, nrb + 1 entries
+  int4 *rbi = nullptr;  // per row block: first row, end row, first nonzero, end nonzero
   int nrb = 0;
 };
 
@@ -235,6 +236,7 @@ struct ks_ctx {
   size_t partials_len = 0;
   unsigned *counters = nullptr; // last-CTA-done counters
   int ncounters = 0;
+  int *d_err = nullptr;         // set by a kernel whose bounded wait ran out
   double *d_result = nullptr;   // device staging for scalar results
   size_t d_result_len = 0;
   double *h_pinned = nullptr;   // pinned host staging (scalars)
@@ -289,7 +291,8 @@ ks_status cuda_fail(ks_ctx *ctx, cudaError_t e, const char *what);
 
 // Scratch sizing.
 int red_grid(const ks_ctx *ctx);  // CTAs of the vector kernels
-int spmv_grid(const ks_ctx *ctx, const CsrDev &A);
+// Reads and clears the context's timeout flag (synchronises the stream).
+ks_status check_device_error(ks_ctx *ctx);
 
 // Workspace pool (device buffers reused across solves).
 ks_status pool_get(ks_ctx *ctx, size_t bytes, void **out);

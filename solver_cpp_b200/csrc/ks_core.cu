@@ -23,9 +23,15 @@ ks_status cuda_fail(ks_ctx *ctx, cudaError_t e, const char *what) {
 
 int red_grid(const ks_ctx *ctx) { return ctx->num_sms * 4; }
 
-int spmv_grid(const ks_ctx *ctx, const CsrDev &A) {
-  int g = ctx->num_sms * 8;
-  return std::max(1, std::min(g, A.nrb));
+ks_status check_device_error(ks_ctx *ctx) {
+  int flag = 0;
+  KS_CUDA(ctx, cudaMemcpyAsync(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (flag) {
+    KS_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    return set_error(ctx, KS_TIMEOUT, "a bounded wait on a shared-memory staging barrier ran out");
+  }
+  return KS_OK;
 }
 
 ks_status pool_get(ks_ctx *ctx, size_t bytes, void **out) {
@@ -204,13 +210,17 @@ static void free_csr(CsrDev &A) {
   cudaFree(A.val32);
   cudaFree(A.val16);
   cudaFree(A.rb);
+  cudaFree(A.rbi);
   A = CsrDev();
 }
 
+// col/val carry kPad tail elements and ptr kPad tail entries (zeroed) so the
+// 16-byte-granular bulk copies of a row block's arrays stay inside them.
 static ks_status alloc_csr(ks_ctx *ctx, CsrDev &A, int n, long long nnz) {
   A.n = n;
   A.nnz = nnz;
-  KS_CUDA(ctx, cudaMalloc(&A.ptr, sizeof(int) * (size_t)(n + 1)));
+  KS_CUDA(ctx, cudaMalloc(&A.ptr, sizeof(int) * (size_t)(n + 1 + kPad)));
+  KS_CUDA(ctx, cudaMemsetAsync(A.ptr + n + 1, 0, sizeof(int) * kPad, ctx->stream));
   KS_CUDA(ctx, cudaMalloc(&A.col, sizeof(int) * (size_t)(nnz + kPad)));
   KS_CUDA(ctx, cudaMalloc(&A.val, sizeof(double) * (size_t)(nnz + kPad)));
   KS_CUDA(ctx, cudaMemsetAsync(A.col + nnz, 0, sizeof(int) * kPad, ctx->stream));
@@ -224,6 +234,11 @@ static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, uns
   KS_CUDA(ctx, cudaMalloc(&A.rb, sizeof(int) * rb.size()));
   KS_CUDA(ctx, cudaMemcpyAsync(A.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice,
                                ctx->stream));
+  std::vector<int4> rbi((size_t)A.nrb);
+  for (int b = 0; b < A.nrb; b++) rbi[b] = make_int4(rb[b], rb[b + 1], host_ptr[rb[b]], host_ptr[rb[b + 1]]);
+  KS_CUDA(ctx, cudaMalloc(&A.rbi, sizeof(int4) * std::max<size_t>(rbi.size(), 1)));
+  KS_CUDA(ctx, cudaMemcpyAsync(A.rbi, rbi.data(), sizeof(int4) * rbi.size(), cudaMemcpyHostToDevice,
+                               ctx->stream));
   const long long tot = A.nnz + kPad;
   const int g = ctx->num_sms * 8;
   if (flags & KS_MAT_FP32) {
@@ -235,7 +250,7 @@ static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, uns
     k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.val, A.val16, tot);
   }
   KS_CUDA(ctx, cudaGetLastError());
-  // rb is a host vector going out of scope: the copy must complete first.
+  // rb and rbi are host vectors going out of scope: the copies must complete first.
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return KS_OK;
 }
@@ -360,6 +375,8 @@ ks_status ks_ctx_create(int device, ks_ctx **out) {
     return fail(KS_OUT_OF_MEMORY);
   if (cudaMemset(ctx->counters, 0, sizeof(unsigned) * ctx->ncounters) != cudaSuccess)
     return fail(KS_CUDA_ERROR);
+  if (cudaMalloc(&ctx->d_err, sizeof(int)) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
+  if (cudaMemset(ctx->d_err, 0, sizeof(int)) != cudaSuccess) return fail(KS_CUDA_ERROR);
   ctx->d_result_len = 4096;
   if (cudaMalloc(&ctx->d_result, sizeof(double) * ctx->d_result_len) != cudaSuccess)
     return fail(KS_OUT_OF_MEMORY);
@@ -392,6 +409,7 @@ ks_status ks_ctx_destroy(ks_ctx *ctx) {
   cudaFree(ctx->partials);
   cudaFree(ctx->counters);
   cudaFree(ctx->d_result);
+  cudaFree(ctx->d_err);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
   if (ctx->flag_events) {

@@ -1,168 +1,41 @@
-// Kernel templates: row-blocked CSR SpMV with fused epilogues, and fused
-// vector (BLAS-1) passes with deterministic single-pass grid reductions.
+// Kernel templates and launchers: the TMA-staged CSR SpMV with fused
+// epilogues (ks_spmv_tma.cuh), fused vector (BLAS-1) passes with
+// deterministic single-pass grid reductions, and single-thread scalar steps.
 #pragma once
 
+#include <atomic>
+#include <type_traits>
+
 #include "ks_common.cuh"
+#include "ks_spmv_tma.cuh"
 
 namespace ks {
 
-// One SpMV row block (CSR-Adaptive style binning, chosen per block):
-//  * "stream" blocks hold up to kRowsPerBlock rows and kNnzPerBlock nonzeros.
-//    The CTA streams the block's col/val with 128-bit loads (int4 columns,
-//    double2/float4 values), gathers x, and parks the products in shared
-//    memory. Rows of up to 16 nonzeros on average are then summed one thread
-//    per row, in index order from 0.0, exactly as blas::MtxVec_mult
-//    (blas.cpp:56-62) does -- the FP64 result equals the reference's bit for
-//    bit. Denser blocks sum one warp per row.
-//  * "long" blocks hold a single row with more than kNnzPerBlock nonzeros,
-//    reduced by the whole CTA.
-// NV right-hand vectors share one pass over the block's col/val (NV = 2 for
-// the k-skip matrix powers). On return rowsum[v*kRowsPerBlock + t] holds row
-// r0+t of product v, visible to all threads.
-template <int NV, class MT, class XT, class AT>
-__device__ __forceinline__ void spmv_block(const CsrK<MT> &A, int blk,
-                                           const XT *const *x,
-                                           AT *__restrict__ rowsum,
-                                           AT *__restrict__ prod, int &r0_out,
-                                           int &nrows_out) {
-  const int r0 = A.rb[blk], r1 = A.rb[blk + 1];
-  const int nrows = r1 - r0;
-  const int j0 = A.ptr[r0], j1 = A.ptr[r1];
-  const int t = threadIdx.x;
-  int rs = 0, re = 0;
-  if (t < nrows) {
-    rs = A.ptr[r0 + t];
-    re = A.ptr[r0 + t + 1];
-  }
-  const int nnz = j1 - j0;
-  r0_out = r0;
-  nrows_out = nrows;
-  if (nnz <= kNnzPerBlock) {
-    const int a0 = j0 & ~(kChunk - 1);
-    const int nch = (j1 - a0 + kChunk - 1) / kChunk;
-    for (int c = t; c < nch; c += kThreads) {
-      const int j = a0 + c * kChunk;
-      const int4 cc = ld_stream(reinterpret_cast<const int4 *>(A.col + j));
-      MT v[4];
-      ld_vals4(A.val + j, v);
-      const int cols[4] = {cc.x, cc.y, cc.z, cc.w};
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int jj = j + q;
-        if (jj >= j0 && jj < j1) {
-#pragma unroll
-          for (int u = 0; u < NV; u++)
-            prod[u * kNnzPerBlock + jj - j0] =
-                mul_rn(mval<AT>(v[q]), (AT)__ldg(x[u] + cols[q]));
-        }
-      }
-    }
-    __syncthreads();
-    if (nnz <= 16 * nrows) {
-      if (t < nrows) {
-#pragma unroll
-        for (int u = 0; u < NV; u++) {
-          const AT *pp = prod + u * kNnzPerBlock;
-          AT s = (AT)0;
-          for (int e = rs - j0; e < re - j0; e++) s = add_rn(s, pp[e]);
-          rowsum[u * kRowsPerBlock + t] = s;
-        }
-      }
-    } else {
-      const int lane = t & 31, w = t >> 5;
-      for (int rr = w; rr < nrows; rr += kThreads / 32) {
-        const int a = A.ptr[r0 + rr] - j0, b = A.ptr[r0 + rr + 1] - j0;
-#pragma unroll
-        for (int u = 0; u < NV; u++) {
-          const AT *pp = prod + u * kNnzPerBlock;
-          AT s = (AT)0;
-          for (int e = a + lane; e < b; e += 32) s += pp[e];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-          if (lane == 0) rowsum[u * kRowsPerBlock + rr] = s;
-        }
-      }
-    }
-    __syncthreads();
-  } else {
-    // A single long row: the CTA strides over it.
-    double v[NV];
-#pragma unroll
-    for (int u = 0; u < NV; u++) {
-      AT s = (AT)0;
-      for (int j = j0 + t; j < j1; j += kThreads)
-        s += mval<AT>(A.val[j]) * (AT)__ldg(x[u] + A.col[j]);
-      v[u] = (double)s;
-    }
-    block_sum<NV>(v);
-    if (t == 0) {
-#pragma unroll
-      for (int u = 0; u < NV; u++) rowsum[u * kRowsPerBlock] = (AT)v[u];
-    }
-    __syncthreads();
-  }
-}
-
-// Epilogue concept for spmv_kernel:
+// SpMV epilogue concept (see spmv_tma_kernel):
 //   using acc_t = double|float;   // row-sum type
 //   static constexpr int ND;      // number of fused reductions (0..kMaxDots)
-//   __device__ void row(int r, acc_t y, double (&acc)[ND?ND:1]) const;
+//   __device__ void row(int r, acc_t y, double (&acc)[ND?ND:1]) const;        (one vector)
+//   __device__ void row(int r, acc_t y0, acc_t y1, double (&acc)[...]) const; (two vectors)
 //   __device__ void finish(const double (&sums)[ND?ND:1]) const;  // thread 0 of last CTA
-template <class MT, class XT, class Epi>
-__global__ void __launch_bounds__(kThreads)
-    spmv_kernel(CsrK<MT> A, const XT *__restrict__ x, Epi epi, Stop stop,
-                Red red) {
-  using AT = typename Epi::acc_t;
-  __shared__ AT prod[kNnzPerBlock];
-  __shared__ AT rowsum[kRowsPerBlock];
-  if (stop()) return;
-  constexpr int ND = Epi::ND > 0 ? Epi::ND : 1;
-  double acc[ND];
-#pragma unroll
-  for (int d = 0; d < ND; d++) acc[d] = 0.0;
-  const XT *xs[1] = {x};
-  for (int blk = blockIdx.x; blk < A.nrb; blk += gridDim.x) {
-    int r0, nrows;
-    spmv_block<1, MT, XT, AT>(A, blk, xs, rowsum, prod, r0, nrows);
-    if (threadIdx.x < nrows) epi.row(r0 + threadIdx.x, rowsum[threadIdx.x], acc);
-    __syncthreads();
-  }
-  if constexpr (Epi::ND > 0) {
-    if (grid_sum<ND>(acc, red.partials, red.counter) && threadIdx.x == 0) epi.finish(acc);
-  }
-}
-
-// Two SpMVs sharing one pass over A (k-skip matrix powers: r and p chains).
-// Epi::row(r, y0, y1, acc).
-template <class MT, class XT, class Epi>
-__global__ void __launch_bounds__(kThreads)
-    spmv2_kernel(CsrK<MT> A, const XT *__restrict__ x0,
-                 const XT *__restrict__ x1, Epi epi, Stop stop, Red red) {
-  using AT = typename Epi::acc_t;
-  __shared__ AT prod[2 * kNnzPerBlock];
-  __shared__ AT rowsum[2 * kRowsPerBlock];
-  if (stop()) return;
-  constexpr int ND = Epi::ND > 0 ? Epi::ND : 1;
-  double acc[ND];
-#pragma unroll
-  for (int d = 0; d < ND; d++) acc[d] = 0.0;
-  const XT *xs[2] = {x0, x1};
-  for (int blk = blockIdx.x; blk < A.nrb; blk += gridDim.x) {
-    int r0, nrows;
-    spmv_block<2, MT, XT, AT>(A, blk, xs, rowsum, prod, r0, nrows);
-    if (threadIdx.x < nrows)
-      epi.row(r0 + threadIdx.x, rowsum[threadIdx.x], rowsum[kRowsPerBlock + threadIdx.x], acc);
-    __syncthreads();
-  }
-  if constexpr (Epi::ND > 0) {
-    if (grid_sum<ND>(acc, red.partials, red.counter) && threadIdx.x == 0) epi.finish(acc);
-  }
-}
 
 // Op concept for vec_kernel:
 //   static constexpr int ND;
-//   __device__ void elem(long long i, double (&acc)[ND?ND:1]) const;
 //   __device__ void finish(const double (&sums)[ND?ND:1]) const;
+// and either
+//   __device__ void elem(long long i, double (&acc)[ND?ND:1]) const;
+// or the two-phase form, which lets every thread keep kVecUnroll elements'
+// loads in flight before its first store (an op's stores might alias its
+// loads, so the compiler cannot reorder a one-phase elem() that way):
+//   using Regs = ...;
+//   __device__ Regs load(long long i) const;
+//   __device__ void store(long long i, const Regs &r, double (&acc)[...]) const;
+constexpr int kVecUnroll = 4;
+
+template <class Op, class = void>
+struct has_two_phase : std::false_type {};
+template <class Op>
+struct has_two_phase<Op, std::void_t<typename Op::Regs>> : std::true_type {};
+
 template <class Op>
 __global__ void __launch_bounds__(kThreads)
     vec_kernel(Op op, long long n, Stop stop, Red red) {
@@ -173,8 +46,20 @@ __global__ void __launch_bounds__(kThreads)
   for (int d = 0; d < ND; d++) acc[d] = 0.0;
   const long long stride = (long long)gridDim.x * kThreads;
   long long i = (long long)blockIdx.x * kThreads + threadIdx.x;
+  if constexpr (has_two_phase<Op>::value) {
+    for (; i < n; i += stride * kVecUnroll) {
+      typename Op::Regs r[kVecUnroll];
+#pragma unroll
+      for (int u = 0; u < kVecUnroll; u++)
+        if (i + u * stride < n) r[u] = op.load(i + u * stride);
+#pragma unroll
+      for (int u = 0; u < kVecUnroll; u++)
+        if (i + u * stride < n) op.store(i + u * stride, r[u], acc);
+    }
+  } else {
 #pragma unroll 4
-  for (; i < n; i += stride) op.elem(i, acc);
+    for (; i < n; i += stride) op.elem(i, acc);
+  }
   if constexpr (Op::ND > 0) {
     if (grid_sum<ND>(acc, red.partials, red.counter) && threadIdx.x == 0) op.finish(acc);
   }
@@ -192,22 +77,59 @@ inline Red red_of(ks_ctx *ctx, int slot = 0) {
   return Red{ctx->partials, ctx->counters + slot};
 }
 
-template <class MT, class XT, class Epi>
-inline void launch_spmv(ks_ctx *ctx, const CsrDev &A, const XT *x, const Epi &epi,
-                        Stop stop, int slot = 0) {
-  const int grid = spmv_grid(ctx, A);
+template <class MT>
+inline CsrT<MT> tview(const CsrDev &A);
+template <>
+inline CsrT<double> tview<double>(const CsrDev &A) {
+  return {A.ptr, A.col, A.val, A.rbi, A.nrb, A.n};
+}
+template <>
+inline CsrT<float> tview<float>(const CsrDev &A) {
+  return {A.ptr, A.col, A.val32, A.rbi, A.nrb, A.n};
+}
+template <>
+inline CsrT<__nv_bfloat16> tview<__nv_bfloat16>(const CsrDev &A) {
+  return {A.ptr, A.col, A.val16, A.rbi, A.nrb, A.n};
+}
+
+// One-time per device and instantiation: opt in to the stage buffers' shared
+// memory and record how many CTAs fit on an SM.
+template <int NV, class MT, class XT, class Epi>
+inline int spmv_tma_ctas_per_sm(int device) {
+  static std::atomic<unsigned long long> configured{0};
+  static int per_sm[64] = {0};
+  const unsigned long long bit = 1ull << (device & 63);
+  if (!(configured.load() & bit)) {
+    auto fn = spmv_tma_kernel<NV, MT, XT, Epi>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spmv_tma_smem<MT>());
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, spmv_tma_smem<MT>()) != cudaSuccess || b < 1)
+      b = 1;
+    per_sm[device & 63] = b;
+    configured.fetch_or(bit);
+  }
+  return per_sm[device & 63];
+}
+
+template <int NV, class MT, class XT, class Epi>
+inline void launch_spmv_nv(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x1, const Epi &epi,
+                           Stop stop, int slot) {
+  const int per_sm = spmv_tma_ctas_per_sm<NV, MT, XT, Epi>(ctx->device);
+  const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
   ctx->launches++;
-  spmv_kernel<MT, XT, Epi><<<grid, kThreads, 0, ctx->stream>>>(view<MT>(A), x, epi, stop,
-                                                              red_of(ctx, slot));
+  spmv_tma_kernel<NV, MT, XT, Epi><<<grid, kThreads, spmv_tma_smem<MT>(), ctx->stream>>>(
+      tview<MT>(A), x0, x1, epi, stop, red_of(ctx, slot), ctx->d_err);
 }
 
 template <class MT, class XT, class Epi>
-inline void launch_spmv2(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x1,
-                         const Epi &epi, Stop stop, int slot = 0) {
-  const int grid = spmv_grid(ctx, A);
-  ctx->launches++;
-  spmv2_kernel<MT, XT, Epi><<<grid, kThreads, 0, ctx->stream>>>(view<MT>(A), x0, x1, epi,
-                                                               stop, red_of(ctx, slot));
+inline void launch_spmv(ks_ctx *ctx, const CsrDev &A, const XT *x, const Epi &epi, Stop stop, int slot = 0) {
+  launch_spmv_nv<1, MT, XT, Epi>(ctx, A, x, x, epi, stop, slot);
+}
+
+template <class MT, class XT, class Epi>
+inline void launch_spmv2(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x1, const Epi &epi, Stop stop,
+                         int slot = 0) {
+  launch_spmv_nv<2, MT, XT, Epi>(ctx, A, x0, x1, epi, stop, slot);
 }
 
 template <class Op>

@@ -21,7 +21,11 @@ struct ConvertOp {  // b = (D) a
   const S *a;
   D *b;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const { b[i] = (D)a[i]; }
+  struct Regs {
+    S a;
+  };
+  __device__ Regs load(long long i) const { return {a[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const { b[i] = (D)g.a; }
   __device__ void finish(const double (&)[1]) const {}
 };
 
@@ -32,8 +36,12 @@ struct DotOp {
   const T *y;
   double *out;
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
-    acc[0] = add_rn(acc[0], mul_rn(widen(x[i]), widen(y[i])));
+  struct Regs {
+    T x, y;
+  };
+  __device__ Regs load(long long i) const { return {x[i], y[i]}; }
+  __device__ void store(long long, const Regs &g, double (&acc)[1]) const {
+    acc[0] = add_rn(acc[0], mul_rn(widen(g.x), widen(g.y)));
   }
   __device__ void finish(const double (&s)[1]) const { *out = s[0]; }
 };

@@ -45,7 +45,7 @@ static ks_status fetch(ks_ctx *ctx, int count, double *host) {
                                cudaMemcpyDeviceToHost, ctx->stream));
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (int i = 0; i < count; i++) host[i] = ctx->h_pinned[i];
-  return KS_OK;
+  return check_device_error(ctx);
 }
 
 static bool same_ctx(const ks_vec *a, const ks_vec *b) { return a && b && a->ctx == b->ctx; }

@@ -204,9 +204,13 @@ struct XpbyOp {
   const VT *r;
   const double *beta;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const {
+  struct Regs {
+    VT p, r;
+  };
+  __device__ Regs load(long long i) const { return {p[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const {
     const VT b = (VT)rd(beta);
-    p[i] = add_rn(mul_rn(b, p[i]), r[i]);
+    p[i] = add_rn(mul_rn(b, g.p), g.r);
   }
   __device__ void finish(const double (&)[1]) const {}
 };
@@ -222,10 +226,14 @@ struct Xpby2Op {
   DevState *st;
   int alpha_from_qq;
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
+  struct Regs {
+    VT p, r, q, s;
+  };
+  __device__ Regs load(long long i) const { return {p[i], r[i], q[i], s[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
     const VT b = (VT)rd(&st->k.s[S_BETA]);
-    p[i] = add_rn(mul_rn(b, p[i]), r[i]);
-    const VT qi = add_rn(mul_rn(b, q[i]), s[i]);
+    p[i] = add_rn(mul_rn(b, g.p), g.r);
+    const VT qi = add_rn(mul_rn(b, g.q), g.s);
     q[i] = qi;
     acc[0] = add_rn(acc[0], mul_rn(widen(qi), widen(qi)));
   }
@@ -337,10 +345,14 @@ struct XrUpdOp {
   DevState *st;
   int mode;
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
+  struct Regs {
+    VT x, p, q, r;
+  };
+  __device__ Regs load(long long i) const { return {x[i], p[i], q[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
     const VT a = (VT)rd(&st->k.s[S_ALPHA]);
-    x[i] = add_rn(mul_rn(a, p[i]), x[i]);
-    const VT ri = add_rn(mul_rn((VT)(-a), q[i]), r[i]);
+    x[i] = add_rn(mul_rn(a, g.p), g.x);
+    const VT ri = add_rn(mul_rn((VT)(-a), g.q), g.r);
     r[i] = ri;
     acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
   }
@@ -481,10 +493,14 @@ struct Xpby2PlainOp {  // p = beta p + r; ps = beta ps + rs
   const VT *rs;
   const double *beta;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const {
+  struct Regs {
+    VT p, r, ps, rs;
+  };
+  __device__ Regs load(long long i) const { return {p[i], r[i], ps[i], rs[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const {
     const VT b = (VT)rd(beta);
-    p[i] = add_rn(mul_rn(b, p[i]), r[i]);
-    ps[i] = add_rn(mul_rn(b, ps[i]), rs[i]);
+    p[i] = add_rn(mul_rn(b, g.p), g.r);
+    ps[i] = add_rn(mul_rn(b, g.ps), g.rs);
   }
   __device__ void finish(const double (&)[1]) const {}
 };
@@ -957,13 +973,16 @@ struct KsUpdOp {
   const double *a;
   const double *bt;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const {
+  struct Regs {
+    VT x, r, p, Av;
+  };
+  __device__ Regs load(long long i) const { return {x[i], r[i], p[i], Av[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const {
     const VT al = (VT)rd(a), be = (VT)rd(bt);
-    const VT pi = p[i];
-    x[i] = add_rn(mul_rn(al, pi), x[i]);
-    const VT ri = add_rn(mul_rn((VT)(-al), Av[i]), r[i]);
+    x[i] = add_rn(mul_rn(al, g.p), g.x);
+    const VT ri = add_rn(mul_rn((VT)(-al), g.Av), g.r);
     r[i] = ri;
-    p[i] = add_rn(mul_rn(be, pi), ri);
+    p[i] = add_rn(mul_rn(be, g.p), ri);
   }
   __device__ void finish(const double (&)[1]) const {}
 };
@@ -974,8 +993,12 @@ struct GammaOp {  // s[GAMMA] = (u, v)
   const VT *v;
   DevState *st;
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
-    acc[0] = add_rn(acc[0], mul_rn(widen(u[i]), widen(v[i])));
+  struct Regs {
+    VT u, v;
+  };
+  __device__ Regs load(long long i) const { return {u[i], v[i]}; }
+  __device__ void store(long long, const Regs &g, double (&acc)[1]) const {
+    acc[0] = add_rn(acc[0], mul_rn(widen(g.u), widen(g.v)));
   }
   __device__ void finish(const double (&s)[1]) const { st->k.s[S_GAMMA] = s[0]; }
 };
@@ -1217,8 +1240,12 @@ struct RzOp {  // rr2 = (r, z); beta = rr2 / rr; rr = rr2   (vpcg.cpp:733-745)
   DevState *st;
   int init;  // 1: just rr = (r,z)
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
-    acc[0] = add_rn(acc[0], mul_rn(widen(r[i]), widen(z[i])));
+  struct Regs {
+    VT r, z;
+  };
+  __device__ Regs load(long long i) const { return {r[i], z[i]}; }
+  __device__ void store(long long, const Regs &g, double (&acc)[1]) const {
+    acc[0] = add_rn(acc[0], mul_rn(widen(g.r), widen(g.z)));
   }
   __device__ void finish(const double (&s)[1]) const {
     if (!init) st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
@@ -1483,6 +1510,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   KS_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, d_out, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(hs, ctx->h_pinned, sizeof(hs));
+  KS_TRY(check_device_error(ctx));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   const int done = (int)hs[0];
