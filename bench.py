@@ -403,6 +403,45 @@ def run_reference(args, world, rank):
     print(json.dumps(out))
 
 
+def spmv_only(args):
+    """The dominant kernel alone: y = A x with the chosen value precision on
+    the workload's matrix, timed with CUDA events over `steps` launches."""
+    import torch
+
+    import solver_cpp_b200 as ks
+    from solver_cpp_b200.matrices import config_problem
+
+    W = WORKLOADS[args.workload]
+    A, _, _ = config_problem(W["problem"], W["grid"])
+    ctx = ks.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    M = ctx.matrix(A, fp32=args.spmv_only == "fp32", bf16=args.spmv_only == "bf16")
+    dt = ks.FP64 if args.spmv_only == "fp64" else ks.FP32
+    vcode = {"fp64": ks.FP64, "fp32": ks.FP32, "bf16": ks.BF16}[args.spmv_only]
+    X = ctx.vector(np.random.default_rng(0).standard_normal(A.n), dtype=dt)
+    Y = ctx.vector(n=A.n, dtype=dt)
+    for _ in range(args.warmup):
+        ks.spmv(M, X, Y, values=vcode)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            ks.spmv(M, X, Y, values=vcode)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    alg = spmv_bytes(A.n, A.nnz, args.spmv_only)
+    peak, kind = load_peaks()
+    gbs = alg / (ms / 1e3) / 1e9
+    print(json.dumps({"kernel": f"spmv_{args.spmv_only}", "workload": args.workload, "n": A.n, "nnz": A.nnz,
+                      "alg_bytes": alg, "ms": round(ms, 5), "gbs": round(gbs, 1), "peak": peak,
+                      "frac": round(gbs / peak, 4), "peak_kind": kind}))
+    M.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,7 +452,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-iterations", type=int, default=0)
+    ap.add_argument("--spmv-only", choices=["fp64", "fp32", "bf16"], default=None,
+                    help="time only the SpMV kernel on the workload's matrix (profiling)")
     args = ap.parse_args()
+    if args.spmv_only:
+        spmv_only(args)
+        return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
