@@ -152,6 +152,25 @@ ks_status ks_axpy_dot(double a, const ks_vec *x, ks_vec *y, const ks_vec *w,
  * tall-skinny pass. */
 ks_status ks_block_dot(const ks_vec *V, int64_t ld, int k, const ks_vec *w,
                        double *h);
+/* Allocation-free form of ks_block_dot, for callers that cannot allocate
+ * device memory when they need the product: code running inside a CUDA stream
+ * capture (cudaMalloc is not allowed there), applications whose device memory
+ * is all owned by their own pool allocator, and loops that must not reach the
+ * driver allocator (cudaMalloc/cudaFree can synchronise the device). It needs
+ * no context. V (k vectors of length n, stride ld), w (n) and h (k results)
+ * are device pointers of the current device; the work is queued on `stream`
+ * (a cudaStream_t; NULL is the legacy default stream) and the call returns
+ * without waiting. Its only scratch is one fixed 151,808-byte device array that
+ * every GPU loading the library holds until the process exits; the first call
+ * on a device looks up that array's address, so make it before any stream
+ * capture starts. Every call uses the same array and clears its counters on
+ * entry: calls that can overlap on the GPU (other streams, other host threads
+ * on the same device) race and must be serialised by the caller. k must be at
+ * most KS_NOALLOC_MAX_K; larger k returns KS_BAD_INPUT (with a message on
+ * stderr). This entry point has no counterpart in the reference. */
+#define KS_NOALLOC_MAX_K 64
+ks_status ks_block_dot_noalloc(const double *V, int64_t ld, int k, const double *w, int64_t n, double *h,
+                               void *stream);
 /* w[j] -= h[i] * V_i[j] for i = 0..k-1 in order (blas::Gmres_sp_1,
  * blas.cpp:477-488). */
 ks_status ks_block_axpy(const ks_vec *V, int64_t ld, int k, const double *h,

@@ -100,6 +100,7 @@ SIGNATURES = [
     ("ks_axpy", C.c_int, [_D, _VP, _VP]),
     ("ks_axpy_dot", C.c_int, [_D, _VP, _VP, _VP, _PD]),
     ("ks_block_dot", C.c_int, [_VP, _I64, C.c_int, _VP, _VP]),
+    ("ks_block_dot_noalloc", C.c_int, [_VP, _I64, C.c_int, _VP, _I64, _VP, _VP]),
     ("ks_block_axpy", C.c_int, [_VP, _I64, C.c_int, _VP, _VP]),
     ("ks_matpow", C.c_int, [_VP, _VP, _VP, C.c_int, _VP, _VP]),
     ("ks_gram_cg", C.c_int, [_VP, _VP, _VP, _VP, C.c_int, _VP, _VP, _VP]),
