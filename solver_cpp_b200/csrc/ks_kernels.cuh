@@ -94,13 +94,13 @@ inline CsrT<__nv_bfloat16> tview<__nv_bfloat16>(const CsrDev &A) {
 
 // One-time per device and instantiation: opt in to the stage buffers' shared
 // memory and record how many CTAs fit on an SM.
-template <int NV, class MT, class XT, class Epi>
+template <int NV, class MT, class GX, class Epi>
 inline int spmv_tma_ctas_per_sm(int device) {
   static std::atomic<unsigned long long> configured{0};
   static int per_sm[64] = {0};
   const unsigned long long bit = 1ull << (device & 63);
   if (!(configured.load() & bit)) {
-    auto fn = spmv_tma_kernel<NV, MT, XT, Epi>;
+    auto fn = spmv_tma_kernel<NV, MT, GX, Epi>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spmv_tma_smem<MT>());
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, spmv_tma_smem<MT>()) != cudaSuccess || b < 1)
@@ -111,25 +111,25 @@ inline int spmv_tma_ctas_per_sm(int device) {
   return per_sm[device & 63];
 }
 
-template <int NV, class MT, class XT, class Epi>
-inline void launch_spmv_nv(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x1, const Epi &epi,
-                           Stop stop, int slot) {
-  const int per_sm = spmv_tma_ctas_per_sm<NV, MT, XT, Epi>(ctx->device);
+template <int NV, class MT, class GX, class Epi>
+inline void launch_spmv_g(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
+                          int slot = 0) {
+  const int per_sm = spmv_tma_ctas_per_sm<NV, MT, GX, Epi>(ctx->device);
   const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
   ctx->launches++;
-  spmv_tma_kernel<NV, MT, XT, Epi><<<grid, kThreads, spmv_tma_smem<MT>(), ctx->stream>>>(
-      tview<MT>(A), x0, x1, epi, stop, red_of(ctx, slot), ctx->d_err);
+  spmv_tma_kernel<NV, MT, GX, Epi><<<grid, kThreads, spmv_tma_smem<MT>(), ctx->stream>>>(
+      tview<MT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err);
 }
 
 template <class MT, class XT, class Epi>
 inline void launch_spmv(ks_ctx *ctx, const CsrDev &A, const XT *x, const Epi &epi, Stop stop, int slot = 0) {
-  launch_spmv_nv<1, MT, XT, Epi>(ctx, A, x, x, epi, stop, slot);
+  launch_spmv_g<1, MT, GPtr<XT>, Epi>(ctx, A, GPtr<XT>{x}, GPtr<XT>{x}, epi, stop, slot);
 }
 
 template <class MT, class XT, class Epi>
 inline void launch_spmv2(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x1, const Epi &epi, Stop stop,
                          int slot = 0) {
-  launch_spmv_nv<2, MT, XT, Epi>(ctx, A, x0, x1, epi, stop, slot);
+  launch_spmv_g<2, MT, GPtr<XT>, Epi>(ctx, A, GPtr<XT>{x0}, GPtr<XT>{x1}, epi, stop, slot);
 }
 
 template <class Op>

@@ -140,17 +140,49 @@ __device__ __forceinline__ bool is_long(int4 info) {
   return info.w - info.z > kNnzPerBlock;
 }
 
-// NV right-hand vectors (1, or 2 for the k-skip matrix powers).
-// Epi::row(r, y) for NV = 1, Epi::row(r, y0, y1) for NV = 2 (with acc).
-template <int NV, class MT, class XT, class Epi>
+// Gathers of the right-hand vector: x[c] from memory ...
+template <class XT>
+struct GPtr {
+  const XT *__restrict__ x;
+  __device__ __forceinline__ GPtr prep() const { return *this; }
+  template <class AT>
+  __device__ __forceinline__ AT get(int c) const {
+    return (AT)__ldg(x + c);
+  }
+};
+
+// ... or the next search direction formed on the fly, p[c] = (beta*q[c]) + r[c]
+// with beta from device memory: the update Scalar_axy(beta, p, r, p)
+// (blas.cpp:226-233) fused into the SpMV that consumes it, rounded the same
+// way element by element.
+template <class VT>
+struct GXpby {
+  const VT *__restrict__ q;
+  const VT *__restrict__ r;
+  const double *beta;
+  VT b;
+  __device__ __forceinline__ GXpby prep() const {
+    GXpby g = *this;
+    g.b = (VT)__ldg(beta);
+    return g;
+  }
+  template <class AT>
+  __device__ __forceinline__ AT get(int c) const {
+    return (AT)add_rn(mul_rn(b, __ldg(q + c)), __ldg(r + c));
+  }
+};
+
+// NV right-hand vectors (1, or 2 for the k-skip matrix powers), gathered by
+// GX. Epi::row(r, y) for NV = 1, Epi::row(r, y0, y1) for NV = 2 (with acc).
+template <int NV, class MT, class GX, class Epi>
 __global__ void __launch_bounds__(kThreads)
-    spmv_tma_kernel(CsrT<MT> A, const XT *__restrict__ x0, const XT *__restrict__ x1, Epi epi, Stop stop,
-                    Red red, int *err) {
+    spmv_tma_kernel(CsrT<MT> A, GX gx0, GX gx1, Epi epi, Stop stop, Red red, int *err) {
   using AT = typename Epi::acc_t;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   StageBuf<MT> *stage = reinterpret_cast<StageBuf<MT> *>(smem_raw);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + kStages * sizeof(StageBuf<MT>));
   if (stop()) return;
+  const GX g0 = gx0.prep(), g1 = gx1.prep();
   constexpr int ND = Epi::ND > 0 ? Epi::ND : 1;
   constexpr int G = granule<MT>();
   double acc[ND];
@@ -187,9 +219,10 @@ __global__ void __launch_bounds__(kThreads)
       double v[NV];
 #pragma unroll
       for (int u = 0; u < NV; u++) {
-        const XT *xu = u == 0 ? x0 : x1;
+        const GX &gu = u == 0 ? g0 : g1;
         AT s = (AT)0;
-        for (int j = j0 + tid; j < info.w; j += kThreads) s += mval<AT>(A.val[j]) * (AT)__ldg(xu + A.col[j]);
+        for (int j = j0 + tid; j < info.w; j += kThreads)
+          s += mval<AT>(A.val[j]) * gu.template get<AT>(A.col[j]);
         v[u] = (double)s;
       }
       block_sum<NV>(v);
@@ -223,8 +256,8 @@ __global__ void __launch_bounds__(kThreads)
         for (int e = rs; e < re; e++) {
           const AT a = mval<AT>(sb->val[e]);
           const int c = sb->col[e];
-          y0 = add_rn(y0, mul_rn(a, (AT)__ldg(x0 + c)));
-          if constexpr (NV == 2) y1 = add_rn(y1, mul_rn(a, (AT)__ldg(x1 + c)));
+          y0 = add_rn(y0, mul_rn(a, g0.template get<AT>(c)));
+          if constexpr (NV == 2) y1 = add_rn(y1, mul_rn(a, g1.template get<AT>(c)));
         }
         if constexpr (NV == 1)
           epi.row(r0 + tid, y0, acc);
@@ -239,8 +272,8 @@ __global__ void __launch_bounds__(kThreads)
         for (int e = rs + lane; e < re; e += 32) {
           const AT a = mval<AT>(sb->val[e]);
           const int c = sb->col[e];
-          y0 += a * (AT)__ldg(x0 + c);
-          if constexpr (NV == 2) y1 += a * (AT)__ldg(x1 + c);
+          y0 += a * g0.template get<AT>(c);
+          if constexpr (NV == 2) y1 += a * g1.template get<AT>(c);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

@@ -1,0 +1,102 @@
+"""The `Solver` command-line drop-in (solver_cpp_b200/bin/Solver).
+
+CPU: option handling and the reference's input checks (collection::readCMD /
+checkCRSMatrix). GPU: the reference's own command lines produce the same
+./output/<NAME>_his.txt as the reference's run (within the parity envelope,
+golden_cases.check_history), the same "loop =" line and verdict.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from golden_cases import check_history, load
+from solver_cpp_b200.matrices import config_problem, write_crs
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "solver_cpp_b200", "bin", "Solver")
+
+
+def run(args, cwd):
+    return subprocess.run([CLI] + args, cwd=cwd, capture_output=True, text=True, timeout=600)
+
+
+@pytest.fixture(scope="module")
+def cli():
+    if not os.path.exists(CLI):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "solver_cpp_b200", "csrc")], check=True)
+    return CLI
+
+
+def _problem_dir(tmp_path, name, prob, grid):
+    A, b, _ = config_problem(prob, grid)
+    write_crs(str(tmp_path / "Matrix" / "CRS" / name), A, b)
+    run_dir = tmp_path / "run"
+    run_dir.mkdir(exist_ok=True)
+    return A, b, str(run_dir)
+
+
+def test_cli_usage_and_option_errors(cli, tmp_path):
+    r = run(["--help"], str(tmp_path))
+    assert r.returncode == 0 and "usage: Solver" in r.stdout
+    r = run(["-m", "x"], str(tmp_path))
+    assert r.returncode != 0 and "OuterSolver" in r.stderr
+    r = run(["-S", "cg"], str(tmp_path))
+    assert r.returncode != 0 and "Must set one input source" in r.stderr
+    r = run(["-S", "nosuch", "-m", "x"], str(tmp_path))
+    assert r.returncode != 0 and "can not found" in r.stderr
+    r = run(["-S", "cg", "-m", "x", "-M", "y"], str(tmp_path))
+    assert r.returncode != 0 and "Only can set one input source" in r.stderr
+    r = run(["-S", "cg", "-m", "x", "--bogus"], str(tmp_path))
+    assert r.returncode != 0 and "unknown option" in r.stderr
+
+
+def test_cli_checks_crs_headers(cli, tmp_path):
+    A, b, rd = _problem_dir(tmp_path, "m", "poisson2d", 8)
+    bx = tmp_path / "Matrix" / "CRS" / "m" / "bx.txt"
+    lines = bx.read_text().splitlines()
+    lines[0] = f"{A.n + 1} {A.n + 1} {A.nnz}"
+    bx.write_text("\n".join(lines) + "\n")
+    r = run(["-S", "cg", "-m", "m", "-p", str(tmp_path)], rd)
+    assert r.returncode != 0 and "Error in CRS files" in r.stderr
+
+
+def test_cli_without_gpu_fails_cleanly(cli, tmp_path, ks):
+    if ks.lib().ks_device_count() > 0:
+        pytest.skip("a GPU is present")
+    _, _, rd = _problem_dir(tmp_path, "m", "poisson2d", 8)
+    r = run(["-S", "cg", "-m", "m", "-p", str(tmp_path)], rd)
+    assert r.returncode == 1 and "no CUDA device" in r.stderr
+
+
+def test_cli_not_implemented_methods(cli, tmp_path):
+    _, _, rd = _problem_dir(tmp_path, "m", "poisson2d", 8)
+    for m in ("kskipcr", "vpbicg"):
+        r = run(["-S", m, "-s", "cg", "-m", "m", "-p", str(tmp_path)], rd)
+        assert r.returncode == 0 and "Not implemented" in r.stdout
+
+
+CLI_CASES = ["c1_cg", "p2_cr", "cd2_bicg", "cd2_gcr", "cd2_gmres", "cd2_kskipbicg", "p3_vpcg_cg", "cd2_vpgcr_gcr",
+             "p2_kskipcg"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cid", CLI_CASES)
+def test_cli_reproduces_reference_run(cli, tmp_path, cid):
+    meta, g = load(cid)
+    _, _, rd = _problem_dir(tmp_path, "prob", meta["problem"], meta["grid"])
+    args = list(meta["args"]) + ["-m", "prob", "-p", str(tmp_path), "--reference-defects"]
+    r = run(args, rd)
+    assert r.returncode == 0, r.stderr
+    loop = int(re.search(r"^loop = (\d+)", r.stdout, re.M).group(1))
+    assert ("not converge" not in r.stdout) == meta["converged"]
+    h = np.loadtxt(os.path.join(rd, "output", f"{meta['outer']}_his.txt"), ndmin=2)
+    check_history(h[:, 0].astype(np.int64), h[:, 1], g["hist_iter"], g["hist_err"], g["envelope"], loop,
+                  meta["loop"], meta["loop_range"])
+    x = np.loadtxt(os.path.join(rd, "output", f"{meta['outer']}_xvec.txt"), ndmin=2)
+    assert x.shape[0] == meta["n"]
+    tr = float(re.search(r"\|b-ax\|2/\|b\|2 = (\S+)", r.stdout).group(1))
+    if meta["converged"]:
+        assert tr == pytest.approx(meta["true_res_log10"], abs=0.21)
