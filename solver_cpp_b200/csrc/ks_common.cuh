@@ -204,25 +204,6 @@ __device__ __forceinline__ bool grid_sum(double (&v)[ND], double *partials,
                         blockIdx.y * gridDim.x + blockIdx.x);
 }
 
-// ---------------------------------------------------------------- loads
-// Streaming (evict-first) loads for matrix data read once per SpMV, so the
-// Krylov vectors keep their place in L2.
-__device__ __forceinline__ int4 ld_stream(const int4 *p) { return __ldcs(p); }
-__device__ __forceinline__ void ld_vals4(const double *p, double (&v)[4]) {
-  double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
-  double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
-  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-}
-__device__ __forceinline__ void ld_vals4(const float *p, float (&v)[4]) {
-  float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
-  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-}
-__device__ __forceinline__ void ld_vals4(const __nv_bfloat16 *p, __nv_bfloat16 (&v)[4]) {
-  uint2 a = __ldcs(reinterpret_cast<const uint2 *>(p));
-  __nv_bfloat162 lo = *reinterpret_cast<__nv_bfloat162 *>(&a.x);
-  __nv_bfloat162 hi = *reinterpret_cast<__nv_bfloat162 *>(&a.y);
-  v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
-}
 
 }  // namespace ks
 

@@ -386,65 +386,24 @@ ks_status init_state(const Env<VT> &E, const VT *b) {
   return KS_OK;
 }
 
-// SpMV with a gather functor (fused direction update), dispatched like mv().
-template <class VT, class GX, class Epi>
-inline void mvg(const Env<VT> &E, const CsrDev &M, const GX &g, const Epi &epi) {
-  if constexpr (std::is_same<VT, double>::value) {
-    launch_spmv_g<1, double, GX, Epi>(E.ctx, M, g, g, epi, E.stop());
-  } else {
-    if (E.mvals == KS_BF16)
-      launch_spmv_g<1, __nv_bfloat16, GX, Epi>(E.ctx, M, g, g, epi, E.stop());
-    else
-      launch_spmv_g<1, float, GX, Epi>(E.ctx, M, g, g, epi, E.stop());
-  }
-}
+inline int cg_vectors() { return 3; }
 
-// The direction update of the previous iteration fused into this
-// iteration's SpMV: the SpMV gathers p_new[c] = (beta*p_old[c]) + r[c]
-// (GXpby); the owner of row i stores p_new[i] and q[i] = (A p_new)[i] and
-// accumulates (p_new, q) -> alpha = rr / (p_new, q) (cg.cpp:200-218,238-239).
-// p_old and p_new are distinct buffers, used in turn.
-template <class VT>
-struct CgFusedEpi {
-  using acc_t = VT;
-  const VT *pold;
-  const VT *r;
-  VT *pnew;
-  VT *q;
-  DevState *st;
-  static constexpr int ND = 1;
-  __device__ void row(int i, VT v, double (&acc)[1]) const {
-    const VT b = (VT)rd(&st->k.s[S_BETA]);
-    const VT pn = add_rn(mul_rn(b, pold[i]), r[i]);
-    pnew[i] = pn;
-    q[i] = v;
-    acc[0] = add_rn(acc[0], mul_rn(widen(pn), widen(v)));
-  }
-  __device__ void finish(const double (&s)[1]) const {
-    st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], s[0]);
-  }
-};
-
-inline int cg_vectors() { return 4; }
-
-// cg::solve: two kernels per iteration -- the fused direction update + SpMV
-// + (p,q), then x += alpha p, r -= alpha q, (r,r), beta and the stopping test.
-// The first iteration forms p = 0*r + r = r (beta starts at 0), which is the
-// reference's p = r (cg.cpp:174) bit for bit.
+// cg::solve, three kernels per iteration. (Forming the next direction inside
+// the SpMV's gather instead of the separate update was measured slower on
+// B200: gathering two vectors per nonzero cost 15 us per SpMV at 128^3, the
+// update kernel it removes 8 us.)
 template <class VT>
 ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
   Ws<VT> W{ws, E.n};
-  VT *r = W.take(), *q = W.take();
-  VT *pb[2] = {W.take(), W.take()};
+  VT *r = W.take(), *p = W.take(), *q = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CG});
+  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CG});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
-    const VT *pold = (L == 1) ? r : pb[L & 1];
-    VT *pnew = pb[(L + 1) & 1];
-    mvg(E, *E.A, GXpby<VT>{pold, r, &E.st->k.s[S_BETA], (VT)0}, CgFusedEpi<VT>{pold, r, pnew, q, E.st});
-    vec(E, XrUpdOp<VT>{x, r, pnew, q, E.st, 0});
+    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
+    vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 0});
+    vec(E, XpbyOp<VT>{p, r, &E.st->k.s[S_BETA]});
     if (E.outer && P.step()) break;
   }
   return KS_OK;
@@ -1209,7 +1168,7 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
 inline long long vec_count(int method, const Params &sp) {
   const long long m = sp.restart, k = sp.kskip;
   switch (method) {
-    case KS_CG: return 4;
+    case KS_CG: return 3;
     case KS_CR: return 4;
     case KS_BICG: return 5;
     case KS_GCR: case KS_VPGCR: return 3 + 2 * m;
@@ -1217,7 +1176,7 @@ inline long long vec_count(int method, const Params &sp) {
     case KS_VPGMRES: return 3 + (m + 1) + m;
     case KS_KSKIPCG: return 3 + (2 * k + 1) + (2 * k + 2);
     case KS_KSKIPBICG: return 5 + (2 * k + 1) + (2 * k + 2);
-    case KS_VPCG: return 5;
+    case KS_VPCG: return 4;
     case KS_VPCR: return 5;
   }
   return 0;
@@ -1301,24 +1260,21 @@ struct RzOp {  // rr2 = (r, z); beta = rr2 / rr; rr = rr2   (vpcg.cpp:733-745)
 
 template <class VT>
 ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT> *inner) {
-  // p = beta p + z (vpcg.cpp:748) is fused into the next iteration's SpMV,
-  // as in run_cg; the first direction is 0*z + z = z (vpcg.cpp:693).
   Ws<VT> W{ws, E.n};
-  VT *r = W.take(), *z = W.take(), *mvv = W.take();
-  VT *pb[2] = {W.take(), W.take()};
+  VT *r = W.take(), *p = W.take(), *z = W.take(), *mvv = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
   inner->solve(r, z);
+  vec(E, CopyOp<VT>{z, p});
   vec(E, RzOp<VT>{r, z, E.st, 1});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
-    const VT *pold = (L == 1) ? z : pb[L & 1];
-    VT *pnew = pb[(L + 1) & 1];
-    mvg(E, *E.A, GXpby<VT>{pold, z, &E.st->k.s[S_BETA], (VT)0}, CgFusedEpi<VT>{pold, z, pnew, mvv, E.st});
-    vec(E, XrUpdOp<VT>{x, r, pnew, mvv, E.st, 1});
+    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, mvv, E.st});
+    vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
     inner->solve(r, z);
     vec(E, RzOp<VT>{r, z, E.st, 0});
+    vec(E, XpbyOp<VT>{p, z, &E.st->k.s[S_BETA]});
     if (P.step()) break;
   }
   return KS_OK;

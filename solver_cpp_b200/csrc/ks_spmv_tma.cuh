@@ -140,7 +140,8 @@ __device__ __forceinline__ bool is_long(int4 info) {
   return info.w - info.z > kNnzPerBlock;
 }
 
-// Gathers of the right-hand vector: x[c] from memory ...
+// Gather of the right-hand vector (GX concept: prep() once per thread, then
+// get<AT>(column)).
 template <class XT>
 struct GPtr {
   const XT *__restrict__ x;
@@ -148,27 +149,6 @@ struct GPtr {
   template <class AT>
   __device__ __forceinline__ AT get(int c) const {
     return (AT)__ldg(x + c);
-  }
-};
-
-// ... or the next search direction formed on the fly, p[c] = (beta*q[c]) + r[c]
-// with beta from device memory: the update Scalar_axy(beta, p, r, p)
-// (blas.cpp:226-233) fused into the SpMV that consumes it, rounded the same
-// way element by element.
-template <class VT>
-struct GXpby {
-  const VT *__restrict__ q;
-  const VT *__restrict__ r;
-  const double *beta;
-  VT b;
-  __device__ __forceinline__ GXpby prep() const {
-    GXpby g = *this;
-    g.b = (VT)__ldg(beta);
-    return g;
-  }
-  template <class AT>
-  __device__ __forceinline__ AT get(int c) const {
-    return (AT)add_rn(mul_rn(b, __ldg(q + c)), __ldg(r + c));
   }
 };
 
