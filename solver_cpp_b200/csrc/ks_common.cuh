@@ -133,6 +133,14 @@ __device__ __forceinline__ float mval<float, __nv_bfloat16>(__nv_bfloat16 v) {
   return __bfloat162float(v);
 }
 
+// ---------------------------------------------------------------- PDL
+// Programmatic dependent launch: every kernel lets the next one in the stream
+// be scheduled at once (trigger) and waits for the previous one's results
+// only where it needs them (wait). Both are no-ops for a kernel launched
+// without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

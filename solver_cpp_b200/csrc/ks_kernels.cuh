@@ -39,6 +39,7 @@ struct has_two_phase<Op, std::void_t<typename Op::Regs>> : std::true_type {};
 template <class Op>
 __global__ void __launch_bounds__(kThreads)
     vec_kernel(Op op, long long n, Stop stop, Red red) {
+  pdl_wait();
   if (stop()) return;
   constexpr int ND = Op::ND > 0 ? Op::ND : 1;
   double acc[ND];
@@ -60,6 +61,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll 4
     for (; i < n; i += stride) op.elem(i, acc);
   }
+  pdl_trigger();  // the next kernel may be scheduled as this one drains
   if constexpr (Op::ND > 0) {
     if (grid_sum<ND>(acc, red.partials, red.counter) && threadIdx.x == 0) op.finish(acc);
   }
@@ -68,13 +70,34 @@ __global__ void __launch_bounds__(kThreads)
 // Scalar step run by a single thread (recurrences that need no vector data).
 template <class Op>
 __global__ void scalar_kernel(Op op, Stop stop) {
+  pdl_wait();
   if (stop()) return;
   if (threadIdx.x == 0 && blockIdx.x == 0) op.run();
+  pdl_trigger();
 }
 
 // ------------------------------------------------------------------ launchers
 inline Red red_of(ks_ctx *ctx, int slot = 0) {
   return Red{ctx->partials, ctx->counters + slot};
+}
+
+// Launch on the context's stream with programmatic stream serialization:
+// the kernel may be scheduled while the previous one finishes, and reads the
+// previous kernels' results only after its griddepcontrol.wait (pdl_wait).
+template <class... KArgs, class... Args>
+inline void launch_k(ks_ctx *ctx, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ctx->launches++;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
 template <class MT>
@@ -116,9 +139,8 @@ inline void launch_spmv_g(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &
                           int slot = 0) {
   const int per_sm = spmv_tma_ctas_per_sm<NV, MT, GX, Epi>(ctx->device);
   const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
-  ctx->launches++;
-  spmv_tma_kernel<NV, MT, GX, Epi><<<grid, kThreads, spmv_tma_smem<MT>(), ctx->stream>>>(
-      tview<MT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err);
+  launch_k(ctx, spmv_tma_kernel<NV, MT, GX, Epi>, dim3(grid), dim3(kThreads), spmv_tma_smem<MT>(), tview<MT>(A), g0,
+           g1, epi, stop, red_of(ctx, slot), ctx->d_err);
 }
 
 template <class MT, class XT, class Epi>
@@ -137,14 +159,12 @@ inline void launch_vec(ks_ctx *ctx, long long n, const Op &op, Stop stop, int sl
   long long need = (n + kThreads - 1) / kThreads;
   int grid = red_grid(ctx);
   if (need < grid) grid = (int)(need > 0 ? need : 1);
-  ctx->launches++;
-  vec_kernel<Op><<<grid, kThreads, 0, ctx->stream>>>(op, n, stop, red_of(ctx, slot));
+  launch_k(ctx, vec_kernel<Op>, dim3(grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
 }
 
 template <class Op>
 inline void launch_scalar(ks_ctx *ctx, const Op &op, Stop stop) {
-  ctx->launches++;
-  scalar_kernel<Op><<<1, 32, 0, ctx->stream>>>(op, stop);
+  launch_k(ctx, scalar_kernel<Op>, dim3(1), dim3(32), 0, op, stop);
 }
 
 }  // namespace ks

@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(kThreads)
     block_dot_kernel(const VT *__restrict__ V, long long ld, int k,
                      const VT *__restrict__ W0, const VT *__restrict__ W1, long long n,
                      Epi epi, Stop stop, double *partials, unsigned *counters) {
+  pdl_wait();
   if (stop()) return;
   constexpr int G8 = kBlockDotGroup;
   const int g = blockIdx.y;
@@ -145,6 +146,7 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
+  pdl_trigger();
   double *part = partials + (size_t)g * NW * G8 * gridDim.x;
   if (grid_sum_n<NW * G8>(acc, part, counters + g, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
     for (int q = 0; q < cnt; q++) {
@@ -171,9 +173,8 @@ inline ks_status launch_block_dot(ks_ctx *ctx, const VT *V, long long ld, int k,
   const long long need = (n + kThreads - 1) / kThreads;
   if (need < gx) gx = (int)std::max<long long>(need, 1);
   dim3 grid(gx, groups);
-  ctx->launches++;
-  block_dot_kernel<NW, VT, Epi><<<grid, kThreads, 0, ctx->stream>>>(
-      V, ld, k, W0, W1, n, epi, stop, ctx->partials, ctx->counters + 16);
+  launch_k(ctx, block_dot_kernel<NW, VT, Epi>, grid, dim3(kThreads), 0, V, ld, k, W0, W1, n, epi, stop,
+           ctx->partials, ctx->counters + 16);
   return KS_OK;
 }
 

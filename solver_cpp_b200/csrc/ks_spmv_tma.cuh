@@ -161,8 +161,6 @@ __global__ void __launch_bounds__(kThreads)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   StageBuf<MT> *stage = reinterpret_cast<StageBuf<MT> *>(smem_raw);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + kStages * sizeof(StageBuf<MT>));
-  if (stop()) return;
-  const GX g0 = gx0.prep(), g1 = gx1.prep();
   constexpr int ND = Epi::ND > 0 ? Epi::ND : 1;
   constexpr int G = granule<MT>();
   double acc[ND];
@@ -176,7 +174,9 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
 
-  // Producer state (thread 0): next block of this CTA to stage.
+  // Producer state (thread 0): next block of this CTA to stage. The matrix
+  // does not depend on the kernels before this one, so the first blocks are
+  // staged before waiting for them (programmatic dependent launch).
   int prod_blk = blockIdx.x;
   int staged = 0;  // copies issued
   if (tid == 0) {
@@ -189,6 +189,14 @@ __global__ void __launch_bounds__(kThreads)
       prod_blk += gridDim.x;
     }
   }
+  pdl_wait();  // x, the stop flags and the scalars come from earlier kernels
+  if (stop()) {
+    if (tid == 0)  // let the copies already issued land before the CTA exits
+      for (int c = 0; c < staged; c++) mbar_wait(&bars[c % kStages], (uint32_t)((c / kStages) & 1));
+    __syncthreads();
+    return;
+  }
+  const GX g0 = gx0.prep(), g1 = gx1.prep();
   int consumed = 0;
   bool failed = false;
   for (int blk = blockIdx.x; blk < A.nrb && !failed; blk += gridDim.x) {
@@ -289,6 +297,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = consumed; c < staged; c++) mbar_wait(&bars[c % kStages], (uint32_t)((c / kStages) & 1));
   }
   __syncthreads();
+  pdl_trigger();  // the next kernel may be scheduled as this one drains
   if constexpr (Epi::ND > 0) {
     if (grid_sum<ND>(acc, red.partials, red.counter) && tid == 0) epi.finish(acc);
   }
