@@ -339,17 +339,29 @@ def cpu_baseline_port(A, b, W, res):
     t0 = time.perf_counter()
     o = pyoracle.solve(P, b, W["outer"], W["inner"], hist_cap=64, **p)
     dt = time.perf_counter() - t0
-    per_iter = dt / max(1, sample_iters)
+    vp = W["inner"] != "NONE"
+    # a VP run of L iterations does L + 1 inner solves (vpcg.cpp:685,743)
+    per_iter = dt / (sample_iters + 1 if vp else sample_iters)
     est = per_iter * max(1, res.loop)
     return {"value": round(est, 3), "unit": "s", "cores": 1, "kind": "port",
             "sample": f"{sample_iters} iterations of {W['outer']}" + (f"/{W['inner']}" if W['inner'] != 'NONE' else '')
                       + f" in FP64 on the full system ({dt:.2f} s), scaled to the GPU run's {res.loop} iterations"}
 
 
+#: Iterations the reference's own full solve takes on each workload (outer
+#: iterations for VPCG), measured once by running oracle/_ref/Solver to
+#: convergence with 8 OpenMP threads: c4_mixed `-S vpcg -s cg -l 20 -e 1e-30
+#: -E 1e-10` 593 outer iterations (285.8 s); plain CG on the same system 5157
+#: (144.8 s); c2_cg `-S cg -E 1e-10` 530.
+REF_FULL_ITERATIONS = {"c4_mixed": 593, "c2_cg": 530}
+
+
 def run_reference(args, world, rank):
     """The reference's own CPU path (oracle/_ref/Solver, all host threads) on
-    the same workload: each step runs a bounded number of iterations and is
-    scaled to the iteration count the full solve needs."""
+    the same workload: each step runs a bounded number of iterations of the
+    same method and is scaled to the iteration count of the reference's full
+    solve (REF_FULL_ITERATIONS). The timed quantity is the reference's own
+    `time =` line, which covers its solve() only, as in the reference."""
     if world > 1 and rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -375,20 +387,28 @@ def run_reference(args, world, rank):
         from solver_cpp_b200.matrices import write_crs
 
         write_crs(mdir, A, b)
-    # iterations to convergence of the reference's method on this system:
-    # the plain and mixed runs use the same outer method; one full run of the
-    # bounded sample gives the per-iteration time.
-    cap = 3 if W["inner"] != "NONE" else 40
+    # A step runs `cap` iterations of the reference's method (-L cap). A VP
+    # method does one inner solve before its loop and one per iteration
+    # (vpcg.cpp:685,743), so cap iterations hold cap + 1 inner solves and a
+    # full solve of `full` iterations holds full + 1.
+    vp = W["inner"] != "NONE"
+    cap = 3 if vp else 40
+    units = cap + 1 if vp else cap
     times, loops = [], []
     for i in range(args.warmup + args.steps):
         r = pyoracle.run_reference(A, b, W["ref_args"] + ["-L", str(cap)], threads=threads, workdir=wd,
                                    name="bench", keep_x=False)
+        if r["time"] is None:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference binary did not report a time: "
+                              + (r["stderr"] or "")[-200:].replace("\n", " ")}))
+            return
         if i >= args.warmup:
             times.append(r["time"])
             loops.append(r["loop"])
-    per_iter = statistics.median(t / max(1, min(l, cap)) for t, l in zip(times, loops))
-    full = args.ref_iterations or {"c4_mixed": 0, "c2_cg": 0}.get(args.workload) or cap
-    value = per_iter * full
+    per_unit = statistics.median(t / units for t in times)
+    full = args.ref_iterations or REF_FULL_ITERATIONS.get(args.workload) or cap
+    value = per_unit * (full + 1 if vp else full)
+    per_iter = per_unit
     out = {"impl": "reference", "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); "
            "SpMV HBM GB/s", "value": round(value, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(statistics.median(times) * 1e3, 2), "higher_is_better": False,
