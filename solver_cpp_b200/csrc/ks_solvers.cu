@@ -315,6 +315,34 @@ __device__ void StartEpi<VT>::finish(const double (&s)[1]) const {
   }
 }
 
+// The start of a method whose x is zero (every method zeroes x first, as
+// cg.cpp:79 does): A*0 is exactly 0, so r = b - A*0 is b bit for bit and the
+// SpMV can be skipped; one vector pass does the copies, (r,r) and the same
+// scalar step as StartEpi::finish.
+template <class VT>
+struct StartZeroOp {
+  StartEpi<VT> e;
+  static constexpr int ND = 1;
+  struct Regs {
+    VT b;
+  };
+  __device__ Regs load(long long i) const { return {e.b[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
+    const VT ri = sub_rn(g.b, (VT)0);
+    e.r[i] = ri;
+    if (e.c1) e.c1[i] = ri;
+    if (e.c2) e.c2[i] = ri;
+    if (e.c3) e.c3[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[1]) const { e.finish(s); }
+};
+
+template <class VT>
+inline void start_from_zero(const Env<VT> &E, const StartEpi<VT> &epi) {
+  vec(E, StartZeroOp<VT>{epi});
+}
+
 // ------------------------------------------------------------------ CG
 // cg::solve (cg.cpp:148-240), three fused kernels per iteration:
 //   q = A p, (p,q) -> alpha;  x += alpha p, r -= alpha q, (r,r) -> beta,
@@ -398,7 +426,7 @@ ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
   VT *r = W.take(), *p = W.take(), *q = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CG});
+  start_from_zero(E, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CG});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
@@ -457,7 +485,7 @@ ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
   VT *r = W.take(), *p = W.take(), *q = W.take(), *s = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CHECK});
+  start_from_zero(E, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CHECK});
   mv(E, *E.A, (const VT *)p, CrStartMvEpi<VT>{r, q, s, E.st});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
@@ -519,7 +547,7 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   // (r*, r) = (r, r) at the start
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, rs, p, ps, E.st, START_CG});
+  start_from_zero(E, StartEpi<VT>{b, r, rs, p, ps, E.st, START_CG});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
@@ -651,14 +679,16 @@ ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws
   Poller P_{E.ctx, E.hflag, E.lookahead};
   long long issued_steps = 0;
   bool stop_host = false;
+  bool x_zero = true;  // the first cycle starts from x = 0
   while (!stop_host) {
     // cycle start: r = b - A x, then the first direction
-    if (inner) {
-      mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_GCR});
-      inner->solve(r, P);  // P_0 = M(r)
-    } else {
-      mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, P, nullptr, nullptr, E.st, START_GCR});
-    }
+    const StartEpi<VT> se{b, r, inner ? nullptr : P, nullptr, nullptr, E.st, START_GCR};
+    if (x_zero)
+      start_from_zero(E, se);
+    else
+      mv(E, *E.A, (const VT *)x, se);
+    x_zero = false;
+    if (inner) inner->solve(r, P);  // P_0 = M(r)
     mv(E, *E.A, (const VT *)P, GcrQ0Epi<VT>{r, Q, qq, E.st});
     for (int k = 0; k < m; k++) {
       const bool last = (k == m - 1);
@@ -861,8 +891,14 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
   long long issued = 0;
   bool stop_host = false;
   const VT *B = inner ? Z : V;
+  bool x_zero = true;  // the first cycle starts from x = 0
   while (!stop_host) {
-    mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_NORM});
+    const StartEpi<VT> se{b, r, nullptr, nullptr, nullptr, E.st, START_NORM};
+    if (x_zero)
+      start_from_zero(E, se);
+    else
+      mv(E, *E.A, (const VT *)x, se);
+    x_zero = false;
     vec(E, ScaleOp<VT>{r, V, &E.st->k.s[S_T]});
     launch_scalar(E.ctx, GmCycleOp{g, E.st}, E.stop());
     for (int k = 0; k < m - 1; k++) {
@@ -1051,7 +1087,7 @@ ks_status run_kskipcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws)
   double *G = dws, *coef = dws + 6 * k + 4;
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_KSKIP});
+  start_from_zero(E, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_KSKIP});
   Poller P{E.ctx, E.hflag, E.lookahead};
   long long nloop = 0;
   for (nloop = 0; nloop < E.sp.maxloop; nloop += k + 1) {
@@ -1140,7 +1176,7 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
   double *G = dws, *coef = dws + 8 * k + 6;
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, p, rs, ps, E.st, START_KSKIP});
+  start_from_zero(E, StartEpi<VT>{b, r, p, rs, ps, E.st, START_KSKIP});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long nloop = 0; nloop < E.sp.maxloop; nloop += k + 1) {
     // the check uses |r|; gamma = (r*, r) comes right after
@@ -1264,7 +1300,7 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
   VT *r = W.take(), *p = W.take(), *z = W.take(), *mvv = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
+  start_from_zero(E, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
   inner->solve(r, z);
   vec(E, CopyOp<VT>{z, p});
   vec(E, RzOp<VT>{r, z, E.st, 1});
@@ -1312,7 +1348,7 @@ ks_status run_vpcr(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
   VT *r = W.take(), *p = W.take(), *z = W.take(), *Av = W.take(), *Ap = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
-  mv(E, *E.A, (const VT *)x, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
+  start_from_zero(E, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
   inner->solve(r, z);
   vec(E, CopyOp<VT>{z, p});
   mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, Ap, E.st, 1});
