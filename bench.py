@@ -11,6 +11,10 @@ Workloads (the default is the one the headline metric is quoted on):
             exactly 20 iterations, to rel-res 1e-10. The plain FP64 CG on the
             same system is timed beside it.
   c2_cg     3D 7-point Poisson 128^3 (n = 2,097,152), b ~ U(0,1): CG FP64.
+  The other entries of WORKLOADS time the remaining methods of the
+  configurations (CR and k-skip CG on the Poisson system; BiCG, k-skip BiCG,
+  GCR(30) and GMRES(30) on the 128^3 upwind convection-diffusion system;
+  VPGMRES and the BF16-valued VPCG on the 160^3 system), one JSON line each.
 Inputs are seeded synthetic data with the configurations' shapes; the matrix
 (>= 175 MB) is larger than the 126 MB L2, so no L2 flush is needed between
 steps.
@@ -39,15 +43,36 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+def _w(problem, grid, outer, params, inner="NONE", plain=None, ref_args=(), spmv_values="fp64", transpose=False):
+    return dict(problem=problem, grid=grid, outer=outer, inner=inner, params=params, plain=plain,
+                ref_args=list(ref_args), spmv_values=spmv_values, transpose=transpose)
+
+
+_VP20 = dict(E=1e-10, L=10000, l=20, e=1e-30)
 WORKLOADS = {
-    "c4_mixed": dict(problem="varcoef3d", grid=160, outer="VPCG", inner="CG",
-                     params=dict(E=1e-10, L=10000, l=20, e=1e-30, inner_precision="fp32"),
-                     plain=dict(outer="CG", params=dict(E=1e-10, L=20000)),
-                     ref_args=["-S", "vpcg", "-s", "cg", "-l", "20", "-e", "1e-30", "-E", "1e-10"],
-                     spmv_values="fp32"),
-    "c2_cg": dict(problem="poisson3d", grid=128, outer="CG", inner="NONE",
-                  params=dict(E=1e-10, L=10000), plain=None,
-                  ref_args=["-S", "cg", "-E", "1e-10"], spmv_values="fp64"),
+    # headline: VPCG (FP64 outer, FP32 inner CG of 20 iterations) against plain FP64 CG
+    "c4_mixed": _w("varcoef3d", 160, "VPCG", dict(_VP20, inner_precision="fp32"), inner="CG",
+                   plain=dict(outer="CG", params=dict(E=1e-10, L=20000)),
+                   ref_args=["-S", "vpcg", "-s", "cg", "-l", "20", "-e", "1e-30", "-E", "1e-10"],
+                   spmv_values="fp32"),
+    "c4_mixed_bf16": _w("varcoef3d", 160, "VPCG", dict(_VP20, inner_precision="bf16"), inner="CG",
+                        plain=dict(outer="CG", params=dict(E=1e-10, L=20000)), spmv_values="bf16"),
+    # VPGMRES (FP64 outer, reference default restart 1000) with the FP32 inner CG,
+    # against plain FP64 GMRES with the same restart
+    "c4_vpgmres": _w("varcoef3d", 160, "VPGMRES", dict(_VP20, inner_precision="fp32"), inner="CG",
+                     plain=dict(outer="GMRES", params=dict(E=1e-10, L=20000)), spmv_values="fp32"),
+    "c2_cg": _w("poisson3d", 128, "CG", dict(E=1e-10, L=10000), ref_args=["-S", "cg", "-E", "1e-10"]),
+    "c2_cr": _w("poisson3d", 128, "CR", dict(E=1e-10, L=10000), ref_args=["-S", "cr", "-E", "1e-10"]),
+    "c2_kskipcg2": _w("poisson3d", 128, "KSKIPCG", dict(E=1e-10, L=10000, K=2)),
+    "c2_kskipcg4": _w("poisson3d", 128, "KSKIPCG", dict(E=1e-10, L=10000, K=4)),
+    "c3_bicg": _w("convdiff3d", 128, "BICG", dict(E=1e-10, L=10000), transpose=True,
+                  ref_args=["-S", "bicg", "-E", "1e-10"]),
+    "c3_kskipbicg2": _w("convdiff3d", 128, "KSKIPBICG", dict(E=1e-10, L=10000, K=2), transpose=True,
+                        ref_args=["-S", "kskipbicg", "-K", "2", "-E", "1e-10"]),
+    "c3_gcr30": _w("convdiff3d", 128, "GCR", dict(E=1e-10, L=10000, R=30),
+                   ref_args=["-S", "gcr", "-R", "30", "-E", "1e-10"]),
+    "c3_gmres30": _w("convdiff3d", 128, "GMRES", dict(E=1e-10, L=10000, R=30),
+                     ref_args=["-S", "gmres", "-R", "30", "-E", "1e-10"]),
 }
 
 
@@ -144,12 +169,13 @@ def barrier(world):
         dist.barrier()
 
 
-def spmv_bytes(n, nnz, values):
-    """Algorithmic bytes of one SpMV: values + int32 columns + int32 row
-    offsets + x read once + y written once."""
+def spmv_bytes(n, nnz, values, index_bytes=4):
+    """Algorithmic bytes of one SpMV: values + column indices (int32, or the
+    int16 row offsets the library stores when they fit) + int32 row offsets
+    + x read once + y written once."""
     vb = {"fp64": 8, "fp32": 4, "bf16": 2}[values]
     xb = 8 if values == "fp64" else 4
-    return nnz * (vb + 4) + 4 * (n + 1) + xb * n + xb * n
+    return nnz * (vb + index_bytes) + 4 * (n + 1) + xb * n + xb * n
 
 
 def run_ours(args, world, rank, local):
@@ -164,7 +190,7 @@ def run_ours(args, world, rank, local):
     ctx = ks.Context(local)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
-    M = ctx.matrix(A, transpose=False, fp32=True, bf16=True)
+    M = ctx.matrix(A, transpose=W["transpose"], fp32=True, bf16=True)
     B = ctx.vector(b)
     X = ctx.vector(n=n)
     launches0 = ks.lib().ks_ctx_launches(ctx.handle)
@@ -238,20 +264,22 @@ def run_ours(args, world, rank, local):
         s1.record(stream)
     torch.cuda.synchronize()
     spmv_ms = s0.elapsed_time(s1) / reps
-    alg = spmv_bytes(n, nnz, vals)
+    ib = M.info()["index_bytes"]
+    alg = spmv_bytes(n, nnz, vals, ib)
     peak, peak_kind = load_peaks()
     achieved = alg / (spmv_ms / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(f"{args.workload}:{vals}")
+            traffic = json.load(open(tf)).get(f"{args.workload}:{vals}:i{ib}")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": f"spmv_{vals}",
-                "alg_bytes_per_launch": alg, "launch_ms": round(spmv_ms, 5), "peak_kind": peak_kind}
-    fp64_bytes = spmv_bytes(n, nnz, "fp64")
+                "alg_bytes_per_launch": alg, "index_bytes": ib, "launch_ms": round(spmv_ms, 5),
+                "peak_kind": peak_kind}
+    fp64_bytes = spmv_bytes(n, nnz, "fp64", ib)
     if vals != "fp64":  # also the FP64 SpMV of the outer loop
         x64, y64 = ctx.vector(np.random.default_rng(0).standard_normal(n)), ctx.vector(n=n)
         ks.spmv(M, x64, y64)
@@ -302,7 +330,8 @@ def run_ours(args, world, rank, local):
         "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); SpMV HBM GB/s",
         "value": round(value, 6), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_per_step, 4), "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 outer / f32 inner" if args.workload == "c4_mixed" else "f64",
+        "vs_baseline": None, "dtype": ("f64 outer / " + {"fp32": "f32", "bf16": "f32 with bf16 values"}[
+            W["params"]["inner_precision"]] + " inner") if "inner_precision" in W["params"] else "f64",
         "data": "synthetic (seeded generator of the configuration; no dataset)",
         "config": {"workload": args.workload, "problem": W["problem"], "grid": W["grid"], "n": n, "nnz": nnz,
                    "method": W["outer"] + ("/" + W["inner"] if W["inner"] != "NONE" else ""),
@@ -335,7 +364,7 @@ def cpu_baseline_port(A, b, W, res):
     p.pop("inner_precision", None)
     sample_iters = 2 if W["inner"] != "NONE" else 20
     p["L"] = sample_iters
-    P = pyoracle.Problem(A, with_transpose=False)
+    P = pyoracle.Problem(A, with_transpose=W["transpose"])
     t0 = time.perf_counter()
     o = pyoracle.solve(P, b, W["outer"], W["inner"], hist_cap=64, **p)
     dt = time.perf_counter() - t0
@@ -436,7 +465,8 @@ def spmv_only(args):
     ctx = ks.Context(0)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
-    M = ctx.matrix(A, fp32=args.spmv_only == "fp32", bf16=args.spmv_only == "bf16")
+    M = ctx.matrix(A, fp32=args.spmv_only == "fp32", bf16=args.spmv_only == "bf16", index32=args.index32)
+    ib = M.info()["index_bytes"]
     dt = ks.FP64 if args.spmv_only == "fp64" else ks.FP32
     vcode = {"fp64": ks.FP64, "fp32": ks.FP32, "bf16": ks.BF16}[args.spmv_only]
     X = ctx.vector(np.random.default_rng(0).standard_normal(A.n), dtype=dt)
@@ -452,11 +482,11 @@ def spmv_only(args):
         e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    alg = spmv_bytes(A.n, A.nnz, args.spmv_only)
+    alg = spmv_bytes(A.n, A.nnz, args.spmv_only, ib)
     peak, kind = load_peaks()
     gbs = alg / (ms / 1e3) / 1e9
     print(json.dumps({"kernel": f"spmv_{args.spmv_only}", "workload": args.workload, "n": A.n, "nnz": A.nnz,
-                      "alg_bytes": alg, "ms": round(ms, 5), "gbs": round(gbs, 1), "peak": peak,
+                      "index_bytes": ib, "alg_bytes": alg, "ms": round(ms, 5), "gbs": round(gbs, 1), "peak": peak,
                       "frac": round(gbs / peak, 4), "peak_kind": kind}))
     M.close()
     ctx.close()
@@ -474,6 +504,7 @@ def main():
     ap.add_argument("--ref-iterations", type=int, default=0)
     ap.add_argument("--spmv-only", choices=["fp64", "fp32", "bf16"], default=None,
                     help="time only the SpMV kernel on the workload's matrix (profiling)")
+    ap.add_argument("--index32", action="store_true", help="with --spmv-only: int32 column indices")
     args = ap.parse_args()
     if args.spmv_only:
         spmv_only(args)

@@ -83,6 +83,11 @@ int ks_abi_version(void);
 #define KS_MAT_TRANSPOSE 1u /* also build A^T (the reference's CTval/CTcol/CTptr) */
 #define KS_MAT_FP32 2u      /* keep an FP32 copy of the values                    */
 #define KS_MAT_BF16 4u      /* keep a BF16 copy of the values                     */
+/* By default the SpMV reads column indices as 16-bit offsets from the row
+ * (col - row) whenever every offset of the matrix fits in int16, halving the
+ * index bytes of banded and stencil matrices; results are identical. This
+ * flag keeps the int32 columns instead. */
+#define KS_MAT_INDEX32 8u
 
 /* Upload a host CSR matrix (collection::CudaCopy_Part1,
  * solver_collection.cpp:932-942) and build the row-block schedule of the
@@ -101,6 +106,9 @@ ks_status ks_mat_destroy(ks_mat *mat);
 /* n, nnz, and the number of SpMV row blocks. */
 ks_status ks_mat_info(const ks_mat *mat, int64_t *n, int64_t *nnz,
                       int64_t *row_blocks);
+/* Bytes per column index the SpMV reads for A (2 or 4) and for A^T (0 when
+ * there is no transpose). No counterpart in the reference. */
+ks_status ks_mat_index_bytes(const ks_mat *mat, int *a_bytes, int *t_bytes);
 /* Copy the device-built transpose back (CSR of A^T: tptr[n+1], trow[nnz],
  * tval[nnz]), i.e. the CSC arrays the reference's CSR2CSC returns. */
 ks_status ks_mat_transpose_download(const ks_mat *mat, int32_t *tptr,

@@ -84,8 +84,8 @@ class Context:
     def set_stream(self, stream_ptr):
         _check(lib().ks_ctx_set_stream(self.handle, C.c_void_p(stream_ptr)), self.handle, "set_stream")
 
-    def matrix(self, A: CSR, transpose=False, fp32=False, bf16=False) -> "Matrix":
-        return Matrix(self, A, transpose=transpose, fp32=fp32, bf16=bf16)
+    def matrix(self, A: CSR, transpose=False, fp32=False, bf16=False, index32=False) -> "Matrix":
+        return Matrix(self, A, transpose=transpose, fp32=fp32, bf16=bf16, index32=index32)
 
     def vector(self, data=None, n=None, dtype=FP64) -> "Vector":
         return Vector(self, data=data, n=n, dtype=dtype)
@@ -93,16 +93,17 @@ class Context:
 
 class Matrix:
     """Device CSR matrix (``ks_mat``), optionally with its transpose and
-    FP32 / BF16 value copies."""
+    FP32 / BF16 value copies. ``index32`` keeps int32 column indices in the
+    SpMV instead of the 16-bit row offsets used when they fit."""
 
-    def __init__(self, ctx: Context, A: CSR, transpose=False, fp32=False, bf16=False):
+    def __init__(self, ctx: Context, A: CSR, transpose=False, fp32=False, bf16=False, index32=False):
         self.ctx = ctx
         self.n, self.nnz = A.n, A.nnz
         ptr = np.ascontiguousarray(A.ptr, dtype=np.int32)
         col = np.ascontiguousarray(A.col, dtype=np.int32)
         val = np.ascontiguousarray(A.val, dtype=np.float64)
         flags = (_abi.MAT_TRANSPOSE if transpose else 0) | (_abi.MAT_FP32 if fp32 else 0) | (
-            _abi.MAT_BF16 if bf16 else 0)
+            _abi.MAT_BF16 if bf16 else 0) | (_abi.MAT_INDEX32 if index32 else 0)
         h = C.c_void_p()
         _check(lib().ks_csr_upload(ctx.handle, self.n, self.nnz, _ptr(ptr), _ptr(col), _ptr(val), flags,
                                    C.byref(h)), ctx.handle, "ks_csr_upload")
@@ -123,7 +124,10 @@ class Matrix:
     def info(self):
         n, nnz, rb = C.c_int64(), C.c_int64(), C.c_int64()
         _check(lib().ks_mat_info(self.handle, C.byref(n), C.byref(nnz), C.byref(rb)), self.ctx.handle, "info")
-        return {"n": n.value, "nnz": nnz.value, "row_blocks": rb.value}
+        a, t = C.c_int(), C.c_int()
+        _check(lib().ks_mat_index_bytes(self.handle, C.byref(a), C.byref(t)), self.ctx.handle, "index_bytes")
+        return {"n": n.value, "nnz": nnz.value, "row_blocks": rb.value, "index_bytes": a.value,
+                "t_index_bytes": t.value}
 
     def transpose_arrays(self):
         tptr = np.zeros(self.n + 1, dtype=np.int32)

@@ -40,6 +40,7 @@ PRECISIONS = {"fp64": FP64, "fp32": FP32, "bf16": BF16}
 MAT_TRANSPOSE = 1
 MAT_FP32 = 2
 MAT_BF16 = 4
+MAT_INDEX32 = 8
 
 
 class Params(C.Structure):
@@ -82,6 +83,7 @@ SIGNATURES = [
     ("ks_csr_upload_device", C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP, C.c_uint, C.POINTER(_VP)]),
     ("ks_mat_destroy", C.c_int, [_VP]),
     ("ks_mat_info", C.c_int, [_VP, _PI64, _PI64, _PI64]),
+    ("ks_mat_index_bytes", C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("ks_mat_transpose_download", C.c_int, [_VP, _VP, _VP, _VP]),
     ("ks_vec_create", C.c_int, [_VP, _I64, C.c_int, C.POINTER(_VP)]),
     ("ks_vec_wrap", C.c_int, [_VP, _I64, C.c_int, _VP, C.POINTER(_VP)]),

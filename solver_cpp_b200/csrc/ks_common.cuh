@@ -68,6 +68,10 @@ struct CsrDev {
   long long nnz = 0;
   int *ptr = nullptr;
   int *col = nullptr;
+  // Column indices as 16-bit offsets from the row (col - row), kept when every
+  // offset fits in [-32768, 32767]; the SpMV then reads 2 bytes per column
+  // instead of 4. Null when an offset does not fit or KS_MAT_INDEX32 is set.
+  short *col16 = nullptr;
   double *val = nullptr;
   float *val32 = nullptr;
   __nv_bfloat16 *val16 = nullptr;

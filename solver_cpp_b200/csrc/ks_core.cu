@@ -203,9 +203,35 @@ __global__ void k_to_bf16(const double *__restrict__ a, __nv_bfloat16 *__restric
     b[i] = __float2bfloat16_rn((float)a[i]);
 }
 
+// Checks every column index (0 <= col < n) and stores col - row as int16
+// where it fits: flags |= 1 for a column out of range, |= 2 for an offset
+// outside [-32768, 32767] (col16 is then discarded by the caller).
+__global__ void k_col16(const int *__restrict__ ptr, const int *__restrict__ col, int n,
+                        short *__restrict__ col16, int *flags) {
+  int bad = 0;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    const int j1 = ptr[r + 1];
+    for (int j = ptr[r]; j < j1; j++) {
+      const int c = col[j];
+      if (c < 0 || c >= n) {
+        bad |= 1;
+        continue;
+      }
+      const int d = c - (int)r;
+      if (d < -32768 || d > 32767)
+        bad |= 2;
+      else if (col16)
+        col16[j] = (short)d;
+    }
+  }
+  if (bad) atomicOr(flags, bad);
+}
+
 static void free_csr(CsrDev &A) {
   cudaFree(A.ptr);
   cudaFree(A.col);
+  cudaFree(A.col16);
   cudaFree(A.val);
   cudaFree(A.val32);
   cudaFree(A.val16);
@@ -241,6 +267,28 @@ static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, uns
                                ctx->stream));
   const long long tot = A.nnz + kPad;
   const int g = ctx->num_sms * 8;
+  {
+    if (!(flags & KS_MAT_INDEX32)) {
+      KS_CUDA(ctx, cudaMalloc(&A.col16, sizeof(short) * (size_t)tot));
+      KS_CUDA(ctx, cudaMemsetAsync(A.col16 + A.nnz, 0, sizeof(short) * kPad, ctx->stream));
+    }
+    int *d_flags = nullptr, h_flags = 0;
+    KS_CUDA(ctx, cudaMalloc(&d_flags, sizeof(int)));
+    cudaError_t e = cudaMemsetAsync(d_flags, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess) {
+      k_col16<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.n, A.col16, d_flags);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_flags);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "column index check");
+    if (h_flags & 1) return set_error(ctx, KS_BAD_INPUT, "column index out of range");
+    if (h_flags & 2) {
+      cudaFree(A.col16);
+      A.col16 = nullptr;
+    }
+  }
   if (flags & KS_MAT_FP32) {
     KS_CUDA(ctx, cudaMalloc(&A.val32, sizeof(float) * (size_t)tot));
     k_to_f32<<<g, 256, 0, ctx->stream>>>(A.val, A.val32, tot);
@@ -504,6 +552,13 @@ ks_status ks_mat_info(const ks_mat *m, int64_t *n, int64_t *nnz, int64_t *row_bl
   if (n) *n = m->A.n;
   if (nnz) *nnz = m->A.nnz;
   if (row_blocks) *row_blocks = m->A.nrb;
+  return KS_OK;
+}
+
+ks_status ks_mat_index_bytes(const ks_mat *m, int *a_bytes, int *t_bytes) {
+  if (!m) return KS_BAD_INPUT;
+  if (a_bytes) *a_bytes = m->A.col16 ? 2 : 4;
+  if (t_bytes) *t_bytes = m->has_T ? (m->T.col16 ? 2 : 4) : 0;
   return KS_OK;
 }
 

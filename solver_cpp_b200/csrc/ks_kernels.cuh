@@ -101,46 +101,66 @@ inline void launch_k(ks_ctx *ctx, void (*kern)(KArgs...), dim3 grid, dim3 block,
 }
 
 template <class MT>
-inline CsrT<MT> tview(const CsrDev &A);
+inline const MT *values_of(const CsrDev &A);
 template <>
-inline CsrT<double> tview<double>(const CsrDev &A) {
-  return {A.ptr, A.col, A.val, A.rbi, A.nrb, A.n};
+inline const double *values_of<double>(const CsrDev &A) {
+  return A.val;
 }
 template <>
-inline CsrT<float> tview<float>(const CsrDev &A) {
-  return {A.ptr, A.col, A.val32, A.rbi, A.nrb, A.n};
+inline const float *values_of<float>(const CsrDev &A) {
+  return A.val32;
 }
 template <>
-inline CsrT<__nv_bfloat16> tview<__nv_bfloat16>(const CsrDev &A) {
-  return {A.ptr, A.col, A.val16, A.rbi, A.nrb, A.n};
+inline const __nv_bfloat16 *values_of<__nv_bfloat16>(const CsrDev &A) {
+  return A.val16;
+}
+
+template <class MT, class IT>
+inline CsrT<MT, IT> tview(const CsrDev &A) {
+  const IT *col;
+  if constexpr (sizeof(IT) == 2)
+    col = A.col16;
+  else
+    col = A.col;
+  return {A.ptr, col, values_of<MT>(A), A.rbi, A.nrb, A.n};
 }
 
 // One-time per device and instantiation: opt in to the stage buffers' shared
 // memory and record how many CTAs fit on an SM.
-template <int NV, class MT, class GX, class Epi>
+template <int NV, class MT, class IT, class GX, class Epi>
 inline int spmv_tma_ctas_per_sm(int device) {
   static std::atomic<unsigned long long> configured{0};
   static int per_sm[64] = {0};
   const unsigned long long bit = 1ull << (device & 63);
   if (!(configured.load() & bit)) {
-    auto fn = spmv_tma_kernel<NV, MT, GX, Epi>;
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)spmv_tma_smem<MT>());
+    auto fn = spmv_tma_kernel<NV, MT, IT, GX, Epi>;
+    constexpr int smem = (int)spmv_tma_smem<MT, IT>();
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, spmv_tma_smem<MT>()) != cudaSuccess || b < 1)
-      b = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kThreads, smem) != cudaSuccess || b < 1) b = 1;
     per_sm[device & 63] = b;
     configured.fetch_or(bit);
   }
   return per_sm[device & 63];
 }
 
+template <int NV, class MT, class IT, class GX, class Epi>
+inline void launch_spmv_i(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
+                          int slot) {
+  const int per_sm = spmv_tma_ctas_per_sm<NV, MT, IT, GX, Epi>(ctx->device);
+  const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
+  launch_k(ctx, spmv_tma_kernel<NV, MT, IT, GX, Epi>, dim3(grid), dim3(kThreads), spmv_tma_smem<MT, IT>(),
+           tview<MT, IT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err);
+}
+
+// 16-bit column offsets when the matrix has them, else int32 columns.
 template <int NV, class MT, class GX, class Epi>
 inline void launch_spmv_g(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
                           int slot = 0) {
-  const int per_sm = spmv_tma_ctas_per_sm<NV, MT, GX, Epi>(ctx->device);
-  const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
-  launch_k(ctx, spmv_tma_kernel<NV, MT, GX, Epi>, dim3(grid), dim3(kThreads), spmv_tma_smem<MT>(), tview<MT>(A), g0,
-           g1, epi, stop, red_of(ctx, slot), ctx->d_err);
+  if (A.col16)
+    launch_spmv_i<NV, MT, short, GX, Epi>(ctx, A, g0, g1, epi, stop, slot);
+  else
+    launch_spmv_i<NV, MT, int, GX, Epi>(ctx, A, g0, g1, epi, stop, slot);
 }
 
 template <class MT, class XT, class Epi>

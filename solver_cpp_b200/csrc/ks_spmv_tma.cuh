@@ -4,7 +4,8 @@
 // and <= kNnzPerBlock nonzeros per block; a longer row is a block of its own)
 // through a two-stage shared-memory pipeline. One thread issues, per block,
 // three 1-D bulk async copies (cp.async.bulk, completing on an mbarrier) of
-// the block's column indices, values and row offsets, two blocks ahead of the
+// the block's column indices (int32, or int16 offsets from the row where the
+// matrix allows them), values and row offsets, two blocks ahead of the
 // compute, with an evict-first L2 policy so the Krylov vectors keep their
 // place in L2. All threads then gather x and sum rows out of shared memory:
 // one thread per row, in index order from 0.0 with separately rounded
@@ -29,16 +30,28 @@ constexpr int kStageElems = kNnzPerBlock + 16;  // values / columns per stage
 constexpr int kStagePtr = kRowsPerBlock + 8;    // row offsets per stage
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
 
-template <class MT>
+template <class MT, class IT>
 struct StageBuf {
   MT val[kStageElems];
-  int col[kStageElems];
+  IT col[kStageElems];
   int ptr[kStagePtr];
 };
 
-template <class MT>
-constexpr int granule() {  // elements per 16 bytes for both col and val copies
-  return sizeof(MT) >= 4 ? 4 : 8;
+// Elements per 16 bytes of the narrower of the value and index arrays: a row
+// block's copies start and end on multiples of this so both stay 16-byte aligned.
+template <class MT, class IT>
+constexpr int granule() {
+  return 16 / (sizeof(MT) < sizeof(IT) ? sizeof(MT) : sizeof(IT));
+}
+
+// Column of a stored index: int32 indices are the column itself, int16 ones
+// the offset of the column from the row.
+template <class IT>
+__device__ __forceinline__ int col_of(int row, IT v) {
+  if constexpr (sizeof(IT) == 2)
+    return row + (int)v;
+  else
+    return v;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -107,10 +120,10 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-template <class MT>
+template <class MT, class IT>
 struct CsrT {
   const int *__restrict__ ptr;   // n+1 offsets, padded to n+1+kPad
-  const int *__restrict__ col;   // nnz, padded
+  const IT *__restrict__ col;    // nnz, padded (int: column; short: column - row)
   const MT *__restrict__ val;    // nnz, padded
   const int4 *__restrict__ rbi;  // per row block: r0, r1, j0, j1
   int nrb;
@@ -118,16 +131,16 @@ struct CsrT {
 };
 
 // Issue the copies of row block `info` into stage buffer `sb`.
-template <class MT>
-__device__ __forceinline__ void stage_issue(const CsrT<MT> &A, int4 info, StageBuf<MT> *sb, uint64_t *bar,
-                                            uint64_t pol) {
-  constexpr int G = granule<MT>();
+template <class MT, class IT>
+__device__ __forceinline__ void stage_issue(const CsrT<MT, IT> &A, int4 info, StageBuf<MT, IT> *sb,
+                                            uint64_t *bar, uint64_t pol) {
+  constexpr int G = granule<MT, IT>();
   const int a0 = info.z & ~(G - 1);
   const int a1 = (info.w + G - 1) & ~(G - 1);
   const int p0 = info.x & ~3;
   const int p1 = (info.y + 1 + 3) & ~3;
   const uint32_t vb = (uint32_t)(a1 - a0) * sizeof(MT);
-  const uint32_t cb = (uint32_t)(a1 - a0) * sizeof(int);
+  const uint32_t cb = (uint32_t)(a1 - a0) * sizeof(IT);
   const uint32_t pb = (uint32_t)(p1 - p0) * sizeof(int);
   mbar_expect_tx(bar, vb + cb + pb);
   if (vb) bulk_g2s(sb->val, A.val + a0, vb, bar, pol);
@@ -135,7 +148,6 @@ __device__ __forceinline__ void stage_issue(const CsrT<MT> &A, int4 info, StageB
   bulk_g2s(sb->ptr, A.ptr + p0, pb, bar, pol);
 }
 
-template <class MT>
 __device__ __forceinline__ bool is_long(int4 info) {
   return info.w - info.z > kNnzPerBlock;
 }
@@ -154,15 +166,16 @@ struct GPtr {
 
 // NV right-hand vectors (1, or 2 for the k-skip matrix powers), gathered by
 // GX. Epi::row(r, y) for NV = 1, Epi::row(r, y0, y1) for NV = 2 (with acc).
-template <int NV, class MT, class GX, class Epi>
+template <int NV, class MT, class IT, class GX, class Epi>
 __global__ void __launch_bounds__(kThreads)
-    spmv_tma_kernel(CsrT<MT> A, GX gx0, GX gx1, Epi epi, Stop stop, Red red, int *err) {
+    spmv_tma_kernel(CsrT<MT, IT> A, GX gx0, GX gx1, Epi epi, Stop stop, Red red, int *err) {
   using AT = typename Epi::acc_t;
+  using SB = StageBuf<MT, IT>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  StageBuf<MT> *stage = reinterpret_cast<StageBuf<MT> *>(smem_raw);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + kStages * sizeof(StageBuf<MT>));
+  SB *stage = reinterpret_cast<SB *>(smem_raw);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + kStages * sizeof(SB));
   constexpr int ND = Epi::ND > 0 ? Epi::ND : 1;
-  constexpr int G = granule<MT>();
+  constexpr int G = granule<MT, IT>();
   double acc[ND];
 #pragma unroll
   for (int d = 0; d < ND; d++) acc[d] = 0.0;
@@ -182,7 +195,7 @@ __global__ void __launch_bounds__(kThreads)
   if (tid == 0) {
     while (staged < kStages && prod_blk < A.nrb) {
       const int4 info = A.rbi[prod_blk];
-      if (!is_long<MT>(info)) {
+      if (!is_long(info)) {
         stage_issue(A, info, &stage[staged % kStages], &bars[staged % kStages], pol);
         staged++;
       }
@@ -202,7 +215,7 @@ __global__ void __launch_bounds__(kThreads)
   for (int blk = blockIdx.x; blk < A.nrb && !failed; blk += gridDim.x) {
     const int4 info = A.rbi[blk];
     const int r0 = info.x, nrows = info.y - info.x, j0 = info.z, nnz = info.w - info.z;
-    if (is_long<MT>(info)) {
+    if (is_long(info)) {
       // whole CTA on one long row, straight from global memory
       double v[NV];
 #pragma unroll
@@ -210,7 +223,7 @@ __global__ void __launch_bounds__(kThreads)
         const GX &gu = u == 0 ? g0 : g1;
         AT s = (AT)0;
         for (int j = j0 + tid; j < info.w; j += kThreads)
-          s += mval<AT>(A.val[j]) * gu.template get<AT>(A.col[j]);
+          s += mval<AT>(A.val[j]) * gu.template get<AT>(col_of(r0, A.col[j]));
         v[u] = (double)s;
       }
       block_sum<NV>(v);
@@ -233,17 +246,18 @@ __global__ void __launch_bounds__(kThreads)
       if (tid == 0) atomicExch(err, 1);
       break;
     }
-    const StageBuf<MT> *sb = &stage[s];
+    const SB *sb = &stage[s];
     const int a0 = j0 & ~(G - 1);
     const int p0 = r0 & ~3;
     if (nnz <= 16 * nrows) {
       if (tid < nrows) {
+        const int row = r0 + tid;
         const int rs = sb->ptr[r0 - p0 + tid] - a0, re = sb->ptr[r0 - p0 + tid + 1] - a0;
         AT y0 = (AT)0, y1 = (AT)0;
 #pragma unroll 4
         for (int e = rs; e < re; e++) {
           const AT a = mval<AT>(sb->val[e]);
-          const int c = sb->col[e];
+          const int c = col_of(row, sb->col[e]);
           y0 = add_rn(y0, mul_rn(a, g0.template get<AT>(c)));
           if constexpr (NV == 2) y1 = add_rn(y1, mul_rn(a, g1.template get<AT>(c)));
         }
@@ -259,7 +273,7 @@ __global__ void __launch_bounds__(kThreads)
         AT y0 = (AT)0, y1 = (AT)0;
         for (int e = rs + lane; e < re; e += 32) {
           const AT a = mval<AT>(sb->val[e]);
-          const int c = sb->col[e];
+          const int c = col_of(r0 + rr, sb->col[e]);
           y0 += a * g0.template get<AT>(c);
           if constexpr (NV == 2) y1 += a * g1.template get<AT>(c);
         }
@@ -283,7 +297,7 @@ __global__ void __launch_bounds__(kThreads)
       while (prod_blk < A.nrb) {
         const int4 nx = A.rbi[prod_blk];
         prod_blk += gridDim.x;
-        if (!is_long<MT>(nx)) {
+        if (!is_long(nx)) {
           fence_proxy_async_smem();
           stage_issue(A, nx, &stage[staged % kStages], &bars[staged % kStages], pol);
           staged++;
@@ -303,9 +317,9 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <class MT>
+template <class MT, class IT>
 constexpr size_t spmv_tma_smem() {
-  return kStages * sizeof(StageBuf<MT>) + kStages * sizeof(uint64_t) + 16;
+  return kStages * sizeof(StageBuf<MT, IT>) + kStages * sizeof(uint64_t) + 16;
 }
 
 }  // namespace ks

@@ -36,10 +36,13 @@ def ragged_matrix(n=6000, seed=0):
 PROBLEMS = [("poisson2d", 64), ("poisson3d", 20), ("convdiff3d", 17), ("varcoef3d", 13), ("varcoef2d", 40)]
 
 
+@pytest.mark.parametrize("index32", [False, True])
 @pytest.mark.parametrize("prob,grid", PROBLEMS)
-def test_spmv_fp64_bitwise_equals_reference_order(ks, ctx, oracle, prob, grid):
+def test_spmv_fp64_bitwise_equals_reference_order(ks, ctx, oracle, prob, grid, index32):
     A, b, _ = config_problem(prob, grid)
-    M = ctx.matrix(A, transpose=True)
+    M = ctx.matrix(A, transpose=True, index32=index32)
+    info = M.info()
+    assert info["index_bytes"] == info["t_index_bytes"] == (4 if index32 else 2)
     x = np.random.default_rng(1).standard_normal(A.n)
     X, Y = ctx.vector(x), ctx.vector(n=A.n)
     ks.spmv(M, X, Y)
@@ -86,10 +89,77 @@ def test_spmv_low_precision_values(ks, ctx, values, tol):
     M = ctx.matrix(A, fp32=True, bf16=True)
     x = np.random.default_rng(4).standard_normal(A.n).astype(np.float32)
     X, Y = ctx.vector(x, dtype=ks.FP32), ctx.vector(n=A.n, dtype=ks.FP32)
-    ks.spmv(M, X, Y, values=ks.FP32 if values == "fp32" else ks.BF16)
+    vt = ks.FP32 if values == "fp32" else ks.BF16
+    ks.spmv(M, X, Y, values=vt)
     ref = A.to_scipy() @ x.astype(np.float64)
     absrow = abs(A.to_scipy()) @ np.abs(x.astype(np.float64))
-    assert np.all(np.abs(Y.numpy() - ref) <= tol * absrow + 1e-30)
+    y = Y.numpy()
+    assert np.all(np.abs(y - ref) <= tol * absrow + 1e-30)
+    # the 16-bit column offsets change nothing in the sums
+    M32 = ctx.matrix(A, fp32=True, bf16=True, index32=True)
+    assert M.info()["index_bytes"] == 2 and M32.info()["index_bytes"] == 4
+    ks.spmv(M32, X, Y, values=vt)
+    assert np.array_equal(Y.numpy(), y)
+
+
+def offset_matrix(n, up, down):
+    """Rows i with the diagonal and columns i + up and i - down where they
+    exist: A's column offsets reach +up and -down, those of A^T +down and -up."""
+    rows = []
+    for i in range(n):
+        c = [j for j in (i - down, i, i + up) if 0 <= j < n]
+        rows.append(c)
+    ptr = np.zeros(n + 1, dtype=np.int32)
+    ptr[1:] = np.cumsum([len(c) for c in rows])
+    col = np.concatenate([np.array(c, dtype=np.int32) for c in rows])
+    val = np.random.default_rng(n + up + down).standard_normal(col.shape[0])
+    return CSR(ptr, col, val)
+
+
+@pytest.mark.parametrize("up,down,a_bytes,t_bytes",
+                         [(32767, 32767, 2, 2), (32767, 32768, 2, 4), (32768, 32767, 4, 2), (40000, 40000, 4, 4)])
+def test_spmv_column_offsets_at_int16_limits(ks, ctx, oracle, up, down, a_bytes, t_bytes):
+    A = offset_matrix(70000, up, down)
+    M = ctx.matrix(A, transpose=True)
+    info = M.info()
+    assert (info["index_bytes"], info["t_index_bytes"]) == (a_bytes, t_bytes)
+    x = np.random.default_rng(5).standard_normal(A.n)
+    X, Y = ctx.vector(x), ctx.vector(n=A.n)
+    P = oracle.Problem(A)
+    ks.spmv(M, X, Y)
+    assert np.array_equal(Y.numpy(), oracle.spmv(P, x))
+    ks.spmv(M, X, Y, trans=True)
+    assert np.array_equal(Y.numpy(), oracle.spmv(P, x, transpose=True))
+
+
+def test_device_upload_checks_columns(ks, ctx):
+    import ctypes as C
+
+    import torch
+
+    from solver_cpp_b200 import _abi
+
+    A, _, _ = config_problem("poisson2d", 30)
+    dev = torch.device("cuda", 0)
+    ptr = torch.from_numpy(A.ptr.astype(np.int32)).to(dev)
+    col = torch.from_numpy(A.col.astype(np.int32)).to(dev)
+    val = torch.from_numpy(A.val.astype(np.float64)).to(dev)
+    torch.cuda.synchronize()
+    L = ks.lib()
+    h = C.c_void_p()
+    st = L.ks_csr_upload_device(ctx.handle, A.n, A.nnz, C.c_void_p(ptr.data_ptr()), C.c_void_p(col.data_ptr()),
+                                C.c_void_p(val.data_ptr()), 0, C.byref(h))
+    assert st == _abi.KS_OK
+    a, t = C.c_int(), C.c_int()
+    assert L.ks_mat_index_bytes(h, C.byref(a), C.byref(t)) == _abi.KS_OK and (a.value, t.value) == (2, 0)
+    assert L.ks_mat_destroy(h) == _abi.KS_OK
+    col[17] = A.n  # one column out of range
+    torch.cuda.synchronize()
+    h = C.c_void_p()
+    st = L.ks_csr_upload_device(ctx.handle, A.n, A.nnz, C.c_void_p(ptr.data_ptr()), C.c_void_p(col.data_ptr()),
+                                C.c_void_p(val.data_ptr()), 0, C.byref(h))
+    assert st == _abi.KS_BAD_INPUT and not h.value
+    assert b"out of range" in L.ks_last_error(ctx.handle)
 
 
 def test_dot_nrm2_axpy(ks, ctx, oracle):
