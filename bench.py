@@ -43,9 +43,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-def _w(problem, grid, outer, params, inner="NONE", plain=None, ref_args=(), spmv_values="fp64", transpose=False):
+def _w(problem, grid, outer, params, inner="NONE", plain=None, ref_args=(), spmv_values="fp64", transpose=False,
+       adjoint=False):
     return dict(problem=problem, grid=grid, outer=outer, inner=inner, params=params, plain=plain,
-                ref_args=list(ref_args), spmv_values=spmv_values, transpose=transpose)
+                ref_args=list(ref_args), spmv_values=spmv_values, transpose=transpose, adjoint=adjoint)
 
 
 _VP20 = dict(E=1e-10, L=10000, l=20, e=1e-30)
@@ -71,6 +72,10 @@ WORKLOADS = {
                         ref_args=["-S", "kskipbicg", "-K", "2", "-E", "1e-10"]),
     "c3_gcr30": _w("convdiff3d", 128, "GCR", dict(E=1e-10, L=10000, R=30),
                    ref_args=["-S", "gcr", "-R", "30", "-E", "1e-10"]),
+    # adjoint gradients of L = 1/2 |x - x*|^2 on the 512^2 systems: one step is
+    # the forward solve, the adjoint solve on A^T and the pattern gather
+    "c5_adjoint_cg": _w("varcoef2d", 512, "CG", dict(E=1e-12, L=40000), transpose=True, adjoint=True),
+    "c5_adjoint_bicg": _w("convdiff2d", 512, "BICG", dict(E=1e-12, L=40000), transpose=True, adjoint=True),
     "c3_gmres30": _w("convdiff3d", 128, "GMRES", dict(E=1e-10, L=10000, R=30),
                      ref_args=["-S", "gmres", "-R", "30", "-E", "1e-10"]),
 }
@@ -195,8 +200,22 @@ def run_ours(args, world, rank, local):
     X = ctx.vector(n=n)
     launches0 = ks.lib().ks_ctx_launches(ctx.handle)
 
+    adj = None
+    if W.get("adjoint"):  # loss 1/2 |x - x*|^2 with x* ~ N(0,1) (seed 6)
+        XS = ctx.vector(np.random.default_rng(6).standard_normal(n))
+        adj = dict(G=ctx.vector(n=n), GB=ctx.vector(n=n), GV=ctx.vector(n=nnz))
+
     def one(outer, inner, params):
-        return ks.solve(ctx, M, outer, B, inner=inner, x=X, **params)
+        r = ks.solve(ctx, M, outer, B, inner=inner, x=X, **params)
+        if adj is not None and params is W["params"]:
+            # g = x - x*, then the adjoint solve on A^T and the pattern gather
+            adj["G"].fill(0.0)
+            ks.axpy(1.0, X, adj["G"])
+            ks.axpy(-1.0, XS, adj["G"])
+            st, _ = ks.adjoint_grad(ctx, M, outer, X, adj["G"], adj["GB"], adj["GV"], **params)
+            if st != 0:
+                raise RuntimeError(f"adjoint solve status {st}")
+        return r
 
     for _ in range(args.warmup):
         r = one(W["outer"], W["inner"], W["params"])
@@ -295,7 +314,7 @@ def run_ours(args, world, rank, local):
 
     # end to end through the public host API: pinned b -> device -> x -> host
     e2e = None
-    if not args.no_e2e:
+    if not args.no_e2e and adj is None:
         bh = torch.from_numpy(b).pin_memory().numpy()
         xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
         import ctypes as C
@@ -323,7 +342,7 @@ def run_ours(args, world, rank, local):
                "d2h_bytes_per_step": 8 * n + 16 * int(rep.hist_len) + 64}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and adj is None:
         cpu = cpu_baseline_port(A, b, W, res)
 
     out = {
@@ -336,7 +355,8 @@ def run_ours(args, world, rank, local):
         "config": {"workload": args.workload, "problem": W["problem"], "grid": W["grid"], "n": n, "nnz": nnz,
                    "method": W["outer"] + ("/" + W["inner"] if W["inner"] != "NONE" else ""),
                    "params": W["params"], "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (matrix >= 175 MB)"},
+                   "l2": "inputs larger than L2 (matrix >= 175 MB)" if nnz * 12 > 126e6 else
+                         "working set fits in the 126 MB L2 (no flush between steps)"},
         "result": {"status": res.status, "loop": res.loop, "true_rel_res": res.true_rel_res,
                    "inner_calls": res.inner_calls},
         "plain_fp64": plain,
@@ -492,6 +512,54 @@ def spmv_only(args):
     ctx.close()
 
 
+def ortho_only(args):
+    """The GMRES orthogonalisation kernels alone on vectors of the workload's
+    length: h = V^T w over k basis vectors (block dot) and w -= V h (block
+    AXPY), through ks_block_dot / ks_block_axpy, timed with CUDA events.
+    Bytes: the block dot reads k + 1 vectors, the block AXPY reads k + 1 and
+    writes 1. Each call also moves the k coefficients between host and
+    device (block dot: device -> host, block AXPY: host -> device)."""
+    import torch
+
+    import solver_cpp_b200 as ks
+    from solver_cpp_b200.matrices import config_problem
+
+    W = WORKLOADS[args.workload]
+    A, _, _ = config_problem(W["problem"], W["grid"])
+    n = A.n
+    ctx = ks.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    peak, kind = load_peaks()
+    kmax = max(args.ortho_only)
+    V = ctx.vector(n=n * kmax)
+    V.fill(1.0 / math.sqrt(n))
+    w = ctx.vector(np.random.default_rng(0).standard_normal(n))
+    for k in args.ortho_only:
+        h = ks.block_dot(V, n, k, w)
+        for _ in range(args.warmup):
+            ks.block_dot(V, n, k, w)
+            ks.block_axpy(V, n, k, h * 0.0, w)
+        torch.cuda.synchronize()
+        out = {"kernel": "gmres_orthogonalisation", "workload": args.workload, "n": n, "k": k, "peak": peak,
+               "peak_kind": kind}
+        for name, fn, nbytes in (("block_dot", lambda: ks.block_dot(V, n, k, w), (k + 1) * 8 * n),
+                                 ("block_axpy", lambda: ks.block_axpy(V, n, k, h * 0.0, w), (k + 2) * 8 * n)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            gbs = nbytes / (ms / 1e3) / 1e9
+            out[name] = {"ms": round(ms, 4), "bytes": nbytes, "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+        print(json.dumps(out), flush=True)
+    V.close()
+    w.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -505,9 +573,14 @@ def main():
     ap.add_argument("--spmv-only", choices=["fp64", "fp32", "bf16"], default=None,
                     help="time only the SpMV kernel on the workload's matrix (profiling)")
     ap.add_argument("--index32", action="store_true", help="with --spmv-only: int32 column indices")
+    ap.add_argument("--ortho-only", type=int, nargs="+", default=None, metavar="K",
+                    help="time only the GMRES block dot / block AXPY over K basis vectors (profiling)")
     args = ap.parse_args()
     if args.spmv_only:
         spmv_only(args)
+        return
+    if args.ortho_only:
+        ortho_only(args)
         return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))

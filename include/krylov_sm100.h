@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define KS_ABI_VERSION 1
+#define KS_ABI_VERSION 2
 
 typedef enum {
   KS_OK = 0,              /* converged / success (reference solve() == 0)      */
@@ -220,6 +220,9 @@ typedef struct {
                                 recurrences and GMRES assembly; 0: corrected */
   int32_t transpose;       /* 1: solve A^T x = b (adjoint solves)            */
   int32_t poll_interval;   /* iterations in flight between host polls; 0=auto */
+  int32_t x_update;        /* CG, CR, BiCG: 0 auto, 1 x += alpha p every
+                              iteration, 2 deferred through a ring of 32
+                              directions (same x bit for bit)              */
 } ks_params;
 
 typedef struct {
@@ -281,6 +284,41 @@ ks_status ks_crs_read(const char *dir, int64_t n, int64_t nnz, int32_t *ptr,
 ks_status ks_crs_write(const char *dir, int64_t n, int64_t nnz,
                        const int32_t *ptr, const int32_t *col,
                        const double *val, const double *b, const double *x);
+
+/* -------------------------------------------------------------- multi-GPU */
+
+/* Row partition for a solve split over `nranks` GPUs (host only): contiguous
+ * blocks row_start[0] = 0 <= ... <= row_start[nranks] = n with every inner
+ * boundary a multiple of `align` rows (for a grid matrix: one plane). With
+ * align = 1 and two ranks the first block has ceil(n/2) rows, the reference's
+ * two-GPU split (solver_collection.cpp:1022-1031). */
+ks_status ks_partition_rows(int64_t n, int nranks, int64_t align, int64_t *row_start);
+/* The contiguous column window [lo, hi) that rows r0..r1-1 read, lo <= r0,
+ * hi >= r1 (host only). ptr holds r1 - r0 + 1 offsets (any base) and col the
+ * global column indices of those rows. A rank keeps x over its window. */
+ks_status ks_halo_window(int64_t r0, int64_t r1, const int32_t *ptr, const int32_t *col,
+                         int64_t *lo, int64_t *hi);
+/* The exchange before every SpMV of rank `rank` (host only), from every
+ * rank's rows (row_start) and window: for each peer q its own rows
+ * [send_lo[q], send_hi[q]) go to q and x[recv_lo[q], recv_hi[q]) comes from
+ * q; empty ranges have lo == hi. Replaces the reference's host gather of x
+ * around each split SpMV (cudaFunction.cu:1942-2226). */
+ks_status ks_halo_plan(int nranks, int rank, const int64_t *row_start, const int64_t *win_lo,
+                       const int64_t *win_hi, int64_t *send_lo, int64_t *send_hi,
+                       int64_t *recv_lo, int64_t *recv_hi);
+
+/* Matrix Market coordinate files: the input source the reference declares
+ * (-P / -D / -M, solver_collection.cpp:278-286,505-601) but never reads.
+ * Fields real / double / integer / pattern (pattern entries are 1.0);
+ * symmetry general / symmetric / skew-symmetric (mirrored to both
+ * triangles); square matrices only. The CSR rows are ordered by column and
+ * entries repeated at one position are summed in file order. The header call
+ * parses the file and returns n and the CSR nnz; ks_mm_read fills
+ * caller-allocated ptr[n+1], col[nnz], val[nnz]. Complex fields and the dense
+ * array format give KS_BAD_INPUT, a missing file KS_IO_ERROR. */
+ks_status ks_mm_read_header(const char *file, int64_t *n, int64_t *nnz);
+ks_status ks_mm_read(const char *file, int64_t n, int64_t nnz, int32_t *ptr,
+                     int32_t *col, double *val);
 
 #ifdef __cplusplus
 }

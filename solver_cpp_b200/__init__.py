@@ -374,3 +374,44 @@ def crs_read(directory: str):
     _check(lib().ks_crs_read(directory.encode(), n.value, nnz.value, _ptr(ptr), _ptr(col), _ptr(val), _ptr(b),
                              _ptr(x)), None, "crs_read")
     return CSR(ptr, col, val), b, x
+
+
+def mm_read(file: str) -> CSR:
+    """Read a Matrix Market coordinate file (real / integer / pattern;
+    general / symmetric / skew-symmetric) into CSR with the library's reader."""
+    n, nnz = C.c_int64(), C.c_int64()
+    _check(lib().ks_mm_read_header(file.encode(), C.byref(n), C.byref(nnz)), None, "mm_read_header")
+    ptr = np.zeros(n.value + 1, dtype=np.int32)
+    col = np.zeros(max(nnz.value, 1), dtype=np.int32)
+    val = np.zeros(max(nnz.value, 1))
+    _check(lib().ks_mm_read(file.encode(), n.value, nnz.value, _ptr(ptr), _ptr(col), _ptr(val)), None, "mm_read")
+    return CSR(ptr, col[:nnz.value], val[:nnz.value])
+
+
+# ----------------------------------------------------------------- multi-GPU plan
+def partition_rows(n: int, nranks: int, align: int = 1) -> np.ndarray:
+    """Row blocks of a solve split over nranks GPUs (ks_partition_rows)."""
+    rs = np.zeros(nranks + 1, dtype=np.int64)
+    _check(lib().ks_partition_rows(n, nranks, align, _ptr(rs)), None, "partition_rows")
+    return rs
+
+
+def halo_window(A: CSR, r0: int, r1: int):
+    """Column window [lo, hi) that rows r0..r1-1 of A read (ks_halo_window)."""
+    lo, hi = C.c_int64(), C.c_int64()
+    ptr = np.ascontiguousarray(A.ptr[r0:r1 + 1], dtype=np.int32)
+    col = np.ascontiguousarray(A.col[A.ptr[r0]:A.ptr[r1]], dtype=np.int32)
+    _check(lib().ks_halo_window(r0, r1, _ptr(ptr), _ptr(col) if col.size else None, C.byref(lo), C.byref(hi)),
+           None, "halo_window")
+    return lo.value, hi.value
+
+
+def halo_plan(row_start, win_lo, win_hi, rank: int):
+    """Per-peer send and receive row ranges of `rank` (ks_halo_plan)."""
+    P = len(row_start) - 1
+    rs = np.ascontiguousarray(row_start, dtype=np.int64)
+    lo = np.ascontiguousarray(win_lo, dtype=np.int64)
+    hi = np.ascontiguousarray(win_hi, dtype=np.int64)
+    out = [np.zeros(P, dtype=np.int64) for _ in range(4)]
+    _check(lib().ks_halo_plan(P, rank, _ptr(rs), _ptr(lo), _ptr(hi), *[_ptr(o) for o in out]), None, "halo_plan")
+    return {"send": list(zip(out[0], out[1])), "recv": list(zip(out[2], out[3]))}

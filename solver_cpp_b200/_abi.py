@@ -43,6 +43,9 @@ MAT_BF16 = 4
 MAT_INDEX32 = 8
 
 
+ABI_VERSION = 2  # KS_ABI_VERSION of the header these structures mirror
+
+
 class Params(C.Structure):
     _fields_ = [
         ("outer_maxloop", C.c_int64), ("outer_eps", C.c_double), ("outer_restart", C.c_int64),
@@ -50,7 +53,7 @@ class Params(C.Structure):
         ("inner_maxloop", C.c_int64), ("inner_eps", C.c_double), ("inner_restart", C.c_int64),
         ("inner_kskip", C.c_int32), ("inner_fix", C.c_int32),
         ("inner_precision", C.c_int32), ("reference_defects", C.c_int32),
-        ("transpose", C.c_int32), ("poll_interval", C.c_int32),
+        ("transpose", C.c_int32), ("poll_interval", C.c_int32), ("x_update", C.c_int32),
     ]
 
 
@@ -118,6 +121,11 @@ SIGNATURES = [
     ("ks_pattern_grad", C.c_int, [_VP, _VP, _VP, _VP]),
     ("ks_crs_read_header", C.c_int, [C.c_char_p, _PI64, _PI64]),
     ("ks_crs_read", C.c_int, [C.c_char_p, _I64, _I64, _VP, _VP, _VP, _VP, _VP]),
+    ("ks_partition_rows", C.c_int, [_I64, C.c_int, _I64, _VP]),
+    ("ks_halo_window", C.c_int, [_I64, _I64, _VP, _VP, _PI64, _PI64]),
+    ("ks_halo_plan", C.c_int, [C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("ks_mm_read_header", C.c_int, [C.c_char_p, _PI64, _PI64]),
+    ("ks_mm_read", C.c_int, [C.c_char_p, _I64, _I64, _VP, _VP, _VP]),
     ("ks_crs_write", C.c_int, [C.c_char_p, _I64, _I64, _VP, _VP, _VP, _VP, _VP]),
 ]
 
@@ -142,5 +150,8 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.ks_abi_version() != ABI_VERSION:  # the structures above would not match
+        raise LibraryMissing(f"{LIB_NAME} has ABI version {lib.ks_abi_version()}, the binding expects "
+                             f"{ABI_VERSION}; rebuild it with `make -C solver_cpp_b200/csrc`")
     _lib = lib
     return lib

@@ -11,6 +11,7 @@
 // compatibility: the solve always runs on the GPU and vectors never leave it.
 // Added options: --precision fp64|fp32|bf16 (inner solve of VP methods),
 // --reference-defects, --device N.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -44,7 +45,8 @@ struct Opt {
 const char *kUsage =
     "usage: Solver -S <method> -m <matrix> [options]\n"
     "  -N --L1_Dir_Name (Matrix)  -p --CRS_Path (../)  -d --CRS_Dir_Name (CRS)  -m --CRS_Matrix_Name\n"
-    "  -P --MM_Path  -D --MM_Dir_Name  -M --MM_Matrix_Name   -t --Openmp_Thread (8, unused on GPU)\n"
+    "  -P --MM_Path (../)  -D --MM_Dir_Name (MM)  -M --MM_Matrix_Name: <P>/<N>/<D>/<M>/<M>.mtx, b = A*1\n"
+    "  -t --Openmp_Thread (8, unused on GPU)\n"
     "  -S --OuterSolver  -L --OuterMaxLoop (10000)  -E --OuterEps (1e-8)  -R --OuterRestart (1000)\n"
     "  -K --OuterKskip (2)  -F --OuterFix (2)\n"
     "  -s --InnerSolver  -l --InnerMaxLoop (50)  -e --InnerEps (1e-1)  -r --InnerRestart (1000)\n"
@@ -182,8 +184,6 @@ int main(int argc, char **argv) {
   if (o.outer.empty()) die(std::string("[X]OuterSolver (-S) is required\n") + kUsage);
   if (o.mm_name == "NONE" && o.crs_name == "NONE") die("[X]Must set one input source");
   if (o.mm_name != "NONE" && o.crs_name != "NONE") die("[X]Only can set one input source");
-  if (o.mm_name != "NONE")
-    die("[X]Matrix Market input is not supported (the reference reads CRS files only)");
   const ks_solver outer = to_solver(o.outer);
   if (outer == KS_NONE) die("[X]OuterSolverName can not found in List");
   const ks_solver inner = o.inner == "NO" ? KS_NONE : to_solver(o.inner);
@@ -194,16 +194,41 @@ int main(int argc, char **argv) {
   else if (o.precision == "bf16") prec = KS_BF16;
   else if (o.precision != "fp64") die("--precision must be fp64, fp32 or bf16");
 
-  // collection::checkCMD / checkCRSMatrix / readMatrix (solver_collection.cpp:391-828)
-  const std::string dir = o.crs_path + "/" + o.l1 + "/" + o.crs_dir + "/" + o.crs_name;
-  if (!is_dir(dir)) die("[X]Error no CRS files Dir -> " + dir);
   int64_t n = 0, nnz = 0;
-  if (ks_crs_read_header(dir.c_str(), &n, &nnz) != KS_OK)
-    die("[X] Error in CRS files (missing, or N / M / NNZ differ between ColVal.txt, Ptr.txt, bx.txt, or N != M)");
-  std::vector<int32_t> ptr((size_t)n + 1), col((size_t)nnz);
-  std::vector<double> val((size_t)nnz), b((size_t)n), x((size_t)n);
-  if (ks_crs_read(dir.c_str(), n, nnz, ptr.data(), col.data(), val.data(), b.data(), x.data()) != KS_OK)
-    die("[X] Read CRS files fail");
+  std::vector<int32_t> ptr, col;
+  std::vector<double> val, b, x;
+  if (o.crs_name != "NONE") {
+    // collection::checkCMD / checkCRSMatrix / readMatrix (solver_collection.cpp:391-828)
+    const std::string dir = o.crs_path + "/" + o.l1 + "/" + o.crs_dir + "/" + o.crs_name;
+    if (!is_dir(dir)) die("[X]Error no CRS files Dir -> " + dir);
+    if (ks_crs_read_header(dir.c_str(), &n, &nnz) != KS_OK)
+      die("[X] Error in CRS files (missing, or N / M / NNZ differ between ColVal.txt, Ptr.txt, bx.txt, or N != M)");
+    ptr.resize((size_t)n + 1);
+    col.resize((size_t)nnz);
+    val.resize((size_t)nnz);
+    b.resize((size_t)n);
+    x.resize((size_t)n);
+    if (ks_crs_read(dir.c_str(), n, nnz, ptr.data(), col.data(), val.data(), b.data(), x.data()) != KS_OK)
+      die("[X] Read CRS files fail");
+  } else {
+    // Matrix Market source, laid out as the reference checks it
+    // (solver_collection.cpp:505-601): <P>/<N>/<D>/<M>/<M>.mtx. The file
+    // holds no right-hand side: b = A * (1, ..., 1), x0 = 0.
+    const std::string dir = o.mm_path + "/" + o.l1 + "/" + o.mm_dir + "/" + o.mm_name;
+    if (!is_dir(dir)) die("[X]Error no MM files Dir -> " + dir);
+    const std::string file = dir + "/" + o.mm_name + ".mtx";
+    const ks_status hs = ks_mm_read_header(file.c_str(), &n, &nnz);
+    if (hs != KS_OK) die("[X]Error in mm file " + file + ": " + ks_status_string(hs));
+    ptr.resize((size_t)n + 1);
+    col.resize((size_t)std::max<int64_t>(nnz, 1));
+    val.resize((size_t)std::max<int64_t>(nnz, 1));
+    if (ks_mm_read(file.c_str(), n, nnz, ptr.data(), col.data(), val.data()) != KS_OK)
+      die("[X] Read mm file fail");
+    b.assign((size_t)n, 0.0);
+    x.assign((size_t)n, 0.0);
+    for (int64_t i = 0; i < n; i++)
+      for (int32_t j = ptr[(size_t)i]; j < ptr[(size_t)i + 1]; j++) b[(size_t)i] += val[(size_t)j];
+  }
 
   const bool vp = outer == KS_VPCG || outer == KS_VPCR || outer == KS_VPGCR || outer == KS_VPGMRES ||
                   outer == KS_VPBICG;

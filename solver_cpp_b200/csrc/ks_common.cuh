@@ -197,14 +197,41 @@ __device__ __forceinline__ bool grid_sum_n(double (&v)[ND], double *partials,
   __syncthreads();
   if (!is_last) return false;
   __threadfence();
+  // Four independent running sums per thread keep four partial loads in
+  // flight; the order is still fixed.
 #pragma unroll
   for (int d = 0; d < ND; d++) {
-    double s = 0.0;
-    for (unsigned i = threadIdx.x; i < G; i += blockDim.x)
-      s += __ldcg(partials + (size_t)d * G + i);
-    v[d] = s;
+    const double *p = partials + (size_t)d * G;
+    const unsigned B = blockDim.x;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    unsigned i = threadIdx.x;
+    for (; i + 3 * B < G; i += 4 * B) {
+      s0 += __ldcg(p + i);
+      s1 += __ldcg(p + i + B);
+      s2 += __ldcg(p + i + 2 * B);
+      s3 += __ldcg(p + i + 3 * B);
+    }
+    for (; i < G; i += B) s0 += __ldcg(p + i);
+    v[d] = (s0 + s1) + (s2 + s3);
   }
   block_sum<ND>(v);
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+// Last-CTA detection without sums (a kernel that only needs one thread to run
+// a scalar step after every CTA has finished its stores).
+__device__ __forceinline__ bool grid_last(unsigned *counter) {
+  __shared__ bool is_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned G = gridDim.x * gridDim.y;
+    is_last = atomicAdd(counter, 1u) == G - 1;
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
   if (threadIdx.x == 0) *counter = 0u;
   return true;
 }
@@ -223,6 +250,7 @@ __device__ __forceinline__ bool grid_sum(double (&v)[ND], double *partials,
 struct ks_ctx {
   int device = 0;
   int num_sms = 148;
+  size_t l2_bytes = 0;  // L2 cache size of the device
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   double *partials = nullptr;   // reduction scratch

@@ -412,6 +412,7 @@ ks_status ks_ctx_create(int device, ks_ctx **out) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return fail(KS_CUDA_ERROR);
   ctx->num_sms = prop.multiProcessorCount;
+  ctx->l2_bytes = (size_t)prop.l2CacheSize;
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail(KS_CUDA_ERROR);
   ctx->stream = ctx->own_stream;

@@ -67,6 +67,80 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Tall-skinny basis combination: every element j runs a sequential chain over
+// k basis vectors (GMRES's w -= sum h_i v_i, the deferred x += sum alpha_i
+// p_i, the GMRES/GCR solution and direction updates), so the order of the
+// terms, and with it every rounding, is the reference's per-element loop.
+// Each thread walks its elements one at a time; the loads of the next chunk
+// of basis vectors are issued before the current chunk is consumed, which
+// keeps enough bytes in flight to stream the basis at HBM speed despite the
+// chain.
+// Op concept:
+//   using vt = element type; static constexpr int NB (1 or 2 bases), ND;
+//   long long ld;                               // stride between basis vectors
+//   struct St;                                  // per-element state
+//   __device__ bool active() const;             // uniform gate (device state)
+//   __device__ int count() const;               // k (may read device memory)
+//   __device__ const vt *base(int b) const;
+//   __device__ St init(long long j) const;
+//   __device__ void step(St &, int i, const vt (&v)[NB]) const;
+//   __device__ void done(long long j, const St &, double (&acc)[ND ? ND : 1]) const;
+//   __device__ void finish(const double (&sums)[ND ? ND : 1]) const;
+//   static constexpr bool kFinishOnly;          // ND == 0 and finish() still runs
+// Loads in flight per element: kBasisLoads (split over the NB bases).
+constexpr int kBasisLoads = 8;
+
+template <class Op, class = void>
+struct finish_only : std::false_type {};
+template <class Op>
+struct finish_only<Op, std::void_t<decltype(Op::kFinishOnly)>> : std::integral_constant<bool, Op::kFinishOnly> {};
+
+template <class Op>
+__global__ void __launch_bounds__(kThreads) basis_kernel(Op op, long long n, Stop stop, Red red) {
+  using VT = typename Op::vt;
+  constexpr int NB = Op::NB, C = kBasisLoads / NB;
+  constexpr int ND = Op::ND > 0 ? Op::ND : 1;
+  pdl_wait();
+  if (stop() || !op.active()) return;
+  double acc[ND];
+#pragma unroll
+  for (int d = 0; d < ND; d++) acc[d] = 0.0;
+  const int k = op.count();
+  const VT *B[NB];
+#pragma unroll
+  for (int b = 0; b < NB; b++) B[b] = op.base(b);
+  const long long ld = op.ld;
+  for (long long j = (long long)blockIdx.x * kThreads + threadIdx.x; j < n; j += (long long)gridDim.x * kThreads) {
+    typename Op::St s = op.init(j);
+    VT cur[C][NB], nxt[C][NB];
+#pragma unroll
+    for (int u = 0; u < C; u++)
+#pragma unroll
+      for (int b = 0; b < NB; b++) cur[u][b] = u < k ? B[b][(long long)u * ld + j] : (VT)0;
+    for (int i0 = 0; i0 < k; i0 += C) {
+#pragma unroll
+      for (int u = 0; u < C; u++)
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+          nxt[u][b] = i0 + C + u < k ? B[b][(long long)(i0 + C + u) * ld + j] : (VT)0;
+#pragma unroll
+      for (int u = 0; u < C; u++)
+        if (i0 + u < k) op.step(s, i0 + u, cur[u]);
+#pragma unroll
+      for (int u = 0; u < C; u++)
+#pragma unroll
+        for (int b = 0; b < NB; b++) cur[u][b] = nxt[u][b];
+    }
+    op.done(j, s, acc);
+  }
+  pdl_trigger();
+  if constexpr (Op::ND > 0) {
+    if (grid_sum<ND>(acc, red.partials, red.counter) && threadIdx.x == 0) op.finish(acc);
+  } else if constexpr (finish_only<Op>::value) {
+    if (grid_last(red.counter) && threadIdx.x == 0) op.finish(acc);
+  }
+}
+
 // Scalar step run by a single thread (recurrences that need no vector data).
 template <class Op>
 __global__ void scalar_kernel(Op op, Stop stop) {
@@ -180,6 +254,20 @@ inline void launch_vec(ks_ctx *ctx, long long n, const Op &op, Stop stop, int sl
   int grid = red_grid(ctx);
   if (need < grid) grid = (int)(need > 0 ? need : 1);
   launch_k(ctx, vec_kernel<Op>, dim3(grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
+}
+
+// k_hint: the number of basis vectors, or a bound when the kernel reads it
+// from the device. Short chains run one full-occupancy wave of CTAs that
+// stride over the elements, which keeps the final reduction short; long
+// chains (measured: from 64 vectors) stream faster with one thread per
+// element, the reduction's cost then being small beside the pass.
+template <class Op>
+inline void launch_basis(ks_ctx *ctx, long long n, int k_hint, const Op &op, Stop stop, int slot = 0) {
+  long long grid = (n + kThreads - 1) / kThreads;
+  const long long cap = k_hint >= 64 ? (long long)(ctx->partials_len / (Op::ND > 0 ? Op::ND : 1))
+                                     : (long long)ctx->num_sms * 8;
+  grid = std::max(1LL, std::min(grid, cap));
+  launch_k(ctx, basis_kernel<Op>, dim3((unsigned)grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
 }
 
 template <class Op>

@@ -94,7 +94,7 @@ extern "C" ks_status ks_block_dot_noalloc(const double *V, int64_t ld, int k, co
   }
   long long gx = (n + kThreads - 1) / kThreads;
   if (gx > kNoAllocGrid) gx = kNoAllocGrid;
-  dim3 grid((unsigned)gx, (unsigned)groups);
+  dim3 grid((unsigned)groups, (unsigned)gx);
   block_dot_kernel<1, double, PutArray><<<grid, kThreads, 0, st>>>(V, ld, k, w, nullptr, n, PutArray{h, 0, 1},
                                                                   Stop{nullptr, nullptr}, partials, counters);
   e = cudaGetLastError();

@@ -116,8 +116,11 @@ __global__ void pattern_grad_kernel(CsrK<double> A, const double *__restrict__ l
 
 // ------------------------------------------------------------ block (tall-skinny)
 // h[w][i] = (W_w, V_i) for i < k and NW left vectors W (1 or 2): one pass over
-// the k basis vectors V_i = V + i*ld, kBlockDotGroup of them per grid row
-// (blockIdx.y), each group reduced deterministically with its own counter.
+// the k basis vectors V_i = V + i*ld, kBlockDotGroup of them per group. The
+// group is the fast grid index (blockIdx.x) and the slice of the vectors the
+// slow one (blockIdx.y): the CTAs of every group that read the same slice of
+// W run together, so W comes from DRAM about once rather than once per group.
+// Each group is reduced deterministically with its own counter;
 // Epi::put(w, i, value) receives every result (thread 0 of the group's last CTA).
 template <int NW, class VT, class Epi>
 __global__ void __launch_bounds__(kThreads)
@@ -127,14 +130,15 @@ __global__ void __launch_bounds__(kThreads)
   pdl_wait();
   if (stop()) return;
   constexpr int G8 = kBlockDotGroup;
-  const int g = blockIdx.y;
+  const int g = blockIdx.x;
+  const int slice = blockIdx.y, nslices = gridDim.y;
   const int i0 = g * G8;
   const int cnt = min(G8, k - i0);
   double acc[NW * G8];
 #pragma unroll
   for (int q = 0; q < NW * G8; q++) acc[q] = 0.0;
-  const long long stride = (long long)gridDim.x * kThreads;
-  for (long long j = (long long)blockIdx.x * kThreads + threadIdx.x; j < n; j += stride) {
+  const long long stride = (long long)nslices * kThreads;
+  for (long long j = (long long)slice * kThreads + threadIdx.x; j < n; j += stride) {
     const double w0 = widen(W0[j]);
     const double w1 = NW > 1 ? widen(W1[j]) : 0.0;
 #pragma unroll
@@ -147,8 +151,8 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   pdl_trigger();
-  double *part = partials + (size_t)g * NW * G8 * gridDim.x;
-  if (grid_sum_n<NW * G8>(acc, part, counters + g, gridDim.x, blockIdx.x) && threadIdx.x == 0) {
+  double *part = partials + (size_t)g * NW * G8 * nslices;
+  if (grid_sum_n<NW * G8>(acc, part, counters + g, nslices, slice) && threadIdx.x == 0) {
     for (int q = 0; q < cnt; q++) {
       epi.put(0, i0 + q, acc[q]);
       if (NW > 1) epi.put(1, i0 + q, acc[G8 + q]);
@@ -172,16 +176,19 @@ inline ks_status launch_block_dot(ks_ctx *ctx, const VT *V, long long ld, int k,
   int gx = red_grid(ctx);
   const long long need = (n + kThreads - 1) / kThreads;
   if (need < gx) gx = (int)std::max<long long>(need, 1);
-  dim3 grid(gx, groups);
+  dim3 grid(groups, gx);
   launch_k(ctx, block_dot_kernel<NW, VT, Epi>, grid, dim3(kThreads), 0, V, ld, k, W0, W1, n, epi, stop,
            ctx->partials, ctx->counters + 16);
   return KS_OK;
 }
 
 // w[j] -= h[i] * V_i[j] for i = 0..k-1 in order (blas::Gmres_sp_1,
-// blas.cpp:477-488), h read from device memory; optionally out = (w, w).
+// blas.cpp:477-488), h read from device memory; optionally out = (w, w), or
+// its square root (the new basis vector's norm, GMRES). Runs in basis_kernel.
 template <class VT>
 struct BlockAxpyOp {
+  using vt = VT;
+  static constexpr int NB = 1, ND = 1;
   const VT *V;
   long long ld;
   int k;
@@ -189,15 +196,23 @@ struct BlockAxpyOp {
   long long hstride;
   VT *w;
   double *out;  // (w,w) after the update if not null
-  static constexpr int ND = 1;
-  __device__ void elem(long long j, double (&acc)[1]) const {
-    VT t = w[j];
-    for (int i = 0; i < k; i++) t = sub_rn(t, mul_rn((VT)__ldg(h + i * hstride), V[(long long)i * ld + j]));
-    w[j] = t;
-    acc[0] = add_rn(acc[0], mul_rn(widen(t), widen(t)));
+  int take_sqrt = 0;
+  struct St {
+    VT t;
+  };
+  __device__ bool active() const { return true; }
+  __device__ int count() const { return k; }
+  __device__ const VT *base(int) const { return V; }
+  __device__ St init(long long j) const { return {w[j]}; }
+  __device__ void step(St &s, int i, const VT (&v)[1]) const {
+    s.t = sub_rn(s.t, mul_rn((VT)__ldg(h + i * hstride), v[0]));
+  }
+  __device__ void done(long long j, const St &s, double (&acc)[1]) const {
+    w[j] = s.t;
+    acc[0] = add_rn(acc[0], mul_rn(widen(s.t), widen(s.t)));
   }
   __device__ void finish(const double (&s)[1]) const {
-    if (out) *out = s[0];
+    if (out) *out = take_sqrt ? sqrt(s[0]) : s[0];
   }
 };
 

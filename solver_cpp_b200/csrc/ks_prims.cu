@@ -150,7 +150,7 @@ ks_status ks_block_axpy(const ks_vec *V, int64_t ld, int k, const double *h, ks_
   if (ld < n || (long long)(k - 1) * ld + n > V->n || (size_t)k > ctx->d_result_len)
     return set_error(ctx, KS_BAD_INPUT, "block_axpy: basis does not fit");
   KS_CUDA(ctx, cudaMemcpyAsync(ctx->d_result, h, sizeof(double) * k, cudaMemcpyHostToDevice, ctx->stream));
-  launch_vec(ctx, n, BlockAxpyOp<double>{(const double *)V->d, ld, k, ctx->d_result, 1, (double *)w->d, nullptr},
+  launch_basis(ctx, n, k, BlockAxpyOp<double>{(const double *)V->d, ld, k, ctx->d_result, 1, (double *)w->d, nullptr},
              Stop{nullptr, nullptr});
   KS_CUDA(ctx, cudaGetLastError());
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // h is a host array

@@ -33,7 +33,7 @@ enum Slot : int {
   S_T = 5,      // GMRES: current norm
   S_GAMMA = 6,  // k-skip
 };
-enum Aux : int { A_MAXLOOP = 0, A_RECORD = 1, A_SPMV = 2, A_CONVK = 3, A_FINAL = 4, A_KIDX = 5 };
+enum Aux : int { A_MAXLOOP = 0, A_RECORD = 1, A_SPMV = 2, A_CONVK = 3, A_FINAL = 4, A_KIDX = 5, A_PENDING = 6, A_XZERO = 7 };
 
 struct DevState {  // KState plus the host-mapped mirror of `done`
   KState k;
@@ -89,6 +89,7 @@ struct Params {
   long long restart;
   int kskip;
   int fix;
+  int x_update = 0;  // ks_params.x_update
 };
 
 template <class VT>
@@ -164,6 +165,8 @@ struct InitOp {
     st->k.aux[A_RECORD] = rec;
     st->k.aux[A_CONVK] = 0;
     st->k.aux[A_FINAL] = 0;
+    st->k.aux[A_PENDING] = 0;
+    st->k.aux[A_XZERO] = 1;  // x = 0 until the first deferred update lands
     st->k.s[S_BETA] = 0.0;  // first fused direction update: p = 0*r + r = r
     if (st->host_done) *(volatile int *)st->host_done = 0;
   }
@@ -395,6 +398,155 @@ struct XrUpdOp {
   }
 };
 
+// ------------------------------------------------------------------ deferred x
+// CG, CR and BiCG update x only through x += alpha p (cg.cpp:211,
+// cr.cpp:240, bicg.cpp:242), and nothing reads x inside their loops. So the
+// update is deferred: iteration L keeps its direction in slot (L-1) % D of a
+// ring of D vectors (the direction update writes the next slot instead of
+// overwriting p), its r-update kernel records alpha beside it and counts the
+// iteration as pending, and every D iterations (and once after the loop) one
+// pass applies x += alpha_i p_i over the pending slots in iteration order.
+// Each element of x sees the same products and sums in the same order, so x
+// is bit-identical, while the r-update no longer reads and writes x and p:
+// two fewer vector passes per iteration for one ring pass per D iterations.
+// The ring pays where x, r and the direction vectors stream from HBM every
+// iteration. When they fit in L2 (here: within 60 % of it) the per-iteration
+// x += alpha p is served from L2 and costs less than streaming the ring back
+// from HBM: measured on B200, the ring made CG 11 % faster at 160^3 in FP64
+// (4 vectors of 32.8 MB) but 3 % slower at 128^3 in FP64 (16.8 MB vectors)
+// and the FP32 inner solves at 160^3 (16.4 MB vectors) 8 % slower.
+constexpr int kDirRing = 32;
+
+inline int loop_vectors(int method) {  // x, r, p, A p (+ s for CR, + r*, p* for BiCG)
+  return method == KS_CG ? 4 : method == KS_CR ? 5 : method == KS_BICG ? 6 : 0;
+}
+
+inline bool defer_x(int method, const Params &sp, long long n, size_t elem, size_t l2) {
+  if (!loop_vectors(method) || sp.x_update == 1) return false;
+  if (sp.x_update == 2) return true;
+  return (double)loop_vectors(method) * (double)n * (double)elem > 0.6 * (double)l2;
+}
+
+inline int dir_ring(const Params &sp) {
+  return (int)std::max<long long>(1, std::min<long long>(kDirRing, sp.maxloop));
+}
+
+// Direction slots a method allocates: the ring, or the single in-place p.
+inline int dir_slots(int method, const Params &sp, long long n, size_t elem, size_t l2) {
+  return defer_x(method, sp, n, elem, l2) ? dir_ring(sp) : 1;
+}
+
+template <class VT>
+inline bool defer_x(const Env<VT> &E, int method) {
+  return defer_x(method, E.sp, E.n, sizeof(VT), E.ctx->l2_bytes);
+}
+
+template <class VT>
+struct DirRing {
+  VT *P;
+  long long n;
+  int D;
+  double *alpha;
+  VT *slot(long long L) const { return P + ((L - 1) % D) * n; }
+  double *aslot(long long L) const { return alpha + (L - 1) % D; }
+};
+
+// r -= alpha q; (r,r); alpha saved to the ring and the iteration counted as
+// pending for x. The scalar step is XrUpdOp's (mode 0: CG beta; 1: check).
+template <class VT>
+struct RUpdOp {
+  VT *r;
+  const VT *q;
+  DevState *st;
+  int mode;
+  double *aslot;
+  static constexpr int ND = 1;
+  struct Regs {
+    VT q, r;
+  };
+  __device__ Regs load(long long i) const { return {q[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
+    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
+    const VT ri = add_rn(mul_rn((VT)(-a), g.q), g.r);
+    r[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    *aslot = st->k.s[S_ALPHA];
+    st->k.aux[A_PENDING]++;
+    const long long L = st->k.loop;
+    if (mode == 0) {
+      st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
+      st->k.s[S_RR] = s[0];
+    }
+    check_top(st, L + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
+  }
+};
+
+// x += alpha_i p_i for the pending slots i = 0, 1, ... in order (basis_kernel),
+// then no iteration is pending. x starts at 0 (cg.cpp:79): the first flush
+// starts from 0 instead of reading x, so x needs no zeroing pass. Every
+// thread reads the pending count and the zero flag before the last CTA's
+// finish() resets them.
+template <class VT>
+struct FlushXOp {
+  using vt = VT;
+  static constexpr int NB = 1, ND = 0;
+  static constexpr bool kFinishOnly = true;
+  VT *x;
+  const VT *P;
+  long long ld;
+  const double *alpha;
+  DevState *st;
+  struct St {
+    VT t;
+  };
+  __device__ bool active() const { return true; }
+  __device__ int count() const { return (int)__ldg(&st->k.aux[A_PENDING]); }
+  __device__ const VT *base(int) const { return P; }
+  __device__ St init(long long j) const { return {__ldg(&st->k.aux[A_XZERO]) ? (VT)0 : x[j]}; }
+  __device__ void step(St &s, int i, const VT (&v)[1]) const {
+    s.t = add_rn(mul_rn((VT)__ldg(alpha + i), v[0]), s.t);
+  }
+  __device__ void done(long long j, const St &s, double (&)[1]) const { x[j] = s.t; }
+  __device__ void finish(const double (&)[1]) const {  // last CTA, after every element
+    st->k.aux[A_PENDING] = 0;
+    st->k.aux[A_XZERO] = 0;
+  }
+};
+
+// p_next = (beta * p) + r into the next ring slot.
+template <class VT>
+struct XpbyToOp {
+  const VT *p;
+  const VT *r;
+  VT *out;
+  const double *beta;
+  static constexpr int ND = 0;
+  struct Regs {
+    VT p, r;
+  };
+  __device__ Regs load(long long i) const { return {p[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const {
+    const VT b = (VT)rd(beta);
+    out[i] = add_rn(mul_rn(b, g.p), g.r);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
+// After iteration L: apply the ring once it is full.
+template <class VT>
+inline void ring_step(const Env<VT> &E, const DirRing<VT> &R, VT *x, long long L) {
+  if (L % R.D == 0) launch_basis(E.ctx, E.n, R.D, FlushXOp<VT>{x, R.P, R.n, R.alpha, E.st}, E.stop());
+}
+
+// After the loop: apply what is pending. Runs after the method has stopped
+// (its own done flag set), so only the outer method's flag stops it.
+template <class VT>
+inline void ring_final(const Env<VT> &E, const DirRing<VT> &R, VT *x) {
+  launch_basis(E.ctx, E.n, R.D, FlushXOp<VT>{x, R.P, R.n, R.alpha, E.st}, Stop{nullptr, E.outer_done});
+}
+
 template <class VT>
 struct Ws {  // carve n-length vectors out of one workspace block
   VT *base;
@@ -414,26 +566,35 @@ ks_status init_state(const Env<VT> &E, const VT *b) {
   return KS_OK;
 }
 
-inline int cg_vectors() { return 3; }
-
-// cg::solve, three kernels per iteration. (Forming the next direction inside
-// the SpMV's gather instead of the separate update was measured slower on
-// B200: gathering two vectors per nonzero cost 15 us per SpMV at 128^3, the
-// update kernel it removes 8 us.)
+// cg::solve, three kernels per iteration with the x update deferred to the
+// direction ring. (Forming the next direction inside the SpMV's gather
+// instead of the separate update was measured slower on B200: gathering two
+// vectors per nonzero cost 15 us per SpMV at 128^3, the update kernel it
+// removes 8 us.)
 template <class VT>
-ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
+ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   Ws<VT> W{ws, E.n};
-  VT *r = W.take(), *p = W.take(), *q = W.take();
+  VT *r = W.take(), *q = W.take();
+  const bool defer = defer_x(E, KS_CG);
+  const int D = defer ? dir_ring(E.sp) : 1;  // D = 1: p updated in place
+  DirRing<VT> R{W.take(D), E.n, D, dws};
   init_state(E, b);
-  vec(E, ZeroOp<VT>{x});
-  start_from_zero(E, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CG});
+  if (!defer) vec(E, ZeroOp<VT>{x});
+  start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CG});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
+    VT *p = R.slot(L);
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
-    vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 0});
-    vec(E, XpbyOp<VT>{p, r, &E.st->k.s[S_BETA]});
+    if (defer) {
+      vec(E, RUpdOp<VT>{r, q, E.st, 0, R.aslot(L)});
+      ring_step(E, R, x, L);
+    } else {
+      vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 0});
+    }
+    vec(E, XpbyToOp<VT>{p, r, R.slot(L + 1), &E.st->k.s[S_BETA]});
     if (E.outer && P.step()) break;
   }
+  if (defer) ring_final(E, R, x);
   return KS_OK;
 }
 
@@ -477,23 +638,55 @@ struct CrMvEpi {  // s = A r; rs2 = (r,s); beta = rs2/rs; rs = rs2
   }
 };
 
-inline int cr_vectors() { return 4; }
+// p = beta p + r into the next ring slot; q = beta q + s in place; (q,q) ->
+// alpha = s[RR] / (q,q) (Xpby2Op with the direction ring).
+template <class VT>
+struct Xpby2ToOp {
+  const VT *p;
+  const VT *r;
+  VT *pn;
+  VT *q;
+  const VT *s;
+  DevState *st;
+  static constexpr int ND = 1;
+  struct Regs {
+    VT p, r, q, s;
+  };
+  __device__ Regs load(long long i) const { return {p[i], r[i], q[i], s[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
+    const VT b = (VT)rd(&st->k.s[S_BETA]);
+    pn[i] = add_rn(mul_rn(b, g.p), g.r);
+    const VT qi = add_rn(mul_rn(b, g.q), g.s);
+    q[i] = qi;
+    acc[0] = add_rn(acc[0], mul_rn(widen(qi), widen(qi)));
+  }
+  __device__ void finish(const double (&sm)[1]) const { st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], sm[0]); }
+};
 
 template <class VT>
-ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
+ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   Ws<VT> W{ws, E.n};
-  VT *r = W.take(), *p = W.take(), *q = W.take(), *s = W.take();
+  VT *r = W.take(), *q = W.take(), *s = W.take();
+  const bool defer = defer_x(E, KS_CR);
+  const int D = defer ? dir_ring(E.sp) : 1;
+  DirRing<VT> R{W.take(D), E.n, D, dws};
   init_state(E, b);
-  vec(E, ZeroOp<VT>{x});
-  start_from_zero(E, StartEpi<VT>{b, r, p, nullptr, nullptr, E.st, START_CHECK});
-  mv(E, *E.A, (const VT *)p, CrStartMvEpi<VT>{r, q, s, E.st});
+  if (!defer) vec(E, ZeroOp<VT>{x});
+  start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CHECK});
+  mv(E, *E.A, (const VT *)R.slot(1), CrStartMvEpi<VT>{r, q, s, E.st});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
-    vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 1});
+    if (defer) {
+      vec(E, RUpdOp<VT>{r, q, E.st, 1, R.aslot(L)});
+      ring_step(E, R, x, L);
+    } else {
+      vec(E, XrUpdOp<VT>{x, r, R.slot(L), q, E.st, 1});
+    }
     mv(E, *E.A, (const VT *)r, CrMvEpi<VT>{r, s, E.st});
-    vec(E, Xpby2Op<VT>{p, r, q, s, E.st, 1});
+    vec(E, Xpby2ToOp<VT>{R.slot(L), r, R.slot(L + 1), q, s, E.st});
     if (E.outer && P.step()) break;
   }
+  if (defer) ring_final(E, R, x);
   return KS_OK;
 }
 
@@ -518,10 +711,12 @@ struct BicgMvTEpi {  // r* = -alpha (A^T p*) + r*; rr2 = (r*, r) -> beta
   }
 };
 
+// p_next = beta p + r (pn: the next ring slot, or p itself); ps = beta ps + rs.
 template <class VT>
-struct Xpby2PlainOp {  // p = beta p + r; ps = beta ps + rs
-  VT *p;
+struct Xpby2PlainOp {
+  const VT *p;
   const VT *r;
+  VT *pn;
   VT *ps;
   const VT *rs;
   const double *beta;
@@ -532,30 +727,38 @@ struct Xpby2PlainOp {  // p = beta p + r; ps = beta ps + rs
   __device__ Regs load(long long i) const { return {p[i], r[i], ps[i], rs[i]}; }
   __device__ void store(long long i, const Regs &g, double (&)[1]) const {
     const VT b = (VT)rd(beta);
-    p[i] = add_rn(mul_rn(b, g.p), g.r);
+    pn[i] = add_rn(mul_rn(b, g.p), g.r);
     ps[i] = add_rn(mul_rn(b, g.ps), g.rs);
   }
   __device__ void finish(const double (&)[1]) const {}
 };
 
-inline int bicg_vectors() { return 5; }
-
 template <class VT>
-ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws) {
+ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   Ws<VT> W{ws, E.n};
-  VT *r = W.take(), *rs = W.take(), *p = W.take(), *ps = W.take(), *mvv = W.take();
+  VT *r = W.take(), *rs = W.take(), *ps = W.take(), *mvv = W.take();
+  const bool defer = defer_x(E, KS_BICG);
+  const int D = defer ? dir_ring(E.sp) : 1;
+  DirRing<VT> R{W.take(D), E.n, D, dws};
   init_state(E, b);
-  vec(E, ZeroOp<VT>{x});
+  if (!defer) vec(E, ZeroOp<VT>{x});
   // (r*, r) = (r, r) at the start
-  start_from_zero(E, StartEpi<VT>{b, r, rs, p, ps, E.st, START_CG});
+  start_from_zero(E, StartEpi<VT>{b, r, rs, R.slot(1), ps, E.st, START_CG});
   Poller P{E.ctx, E.hflag, E.lookahead};
   for (long long L = 1; L <= E.sp.maxloop; L++) {
+    VT *p = R.slot(L);
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
-    vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
+    if (defer) {
+      vec(E, RUpdOp<VT>{r, mvv, E.st, 1, R.aslot(L)});
+      ring_step(E, R, x, L);
+    } else {
+      vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
+    }
     mv(E, *E.AT, (const VT *)ps, BicgMvTEpi<VT>{rs, r, E.st});
-    vec(E, Xpby2PlainOp<VT>{p, r, ps, rs, &E.st->k.s[S_BETA]});
+    vec(E, Xpby2PlainOp<VT>{p, r, R.slot(L + 1), ps, rs, &E.st->k.s[S_BETA]});
     if (E.outer && P.step()) break;
   }
+  if (defer) ring_final(E, R, x);
   return KS_OK;
 }
 
@@ -613,12 +816,15 @@ struct GcrBetaPut {  // beta[i] = -(Av, Q_i) / qq[i]   (blas::Gcr_sp_1)
 
 // P_{k+1} = z + sum_i beta_i P_i, Q_{k+1} = Av + sum_i beta_i Q_i, the sums
 // accumulated from zero in index order (gcr.cpp:277-308); then
-// qq[k+1] = (Q_{k+1},Q_{k+1}) and alpha = (r, Q_{k+1}) / qq[k+1].
+// qq[k+1] = (Q_{k+1},Q_{k+1}) and alpha = (r, Q_{k+1}) / qq[k+1]. Runs in
+// basis_kernel over the two bases P and Q.
 template <class VT>
 struct GcrPQOp {
+  using vt = VT;
+  static constexpr int NB = 2, ND = 2;
   const VT *P;
   const VT *Q;
-  long long n;
+  long long ld;
   int k1;  // number of terms (k+1)
   const double *beta;
   const VT *z;
@@ -628,23 +834,28 @@ struct GcrPQOp {
   VT *qn;
   double *qq_next;
   DevState *st;
-  static constexpr int ND = 2;
-  __device__ void elem(long long j, double (&acc)[2]) const {
-    VT pa = (VT)0, qa = (VT)0;
-    for (int i = 0; i < k1; i++) {
-      const VT bi = (VT)rd(beta + i);
-      pa = add_rn(mul_rn(bi, P[(long long)i * n + j]), pa);
-      qa = add_rn(mul_rn(bi, Q[(long long)i * n + j]), qa);
-    }
-    pn[j] = add_rn(z[j], pa);
-    const VT qv = add_rn(Av[j], qa);
+  struct St {
+    VT pa, qa;
+  };
+  __device__ bool active() const { return true; }
+  __device__ int count() const { return k1; }
+  __device__ const VT *base(int b) const { return b == 0 ? P : Q; }
+  __device__ St init(long long) const { return {(VT)0, (VT)0}; }
+  __device__ void step(St &s, int i, const VT (&v)[2]) const {
+    const VT bi = (VT)rd(beta + i);
+    s.pa = add_rn(mul_rn(bi, v[0]), s.pa);
+    s.qa = add_rn(mul_rn(bi, v[1]), s.qa);
+  }
+  __device__ void done(long long j, const St &s, double (&acc)[2]) const {
+    pn[j] = add_rn(z[j], s.pa);
+    const VT qv = add_rn(Av[j], s.qa);
     qn[j] = qv;
     acc[0] = add_rn(acc[0], mul_rn(widen(qv), widen(qv)));
     acc[1] = add_rn(acc[1], mul_rn(widen(r[j]), widen(qv)));
   }
-  __device__ void finish(const double (&s)[2]) const {
-    *qq_next = s[0];
-    st->k.s[S_ALPHA] = rdiv(st, s[1], s[0]);
+  __device__ void finish(const double (&sm)[2]) const {
+    *qq_next = sm[0];
+    st->k.s[S_ALPHA] = rdiv(st, sm[1], sm[0]);
   }
 };
 
@@ -655,11 +866,6 @@ struct SetLoopOp {
   DevState *st;
   long long v;
   __device__ void run() const { st->k.loop = v; }
-};
-
-struct SqrtTOp {  // s[T] = sqrt(s[T])
-  DevState *st;
-  __device__ void run() const { st->k.s[S_T] = sqrt(st->k.s[S_T]); }
 };
 
 // Shared GCR / VPGCR body. With `inner` set, each new direction is the inner
@@ -703,8 +909,10 @@ ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws
       mv(E, *E.A, znew, StoreEpi<VT, VT>{Av});
       KS_TRY(launch_block_dot<1, VT>(E.ctx, Q, n, k + 1, Av, nullptr, n, GcrBetaPut{beta, qq, E.st},
                                      E.stop()));
-      vec(E, GcrPQOp<VT>{P, Q, n, k + 1, beta, znew, Av, r, P + (long long)(k + 1) * n,
-                         Q + (long long)(k + 1) * n, qq + k + 1, E.st});
+      launch_basis(E.ctx, n, k + 1,
+                   GcrPQOp<VT>{P, Q, n, k + 1, beta, znew, Av, r, P + (long long)(k + 1) * n,
+                               Q + (long long)(k + 1) * n, qq + k + 1, E.st},
+                   E.stop());
       // Each step is one check of the loop counter, so the method has
       // stopped on the device after at most maxloop steps.
       if ((E.outer && P_.step()) || issued_steps >= E.sp.maxloop) {
@@ -737,7 +945,22 @@ struct ScaleOp {  // out = a / t, t from slot (Scalar_x_div_a)
   __device__ void finish(const double (&)[1]) const {}
 };
 
-// Cycle start scalars: e = 0, e[0] = t; done checks happen per step.
+// Stopping test of step k (gmres.cpp:270-324): record (count+1, |e_k|/|b|);
+// maxloop first, then eps. The device remembers k for the final assembly.
+__device__ __forceinline__ void gm_check(const GmArrays &g, DevState *st, int k) {
+  const long long count = st->k.loop;
+  const double err = fabs(g.e[k]) / st->k.s[S_BNORM];
+  record(st, count + 1, err);
+  st->k.aux[A_CONVK] = k;
+  if (count + 1 >= st->k.aux[A_MAXLOOP])
+    set_done(st, kMaxLoop);
+  else if (err <= st->k.s[S_EPS])
+    set_done(st, kConverged);
+  else if (err != err)
+    set_done(st, kNaN);
+}
+
+// Cycle start scalars: e = 0, e[0] = t; then the stopping test of step 0.
 struct GmCycleOp {
   GmArrays g;
   DevState *st;
@@ -745,26 +968,7 @@ struct GmCycleOp {
     for (int i = 0; i < g.m; i++) g.e[i] = 0.0;
     g.e[0] = st->k.s[S_T];
     st->k.aux[A_KIDX] = 0;
-  }
-};
-
-// Stopping test of step k (gmres.cpp:270-324): record (count+1, |e_k|/|b|);
-// maxloop first, then eps. The device remembers k for the final assembly.
-struct GmCheckOp {
-  GmArrays g;
-  DevState *st;
-  int k;
-  __device__ void run() const {
-    const long long count = st->k.loop;
-    const double err = fabs(g.e[k]) / st->k.s[S_BNORM];
-    record(st, count + 1, err);
-    st->k.aux[A_CONVK] = k;
-    if (count + 1 >= st->k.aux[A_MAXLOOP])
-      set_done(st, kMaxLoop);
-    else if (err <= st->k.s[S_EPS])
-      set_done(st, kConverged);
-    else if (err != err)
-      set_done(st, kNaN);
+    gm_check(g, st, 0);
   }
 };
 
@@ -775,11 +979,13 @@ struct GmPutH {  // H[i][k] = (w, V_i)
 };
 
 // H[k+1][k] = |w| arrives in s[T] from the block AXPY; then the Givens
-// rotations of column k (gmres.cpp:384-399) and count++.
+// rotations of column k (gmres.cpp:384-399), count++ and, unless step k ends
+// the cycle, the stopping test at the top of step k+1.
 struct GmGivensOp {
   GmArrays g;
   DevState *st;
   int k;
+  int check_next;
   __device__ void run() const {
     const int m = g.m;
     double *H = g.H;
@@ -798,6 +1004,7 @@ struct GmGivensOp {
     H[(long long)k * m + k] = g.cs[k] * H[(long long)k * m + k] - g.sn[k] * H[(long long)(k + 1) * m + k];
     H[(long long)(k + 1) * m + k] = 0.0;
     st->k.loop += 1;
+    if (check_next) gm_check(g, st, k + 1);
   }
 };
 
@@ -824,46 +1031,43 @@ struct GmHyeOp {
 };
 
 // x = x + sum_i y_i B_i, the sum accumulated from zero in index order
-// (gmres.cpp:409-419). With `final_mode` the count comes from the stop step;
-// `overwrite` reproduces the reference's Scalar_ax assembly
-// (gmres.cpp:290-297): only the last term survives.
+// (gmres.cpp:409-419), in basis_kernel. With `final_mode` the count comes
+// from the stop step, and the update runs only once the method has stopped
+// by convergence or maxloop and has not been assembled yet; `overwrite`
+// reproduces the reference's Scalar_ax assembly (gmres.cpp:290-297): only
+// the last term survives.
 template <class VT>
 struct GmUpdateOp {
+  using vt = VT;
+  static constexpr int NB = 1, ND = 0;
   const VT *B;
-  long long n;
+  long long ld;
   int cnt;
   const double *y;
   VT *x;
   const DevState *st;
   int final_mode;
   int overwrite;
-  static constexpr int ND = 0;
-  __device__ void elem(long long j, double (&)[1]) const {
-    int c = cnt;
-    if (final_mode) c = (int)st->k.aux[A_CONVK];
-    VT t = (VT)0;
-    if (overwrite) {
-      if (c > 0) t = mul_rn((VT)rd(y + c - 1), B[(long long)(c - 1) * n + j]);
-    } else {
-      for (int i = 0; i < c; i++) t = add_rn(t, mul_rn((VT)rd(y + i), B[(long long)i * n + j]));
-    }
-    x[j] = add_rn(x[j], t);
+  struct St {
+    VT t;
+  };
+  __device__ int terms() const { return final_mode ? (int)st->k.aux[A_CONVK] : cnt; }
+  __device__ bool active() const {
+    if (!final_mode) return true;
+    const int d = st->k.done;
+    return (d == kConverged || d == kMaxLoop) && !st->k.aux[A_FINAL];
   }
+  __device__ int count() const { return overwrite ? 0 : terms(); }
+  __device__ const VT *base(int) const { return B; }
+  __device__ St init(long long j) const {
+    const int c = terms();
+    if (overwrite && c > 0) return {mul_rn((VT)rd(y + c - 1), B[(long long)(c - 1) * ld + j])};
+    return {(VT)0};
+  }
+  __device__ void step(St &s, int i, const VT (&v)[1]) const { s.t = add_rn(s.t, mul_rn((VT)rd(y + i), v[0])); }
+  __device__ void done(long long j, const St &s, double (&)[1]) const { x[j] = add_rn(x[j], s.t); }
   __device__ void finish(const double (&)[1]) const {}
 };
-
-// Final assembly runs in a kernel that is not gated by `done`; it checks the
-// stop reason itself and marks the state assembled.
-template <class VT>
-__global__ void gm_final_kernel(GmUpdateOp<VT> op, DevState *st, const int *outer_done) {
-  if (outer_done && *(volatile const int *)outer_done) return;
-  const int d = st->k.done;
-  if (!(d == kConverged || d == kMaxLoop) || st->k.aux[A_FINAL]) return;
-  double acc[1];
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < op.n;
-       j += (long long)gridDim.x * blockDim.x)
-    op.elem(j, acc);
-}
 
 struct GmMarkFinal {
   DevState *st;
@@ -902,7 +1106,6 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
     vec(E, ScaleOp<VT>{r, V, &E.st->k.s[S_T]});
     launch_scalar(E.ctx, GmCycleOp{g, E.st}, E.stop());
     for (int k = 0; k < m - 1; k++) {
-      launch_scalar(E.ctx, GmCheckOp{g, E.st, k}, E.stop());
       const VT *vk = V + (long long)k * n;
       if (inner) {
         inner->solve(vk, Z + (long long)k * n);
@@ -911,10 +1114,10 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
         mv(E, *E.A, vk, StoreEpi<VT, VT>{w});
       }
       KS_TRY(launch_block_dot<1, VT>(E.ctx, V, n, k + 1, w, nullptr, n, GmPutH{g.H, m, k}, E.stop()));
-      vec(E, BlockAxpyOp<VT>{V, n, k + 1, g.H + k, m, w, &E.st->k.s[S_T]});
-      launch_scalar(E.ctx, SqrtTOp{E.st}, E.stop());
+      launch_basis(E.ctx, n, k + 1, BlockAxpyOp<VT>{V, n, k + 1, g.H + k, m, w, &E.st->k.s[S_T], 1},
+                   E.stop());  // s[T] = |w|
       vec(E, ScaleOp<VT>{w, V + (long long)(k + 1) * n, &E.st->k.s[S_T]});
-      launch_scalar(E.ctx, GmGivensOp{g, E.st, k}, E.stop());
+      launch_scalar(E.ctx, GmGivensOp{g, E.st, k, k + 1 < m - 1 ? 1 : 0}, E.stop());
       issued++;
       if (E.outer && P.step()) {
         stop_host = true;
@@ -928,17 +1131,14 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
     if (stop_host) break;
     // end of cycle (gmres.cpp:409-421)
     launch_scalar(E.ctx, GmHyeOp{g, E.st, m - 1, 0}, E.stop());
-    vec(E, GmUpdateOp<VT>{B, n, m - 1, g.y, x, E.st, 0, 0});
+    launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, n, m - 1, g.y, x, E.st, 0, 0}, E.stop());
     if (E.outer && P.step()) break;
   }
-  // The step that stopped the method (converged or maxloop) assembles x.
+  // The step that stopped the method (converged or maxloop) assembles x;
+  // these kernels are gated by the stop reason, not by `done`.
   launch_scalar(E.ctx, GmHyeOp{g, E.st, -1, 1}, Stop{nullptr, E.outer_done});
-  {
-    GmUpdateOp<VT> op{B, n, 0, g.y, x, E.st, 1, E.faithful ? 1 : 0};
-    int grid = red_grid(E.ctx);
-    E.ctx->launches++;
-    gm_final_kernel<VT><<<grid, kThreads, 0, E.ctx->stream>>>(op, E.st, E.outer_done);
-  }
+  launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, n, 0, g.y, x, E.st, 1, E.faithful ? 1 : 0},
+               Stop{nullptr, E.outer_done});
   launch_scalar(E.ctx, GmMarkFinal{E.st}, Stop{nullptr, E.outer_done});
   return KS_OK;
 }
@@ -1193,7 +1393,7 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
       mv(E, *E.A, (const VT *)p, StoreEpi<VT, VT>{Av});
       vec(E, KsXrOp<VT>{x, r, p, Av, coef + i});
       mv(E, *E.AT, (const VT *)ps, KsRsEpi<VT>{rs, coef + i});
-      vec(E, Xpby2PlainOp<VT>{p, r, ps, rs, coef + k + 1 + i});
+      vec(E, Xpby2PlainOp<VT>{p, r, p, ps, rs, coef + k + 1 + i});
     }
     if (E.outer && P.step()) break;
   }
@@ -1201,12 +1401,12 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
 }
 
 // ------------------------------------------------------------------ sizes
-inline long long vec_count(int method, const Params &sp) {
+inline long long vec_count(int method, const Params &sp, long long n, size_t elem, size_t l2) {
   const long long m = sp.restart, k = sp.kskip;
   switch (method) {
-    case KS_CG: return 3;
-    case KS_CR: return 4;
-    case KS_BICG: return 5;
+    case KS_CG: return 2 + dir_slots(method, sp, n, elem, l2);
+    case KS_CR: return 3 + dir_slots(method, sp, n, elem, l2);
+    case KS_BICG: return 4 + dir_slots(method, sp, n, elem, l2);
     case KS_GCR: case KS_VPGCR: return 3 + 2 * m;
     case KS_GMRES: return 3 + (m + 1);
     case KS_VPGMRES: return 3 + (m + 1) + m;
@@ -1225,6 +1425,7 @@ inline long long dws_count(int method, const Params &sp) {
     case KS_GMRES: case KS_VPGMRES: return (m + 1) * m + 4 * m + 4;
     case KS_KSKIPCG: return 6 * k + 4 + 2 * (k + 1) + 4;
     case KS_KSKIPBICG: return 8 * k + 6 + 2 * (k + 1) + 4;
+    case KS_CG: case KS_CR: case KS_BICG: return kDirRing + 4;  // alpha ring
   }
   return 4;
 }
@@ -1367,9 +1568,9 @@ template <class IT>
 ks_status run_method(int method, const Env<IT> &E, const IT *b, IT *x, IT *ws, double *dws,
                      InnerRunner<IT> *inner) {
   switch (method) {
-    case KS_CG: return run_cg(E, b, x, ws);
-    case KS_CR: return run_cr(E, b, x, ws);
-    case KS_BICG: return run_bicg(E, b, x, ws);
+    case KS_CG: return run_cg(E, b, x, ws, dws);
+    case KS_CR: return run_cr(E, b, x, ws, dws);
+    case KS_BICG: return run_bicg(E, b, x, ws, dws);
     case KS_GCR: return run_gcr_core(E, b, x, ws, dws, (InnerRunner<IT> *)nullptr);
     case KS_GMRES: return run_gmres_core(E, b, x, ws, dws, (InnerRunner<IT> *)nullptr);
     case KS_KSKIPCG: return run_kskipcg(E, b, x, ws, dws);
@@ -1441,8 +1642,11 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   if (ip != KS_FP64 && needs_T(inner) && !(ip == KS_FP32 ? (const void *)AT->val32 : (const void *)AT->val16))
     return set_error(ctx, KS_BAD_INPUT, "low-precision inner BiCG needs the transpose's value copy");
 
-  Params outer_sp{prm->outer_maxloop, prm->outer_eps, prm->outer_restart, prm->outer_kskip, prm->outer_fix};
-  Params inner_sp{prm->inner_maxloop, prm->inner_eps, prm->inner_restart, prm->inner_kskip, prm->inner_fix};
+  Params outer_sp{prm->outer_maxloop, prm->outer_eps, prm->outer_restart, prm->outer_kskip, prm->outer_fix,
+                  prm->x_update};
+  Params inner_sp{prm->inner_maxloop, prm->inner_eps, prm->inner_restart, prm->inner_kskip, prm->inner_fix,
+                  prm->x_update};
+  if (prm->x_update < 0 || prm->x_update > 2) return set_error(ctx, KS_BAD_INPUT, "x_update must be 0, 1 or 2");
   if ((outer == KS_GCR || outer == KS_GMRES || outer == KS_VPGCR || outer == KS_VPGMRES) &&
       (outer_sp.restart < 1 || outer_sp.restart > 1024))
     return set_error(ctx, KS_BAD_INPUT, "restart must be in [1, 1024]");
@@ -1479,7 +1683,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
 
   // workspaces
   double *ws = nullptr, *dws = nullptr;
-  KS_TRY(al.get((size_t)(vec_count(outer, outer_sp) * n), &ws));
+  KS_TRY(al.get((size_t)(vec_count(outer, outer_sp, n, sizeof(double), ctx->l2_bytes) * n), &ws));
   KS_TRY(al.get((size_t)dws_count(outer, outer_sp), &dws));
 
   Env<double> E;
@@ -1514,7 +1718,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
       I.outer = false;
       I.sp = inner_sp;
       I.hflag = nullptr;
-      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp) * n), &IR.ws64));
+      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp, n, sizeof(double), ctx->l2_bytes) * n), &IR.ws64));
     } else {
       Env<float> &I = IR.E32;
       I.ctx = ctx;
@@ -1529,7 +1733,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
       I.faithful = E.faithful;
       I.n = n;
       I.hflag = nullptr;
-      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp) * n), &IR.ws32));
+      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp, n, sizeof(float), ctx->l2_bytes) * n), &IR.ws32));
       KS_TRY(al.get((size_t)n, &IR.b32));
       KS_TRY(al.get((size_t)n, &IR.z32));
     }

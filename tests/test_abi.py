@@ -31,8 +31,10 @@ def test_library_exports_every_declared_symbol(ks):
 
 
 def test_abi_version_and_status_strings(ks):
+    from solver_cpp_b200 import _abi
+
     lib = ks.lib()
-    assert lib.ks_abi_version() == 1
+    assert lib.ks_abi_version() == _abi.ABI_VERSION == 2  # 2: ks_params.x_update
     assert b"not converged" in lib.ks_status_string(2)
     assert b"not implemented" in lib.ks_status_string(99)
 

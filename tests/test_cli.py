@@ -100,3 +100,42 @@ def test_cli_reproduces_reference_run(cli, tmp_path, cid):
     tr = float(re.search(r"\|b-ax\|2/\|b\|2 = (\S+)", r.stdout).group(1))
     if meta["converged"]:
         assert tr == pytest.approx(meta["true_res_log10"], abs=0.21)
+
+
+def _mm_dir(tmp_path, name, prob, grid):
+    """The Matrix Market layout the reference checks: <P>/<N>/<D>/<M>/<M>.mtx."""
+    import scipy.io
+
+    A, _, _ = config_problem(prob, grid)
+    d = tmp_path / "Matrix" / "MM" / name
+    d.mkdir(parents=True)
+    scipy.io.mmwrite(str(d / f"{name}.mtx"), A.to_scipy(), precision=17)
+    run_dir = tmp_path / "run"
+    run_dir.mkdir(exist_ok=True)
+    return A, str(run_dir)
+
+
+def test_cli_matrix_market_input_checks(cli, tmp_path, ks):
+    _, rd = _mm_dir(tmp_path, "mm", "poisson2d", 8)
+    r = run(["-S", "cg", "-M", "nothere", "-P", str(tmp_path)], rd)
+    assert r.returncode != 0 and "Error no MM files Dir" in r.stderr
+    r = run(["-S", "cg", "-M", "mm", "-m", "mm", "-P", str(tmp_path)], rd)
+    assert r.returncode != 0 and "Only can set one input source" in r.stderr
+    bad = tmp_path / "Matrix" / "MM" / "bad"
+    bad.mkdir()
+    (bad / "bad.mtx").write_text("%%MatrixMarket matrix coordinate complex general\n1 1 1\n1 1 1 0\n")
+    r = run(["-S", "cg", "-M", "bad", "-P", str(tmp_path)], rd)
+    assert r.returncode != 0 and "Error in mm file" in r.stderr
+    if ks.lib().ks_device_count() == 0:  # the file is read; only the device is missing
+        r = run(["-S", "cg", "-M", "mm", "-P", str(tmp_path)], rd)
+        assert r.returncode == 1 and "no CUDA device" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_matrix_market_solve(cli, tmp_path):
+    A, rd = _mm_dir(tmp_path, "mm", "poisson2d", 40)
+    r = run(["-S", "cg", "-M", "mm", "-P", str(tmp_path), "-E", "1e-12"], rd)
+    assert r.returncode == 0, r.stderr
+    assert "converge" in r.stdout and "not converge" not in r.stdout
+    x = np.loadtxt(os.path.join(rd, "output", "CG_xvec.txt"), ndmin=2)[:, 1]
+    assert x.shape[0] == A.n and np.max(np.abs(x - 1.0)) < 1e-9  # b = A * 1

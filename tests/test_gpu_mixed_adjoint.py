@@ -78,3 +78,57 @@ def test_adjoint_gradient_dense_and_fd(ks, ctx, prob, solver):
         bm[i] -= h
         fd = (_loss(A, A.val, bp, xstar) - _loss(A, A.val, bm, xstar)) / (2 * h)
         assert abs(gb[i] - fd) <= 1e-6 * max(abs(fd), 1e-3 * np.max(np.abs(lam_d)))
+
+
+@pytest.mark.parametrize("prob,solver", [("varcoef2d", "CG"), ("convdiff2d", "BICG")])
+def test_adjoint_gradient_fd_512(ks, ctx, prob, solver):
+    """The 512^2 adjoint configuration: gradients with respect to 64 random
+    CSR values (and 8 entries of b) against central finite differences with
+    h = 1e-6 (relative to the entry), to 1e-6 relative. Each difference
+    quotient is formed from the exact identity for the two perturbed
+    solutions, so that it does not cancel in the loss (L ~ n/2): with
+    A+- = A +- h e_i e_c^T and A- x- = b, the difference d = x+ - x- solves
+    A+ d = -2 h x-_c e_i, and L(x+) - L(x-) = d^T (x- + d/2 - x*)."""
+    from solver_cpp_b200.matrices import CSR
+
+    A, b, _ = config_problem(prob, 512)
+    xstar = np.random.default_rng(6).standard_normal(A.n)
+    kw = dict(E=1e-14, L=40000)
+    tr = solver == "BICG"
+    M = ctx.matrix(A, transpose=True)
+    fw = ks.solve(ctx, M, solver, b, **kw)
+    assert fw.converged
+    X = ctx.vector(fw.x)
+    G = ctx.vector(fw.x - xstar)
+    GB, GV = ctx.vector(n=A.n), ctx.vector(n=A.nnz)
+    st, _ = ks.adjoint_grad(ctx, M, solver, X, G, GB, GV, **kw)
+    assert st == 0
+    gb, gv = GB.numpy(), GV.numpy()
+    rows = np.repeat(np.arange(A.n), np.diff(A.ptr))
+    rng = np.random.default_rng(7)
+    worst = []
+    for j in rng.choice(A.nnz, 64, replace=False):
+        i, c = rows[j], A.col[j]
+        step = 1e-6 * max(1.0, abs(A.val[j]))
+        vm, vp = A.val.copy(), A.val.copy()
+        vm[j] -= step
+        vp[j] += step
+        Mm = ctx.matrix(CSR(A.ptr, A.col, vm), transpose=tr)
+        xm = ks.solve(ctx, Mm, solver, b, **kw)
+        Mm.close()
+        rhs = np.zeros(A.n)
+        rhs[i] = -2.0 * step * xm.x[c]
+        Mp = ctx.matrix(CSR(A.ptr, A.col, vp), transpose=tr)
+        d = ks.solve(ctx, Mp, solver, rhs, **kw)
+        Mp.close()
+        assert xm.converged and d.converged
+        fd = d.x @ (xm.x + 0.5 * d.x - xstar) / (2.0 * step)
+        worst.append(abs(gv[j] - fd) / (abs(fd) + 1e-9 * np.max(np.abs(gv))))
+    # b: x+ - x- = 2h A^{-1} e_i exactly, so the quotient is e_i^T A^{-T} (x - x*)
+    for i in rng.choice(A.n, 8, replace=False):
+        rhs = np.zeros(A.n)
+        rhs[i] = 2e-6
+        d = ks.solve(ctx, M, solver, rhs, **kw)
+        fd = d.x @ (fw.x - xstar) / 2e-6
+        worst.append(abs(gb[i] - fd) / (abs(fd) + 1e-9 * np.max(np.abs(gb))))
+    assert max(worst) <= 1e-6, f"largest relative deviation {max(worst):.3e}"

@@ -107,3 +107,21 @@ def test_device_vectors_path(ks, ctx):
     r = ks.solve(ctx, M, "CG", B, x=X, E=1e-10)
     h = ks.solve(ctx, M, "CG", b, E=1e-10)
     assert r.converged and np.array_equal(X.numpy(), h.x)
+
+
+@pytest.mark.parametrize("name", ["CG", "CR", "BICG"])
+def test_deferred_solution_update_at_ring_boundaries(ks, ctx, oracle, name):
+    """CG, CR and BiCG apply x += alpha p either every iteration or through a
+    ring of 32 directions (x_update 1 / 2; 0 picks by L2 fit). Stopping
+    before, at and after a full ring (and at maxloop = the ring size) must
+    leave the same x bit for bit, and the x of the per-iteration update."""
+    A, b, _ = config_problem("convdiff3d" if name == "BICG" else "poisson3d", 24)
+    M = _mat(ctx, A)
+    for L in (1, 5, 31, 32, 33, 64, 65, 90):
+        r1 = ks.solve(ctx, M, name, b, L=L, E=1e-30, x_update=1)
+        r2 = ks.solve(ctx, M, name, b, L=L, E=1e-30, x_update=2)
+        assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.hist_err, r2.hist_err), (name, L)
+        o = oracle.solve(A, b, name, L=L, E=1e-30)
+        assert r2.loop == o["loop"] and r2.status == o["status"] == 2, (name, L)
+        scale = np.linalg.norm(o["x"])
+        assert np.linalg.norm(r2.x - o["x"]) <= 1e-10 * scale, (name, L)
