@@ -195,9 +195,27 @@ def run_ours(args, world, rank, local):
     ctx = ks.Context(local)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
-    M = ctx.matrix(A, transpose=W["transpose"], fp32=True, bf16=True)
-    B = ctx.vector(b)
-    X = ctx.vector(n=n)
+    split = args.split and world > 1
+    comm = None
+    if split:  # row-split solve of the one system over the ranks (strong scaling), NCCL transport
+        import torch.distributed as dist
+
+        if W.get("adjoint"):
+            raise SystemExit("--split does not cover the adjoint workloads")
+        uid = [ks.Comm.unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(uid, src=0)
+        comm = ks.Comm.nccl(ctx, world, rank, uid[0])
+        plane = W["grid"] ** 2 if "3d" in W["problem"] else W["grid"]
+        rs = ks.partition_rows(n, world, plane)
+        r0, r1 = int(rs[rank]), int(rs[rank + 1])
+        M = ks.SplitMatrix(ctx, comm, A, r0, r1, transpose=W["transpose"], fp32=True, bf16=True)
+    else:
+        r0, r1 = 0, n
+        M = ctx.matrix(A, transpose=W["transpose"], fp32=True, bf16=True)
+    nl, nnzl = r1 - r0, M.nnz  # this rank's rows and nonzeros
+    b_loc = np.ascontiguousarray(b[r0:r1])
+    B = ctx.vector(b_loc)
+    X = ctx.vector(n=nl)
     launches0 = ks.lib().ks_ctx_launches(ctx.handle)
 
     adj = None
@@ -268,8 +286,8 @@ def run_ours(args, world, rank, local):
     # dominant kernel: SpMV with the workload's value precision, timed alone
     vals = W["spmv_values"]
     dt = ks.FP64 if vals == "fp64" else ks.FP32
-    xs = ctx.vector(np.random.default_rng(0).standard_normal(n), dtype=dt)
-    ys = ctx.vector(n=n, dtype=dt)
+    xs = ctx.vector(np.random.default_rng(0).standard_normal(nl), dtype=dt)
+    ys = ctx.vector(n=nl, dtype=dt)
     vcode = {"fp64": ks.FP64, "fp32": ks.FP32, "bf16": ks.BF16}[vals]
     for _ in range(5):
         ks.spmv(M, xs, ys, values=vcode)
@@ -284,7 +302,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     spmv_ms = s0.elapsed_time(s1) / reps
     ib = M.info()["index_bytes"]
-    alg = spmv_bytes(n, nnz, vals, ib)
+    alg = spmv_bytes(nl, nnzl, vals, ib)
     peak, peak_kind = load_peaks()
     achieved = alg / (spmv_ms / 1e3) / 1e9
     traffic = None
@@ -298,9 +316,9 @@ def run_ours(args, world, rank, local):
                 "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": f"spmv_{vals}",
                 "alg_bytes_per_launch": alg, "index_bytes": ib, "launch_ms": round(spmv_ms, 5),
                 "peak_kind": peak_kind}
-    fp64_bytes = spmv_bytes(n, nnz, "fp64", ib)
+    fp64_bytes = spmv_bytes(nl, nnzl, "fp64", ib)
     if vals != "fp64":  # also the FP64 SpMV of the outer loop
-        x64, y64 = ctx.vector(np.random.default_rng(0).standard_normal(n)), ctx.vector(n=n)
+        x64, y64 = ctx.vector(np.random.default_rng(0).standard_normal(nl)), ctx.vector(n=nl)
         ks.spmv(M, x64, y64)
         torch.cuda.synchronize()
         s0.record(stream)
@@ -315,8 +333,8 @@ def run_ours(args, world, rank, local):
     # end to end through the public host API: pinned b -> device -> x -> host
     e2e = None
     if not args.no_e2e and adj is None:
-        bh = torch.from_numpy(b).pin_memory().numpy()
-        xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        bh = torch.from_numpy(b_loc).pin_memory().numpy()
+        xh = torch.empty(nl, dtype=torch.float64).pin_memory().numpy()
         import ctypes as C
 
         p = ks.make_params(**W["params"])
@@ -338,8 +356,8 @@ def run_ours(args, world, rank, local):
             e1.record(stream)
         torch.cuda.synchronize()
         ems = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
-        e2e = {"value": ems / 1e3, "unit": "s", "h2d_bytes_per_step": 8 * n,
-               "d2h_bytes_per_step": 8 * n + 16 * int(rep.hist_len) + 64}
+        e2e = {"value": ems / 1e3, "unit": "s", "h2d_bytes_per_step": 8 * nl,
+               "d2h_bytes_per_step": 8 * nl + 16 * int(rep.hist_len) + 64}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and adj is None:
@@ -348,13 +366,15 @@ def run_ours(args, world, rank, local):
     out = {
         "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); SpMV HBM GB/s",
         "value": round(value, 6), "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(ms_per_step, 4), "higher_is_better": False, "scaling": "weak",
+        "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": ("f64 outer / " + {"fp32": "f32", "bf16": "f32 with bf16 values"}[
             W["params"]["inner_precision"]] + " inner") if "inner_precision" in W["params"] else "f64",
         "data": "synthetic (seeded generator of the configuration; no dataset)",
         "config": {"workload": args.workload, "problem": W["problem"], "grid": W["grid"], "n": n, "nnz": nnz,
                    "method": W["outer"] + ("/" + W["inner"] if W["inner"] != "NONE" else ""),
-                   "params": W["params"], "parallelism": f"replicas x{world}",
+                   "params": W["params"],
+                   "parallelism": f"row split x{world} (NCCL halo + all-reduce)" if split else f"replicas x{world}",
                    "l2": "inputs larger than L2 (matrix >= 175 MB)" if nnz * 12 > 126e6 else
                          "working set fits in the 126 MB L2 (no flush between steps)"},
         "result": {"status": res.status, "loop": res.loop, "true_rel_res": res.true_rel_res,
@@ -369,6 +389,8 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         print(json.dumps(out))
     M.close()
+    if comm is not None:
+        comm.close()
     ctx.close()
     del launches0
 
@@ -573,6 +595,9 @@ def main():
     ap.add_argument("--spmv-only", choices=["fp64", "fp32", "bf16"], default=None,
                     help="time only the SpMV kernel on the workload's matrix (profiling)")
     ap.add_argument("--index32", action="store_true", help="with --spmv-only: int32 column indices")
+    ap.add_argument("--split", action="store_true",
+                    help="with --gpus N > 1: split the one system's rows over the ranks (strong scaling) "
+                         "instead of one replica per rank")
     ap.add_argument("--ortho-only", type=int, nargs="+", default=None, metavar="K",
                     help="time only the GMRES block dot / block AXPY over K basis vectors (profiling)")
     args = ap.parse_args()

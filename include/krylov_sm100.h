@@ -307,6 +307,44 @@ ks_status ks_halo_plan(int nranks, int rank, const int64_t *row_start, const int
                        const int64_t *win_hi, int64_t *send_lo, int64_t *send_hi,
                        int64_t *recv_lo, int64_t *recv_hi);
 
+/* A row-split solve: every rank (one GPU each, one process or host thread
+ * each) holds a contiguous block of rows and runs the same calls. */
+typedef struct ks_comm ks_comm;
+/* NCCL transport, libnccl.so.2 loaded at run time: rank 0 makes the 128-byte
+ * id, the caller hands it to the other ranks (e.g. over torch.distributed),
+ * and every rank joins with the context of its own GPU. KS_UNIMPLEMENTED when
+ * NCCL cannot be loaded. */
+ks_status ks_comm_unique_id(void *id128);
+ks_status ks_comm_create_nccl(ks_ctx *ctx, int nranks, int rank,
+                              const void *id128, ks_comm **out);
+/* Ranks emulated inside one process (e.g. several contexts on one GPU): the
+ * same split solve, the halo copied device to device from the peer's vector
+ * and the dots summed by a kernel in rank order, with CUDA events ordering the
+ * streams. Every rank's calls must come from its own host thread; a rank that
+ * does not arrive within 120 s ends the others' calls with KS_TIMEOUT. */
+ks_status ks_comm_create_local(ks_ctx *const *ctxs, int nranks, ks_comm **comms);
+ks_status ks_comm_destroy(ks_comm *comm);
+ks_status ks_comm_info(const ks_comm *comm, int *nranks, int *rank);
+/* This rank's rows r0..r1-1 of an n_global x n_global matrix (global column
+ * indices; ptr holds r1 - r0 + 1 offsets of any base) and, with
+ * KS_MAT_TRANSPOSE, the same rows of A^T (tptr/tcol/tval). Every rank calls
+ * it with its own block, blocks contiguous in rank order (ks_partition_rows
+ * gives one). ks_solve / ks_solve_host / ks_spmv on the result take vectors
+ * of the local length r1 - r0 and run the split method: before each SpMV the
+ * halo of the input vector comes from the peers (ks_halo_plan), and every
+ * reduction is summed over the ranks before its scalar step, so every rank
+ * takes the same decisions. Replaces the reference's two-GPU split
+ * (cudaFunction.cu:1942-2226), which gathers all of x through the host. */
+ks_status ks_dist_upload(ks_ctx *ctx, ks_comm *comm, int64_t n_global,
+                         int64_t r0, int64_t r1, const int32_t *ptr,
+                         const int32_t *col, const double *val,
+                         const int32_t *tptr, const int32_t *tcol,
+                         const double *tval, unsigned flags, ks_mat **out);
+/* Global size, own rows and the vector window [ext_lo, ext_hi) of a split
+ * matrix (a single-GPU matrix reports 0..n for all). */
+ks_status ks_mat_dist_info(const ks_mat *mat, int64_t *n_global, int64_t *r0,
+                           int64_t *r1, int64_t *ext_lo, int64_t *ext_hi);
+
 /* Matrix Market coordinate files: the input source the reference declares
  * (-P / -D / -M, solver_collection.cpp:278-286,505-601) but never reads.
  * Fields real / double / integer / pattern (pattern entries are 1.0);

@@ -415,3 +415,86 @@ def halo_plan(row_start, win_lo, win_hi, rank: int):
     out = [np.zeros(P, dtype=np.int64) for _ in range(4)]
     _check(lib().ks_halo_plan(P, rank, _ptr(rs), _ptr(lo), _ptr(hi), *[_ptr(o) for o in out]), None, "halo_plan")
     return {"send": list(zip(out[0], out[1])), "recv": list(zip(out[2], out[3]))}
+
+
+# ----------------------------------------------------------------- row-split solves
+class Comm:
+    """Transport of a row-split solve (``ks_comm``)."""
+
+    def __init__(self, handle, ctx: Context):
+        self.handle = handle
+        self.ctx = ctx
+        n, r = C.c_int(), C.c_int()
+        _check(lib().ks_comm_info(handle, C.byref(n), C.byref(r)), None, "comm_info")
+        self.nranks, self.rank = n.value, r.value
+
+    @staticmethod
+    def unique_id() -> bytes:
+        """NCCL id made on rank 0, to be handed to every rank."""
+        buf = C.create_string_buffer(128)
+        _check(lib().ks_comm_unique_id(buf), None, "comm_unique_id")
+        return buf.raw
+
+    @classmethod
+    def nccl(cls, ctx: Context, nranks: int, rank: int, uid: bytes) -> "Comm":
+        h = C.c_void_p()
+        buf = C.create_string_buffer(uid, 128)
+        _check(lib().ks_comm_create_nccl(ctx.handle, nranks, rank, buf, C.byref(h)), ctx.handle, "comm_create_nccl")
+        return cls(h, ctx)
+
+    @classmethod
+    def local(cls, ctxs) -> list:
+        """Ranks emulated in this process, one context each (each rank's calls
+        must then run on its own thread)."""
+        P = len(ctxs)
+        arr = (C.c_void_p * P)(*[c.handle for c in ctxs])
+        out = (C.c_void_p * P)()
+        _check(lib().ks_comm_create_local(arr, P, out), None, "comm_create_local")
+        return [cls(C.c_void_p(out[q]), ctxs[q]) for q in range(P)]
+
+    def close(self):
+        if self.handle:
+            lib().ks_comm_destroy(self.handle)
+            self.handle = None
+
+
+class SplitMatrix(Matrix):
+    """This rank's rows r0..r1-1 of a row-split matrix (``ks_dist_upload``);
+    solves on it take and return vectors of the local length r1 - r0."""
+
+    def __init__(self, ctx: Context, comm: Comm, A: CSR, r0: int, r1: int, transpose=False, fp32=False,
+                 bf16=False, index32=False, AT: CSR | None = None):
+        self.ctx = ctx
+        self.comm = comm
+        self.r0, self.r1, self.n_global = int(r0), int(r1), A.n
+        self.n = self.r1 - self.r0
+        j0, j1 = A.ptr[r0], A.ptr[r1]
+        ptr = np.ascontiguousarray(A.ptr[r0:r1 + 1], dtype=np.int32)
+        col = np.ascontiguousarray(A.col[j0:j1], dtype=np.int32)
+        val = np.ascontiguousarray(A.val[j0:j1], dtype=np.float64)
+        self.nnz = int(j1 - j0)
+        tp = tc = tv = None
+        if transpose:
+            from .matrices import transpose as _transpose
+
+            T = AT if AT is not None else _transpose(A)
+            k0, k1 = T.ptr[r0], T.ptr[r1]
+            tp = np.ascontiguousarray(T.ptr[r0:r1 + 1], dtype=np.int32)
+            tc = np.ascontiguousarray(T.col[k0:k1], dtype=np.int32)
+            tv = np.ascontiguousarray(T.val[k0:k1], dtype=np.float64)
+        flags = (_abi.MAT_TRANSPOSE if transpose else 0) | (_abi.MAT_FP32 if fp32 else 0) | (
+            _abi.MAT_BF16 if bf16 else 0) | (_abi.MAT_INDEX32 if index32 else 0)
+        h = C.c_void_p()
+        _check(lib().ks_dist_upload(ctx.handle, comm.handle, A.n, self.r0, self.r1, _ptr(ptr),
+                                    _ptr(col) if col.size else None, _ptr(val) if val.size else None,
+                                    _ptr(tp) if tp is not None else None,
+                                    _ptr(tc) if tc is not None and tc.size else None,
+                                    _ptr(tv) if tv is not None and tv.size else None, flags, C.byref(h)),
+               ctx.handle, "ks_dist_upload")
+        self.handle = h
+        self.flags = flags
+
+    def window(self):
+        vals = [C.c_int64() for _ in range(5)]
+        _check(lib().ks_mat_dist_info(self.handle, *[C.byref(v) for v in vals]), self.ctx.handle, "dist_info")
+        return {k: v.value for k, v in zip(("n_global", "r0", "r1", "ext_lo", "ext_hi"), vals)}

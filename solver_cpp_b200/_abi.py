@@ -124,6 +124,13 @@ SIGNATURES = [
     ("ks_partition_rows", C.c_int, [_I64, C.c_int, _I64, _VP]),
     ("ks_halo_window", C.c_int, [_I64, _I64, _VP, _VP, _PI64, _PI64]),
     ("ks_halo_plan", C.c_int, [C.c_int, C.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("ks_comm_unique_id", C.c_int, [_VP]),
+    ("ks_comm_create_nccl", C.c_int, [_VP, C.c_int, C.c_int, _VP, C.POINTER(_VP)]),
+    ("ks_comm_create_local", C.c_int, [_VP, C.c_int, _VP]),
+    ("ks_comm_destroy", C.c_int, [_VP]),
+    ("ks_comm_info", C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("ks_dist_upload", C.c_int, [_VP, _VP, _I64, _I64, _I64, _VP, _VP, _VP, _VP, _VP, _VP, C.c_uint, C.POINTER(_VP)]),
+    ("ks_mat_dist_info", C.c_int, [_VP, _PI64, _PI64, _PI64, _PI64, _PI64]),
     ("ks_mm_read_header", C.c_int, [C.c_char_p, _PI64, _PI64]),
     ("ks_mm_read", C.c_int, [C.c_char_p, _I64, _I64, _VP, _VP, _VP]),
     ("ks_crs_write", C.c_int, [C.c_char_p, _I64, _I64, _VP, _VP, _VP, _VP, _VP]),

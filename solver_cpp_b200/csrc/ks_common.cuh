@@ -270,7 +270,24 @@ struct ks_ctx {
   std::vector<bool> pool_busy;
   std::string last_error;
   long long launches = 0;       // kernels launched (diagnostics)
+  // Row-split solve in progress: its communicator (reductions are summed over
+  // the ranks), the first transport error, the stage of the summed values,
+  // and the outer method's `done` with a mapped snapshot ring for polling.
+  struct ks_comm *red_comm = nullptr;
+  ks_status dist_status = KS_OK;
+  double *d_stage = nullptr;    // kStageLen doubles
+  const int *poll_done = nullptr;
+  int *h_snap = nullptr;        // mapped host ring (nflags entries)
+  int *d_snap = nullptr;        // its device view
 };
+
+namespace ks {
+constexpr int kStageLen = 4096;  // >= 2 x 1024 block-dot results, >= kMaxDots
+}
+
+namespace ks {
+struct DistInfo;  // ks_dist.cuh
+}
 
 struct ks_mat {
   ks_ctx *ctx = nullptr;
@@ -278,6 +295,7 @@ struct ks_mat {
   ks::CsrDev T;
   bool has_T = false;
   unsigned flags = 0;
+  ks::DistInfo *dist = nullptr;  // rows of a split solve; null on one GPU
 };
 
 struct ks_vec {

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "ks_dist.cuh"
 #include "ks_kernels.cuh"
 #include "ks_ops.cuh"
 
@@ -203,18 +204,19 @@ __global__ void k_to_bf16(const double *__restrict__ a, __nv_bfloat16 *__restric
     b[i] = __float2bfloat16_rn((float)a[i]);
 }
 
-// Checks every column index (0 <= col < n) and stores col - row as int16
-// where it fits: flags |= 1 for a column out of range, |= 2 for an offset
-// outside [-32768, 32767] (col16 is then discarded by the caller).
-__global__ void k_col16(const int *__restrict__ ptr, const int *__restrict__ col, int n,
-                        short *__restrict__ col16, int *flags) {
+// Checks every column index (cmin <= col < cmax) and stores col - row as
+// int16 where it fits: flags |= 1 for a column out of range, |= 2 for an
+// offset outside [-32768, 32767] (col16 is then discarded by the caller).
+// Rows of a split solve store col - r0, so col - row is the global offset.
+__global__ void k_col16(const int *__restrict__ ptr, const int *__restrict__ col, int n, long long cmin,
+                        long long cmax, short *__restrict__ col16, int *flags) {
   int bad = 0;
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
        r += (long long)gridDim.x * blockDim.x) {
     const int j1 = ptr[r + 1];
     for (int j = ptr[r]; j < j1; j++) {
       const int c = col[j];
-      if (c < 0 || c >= n) {
+      if (c < cmin || c >= cmax) {
         bad |= 1;
         continue;
       }
@@ -254,7 +256,9 @@ static ks_status alloc_csr(ks_ctx *ctx, CsrDev &A, int n, long long nnz) {
   return KS_OK;
 }
 
-static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, unsigned flags) {
+static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, unsigned flags, long long cmin = 0,
+                            long long cmax = -1) {
+  if (cmax < 0) cmax = A.n;
   std::vector<int> rb = row_blocks(host_ptr, A.n);
   A.nrb = (int)rb.size() - 1;
   KS_CUDA(ctx, cudaMalloc(&A.rb, sizeof(int) * rb.size()));
@@ -276,7 +280,7 @@ static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, uns
     KS_CUDA(ctx, cudaMalloc(&d_flags, sizeof(int)));
     cudaError_t e = cudaMemsetAsync(d_flags, 0, sizeof(int), ctx->stream);
     if (e == cudaSuccess) {
-      k_col16<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.n, A.col16, d_flags);
+      k_col16<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.n, cmin, cmax, A.col16, d_flags);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h_flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
@@ -437,6 +441,12 @@ ks_status ks_ctx_create(int device, ks_ctx **out) {
                     cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
     return fail(KS_OUT_OF_MEMORY);
   std::memset(ctx->h_flags, 0, sizeof(int) * ctx->nflags);
+  if (cudaHostAlloc(&ctx->h_snap, sizeof(int) * ctx->nflags, cudaHostAllocMapped | cudaHostAllocPortable) !=
+          cudaSuccess ||
+      cudaHostGetDevicePointer((void **)&ctx->d_snap, ctx->h_snap, 0) != cudaSuccess)
+    return fail(KS_OUT_OF_MEMORY);
+  std::memset(ctx->h_snap, 0, sizeof(int) * ctx->nflags);
+  if (cudaMalloc(&ctx->d_stage, sizeof(double) * kStageLen) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
   ctx->flag_events = new cudaEvent_t[ctx->nflags];
   for (int i = 0; i < ctx->nflags; i++) {
     if (cudaEventCreateWithFlags(&ctx->flag_events[i], cudaEventDisableTiming) != cudaSuccess)
@@ -461,6 +471,8 @@ ks_status ks_ctx_destroy(ks_ctx *ctx) {
   cudaFree(ctx->d_err);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->h_flags) cudaFreeHost(ctx->h_flags);
+  if (ctx->h_snap) cudaFreeHost(ctx->h_snap);
+  cudaFree(ctx->d_stage);
   if (ctx->flag_events) {
     for (int i = 0; i < ctx->nflags; i++)
       if (ctx->flag_events[i]) cudaEventDestroy(ctx->flag_events[i]);
@@ -544,6 +556,7 @@ ks_status ks_mat_destroy(ks_mat *m) {
   }
   free_csr(m->A);
   free_csr(m->T);
+  delete m->dist;
   delete m;
   return KS_OK;
 }
@@ -556,6 +569,117 @@ ks_status ks_mat_info(const ks_mat *m, int64_t *n, int64_t *nnz, int64_t *row_bl
   return KS_OK;
 }
 
+// ============================================================= C ABI: split rows
+// Uploads one rank's rows of a row-split matrix (global column indices) and,
+// for BiCG-type methods, the same rows of A^T; exchanges every rank's rows
+// and windows once to build the halo plans.
+static ks_status upload_rows(ks_ctx *ctx, CsrDev &A, long long nloc, const int32_t *ptr, const int32_t *col,
+                             const double *val, long long r0, long long lo, long long hi, unsigned flags) {
+  const long long j0 = ptr[0], nnz = ptr[nloc] - j0;
+  std::vector<int32_t> lp((size_t)nloc + 1), lc((size_t)nnz);
+  for (long long i = 0; i <= nloc; i++) lp[(size_t)i] = (int32_t)(ptr[i] - j0);
+  for (long long j = 0; j < nnz; j++) lc[(size_t)j] = (int32_t)(col[j] - r0);
+  KS_TRY(alloc_csr(ctx, A, (int)nloc, nnz));
+  KS_CUDA(ctx, cudaMemcpyAsync(A.ptr, lp.data(), sizeof(int) * (size_t)(nloc + 1), cudaMemcpyHostToDevice, ctx->stream));
+  if (nnz > 0) {
+    KS_CUDA(ctx, cudaMemcpyAsync(A.col, lc.data(), sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream));
+    KS_CUDA(ctx, cudaMemcpyAsync(A.val, val, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  return finish_csr(ctx, A, lp.data(), flags, lo - r0, hi - r0);  // synchronises: lp, lc may go
+}
+
+static ks_status plan_of(ks_ctx *ctx, const std::vector<long long> &all, int P, int rank, int lo_i, HaloPlan &plan) {
+  std::vector<int64_t> rs((size_t)P + 1), lo((size_t)P), hi((size_t)P), sl(P), sh(P), rl(P), rh(P);
+  for (int q = 0; q < P; q++) {
+    rs[(size_t)q] = all[(size_t)q * 6 + 0];
+    lo[(size_t)q] = all[(size_t)q * 6 + lo_i];
+    hi[(size_t)q] = all[(size_t)q * 6 + lo_i + 1];
+  }
+  rs[(size_t)P] = all[(size_t)(P - 1) * 6 + 1];
+  const ks_status s = ks_halo_plan(P, rank, rs.data(), lo.data(), hi.data(), sl.data(), sh.data(), rl.data(), rh.data());
+  if (s != KS_OK) return set_error(ctx, s, "halo plan: windows do not cover the rows");
+  plan.row_start.assign(rs.begin(), rs.end());
+  plan.peer.resize((size_t)P);
+  for (int q = 0; q < P; q++) plan.peer[(size_t)q] = HaloRange{sl[q], sh[q], rl[q], rh[q]};
+  return KS_OK;
+}
+
+ks_status ks_dist_upload(ks_ctx *ctx, ks_comm *comm, int64_t n_global, int64_t r0, int64_t r1, const int32_t *ptr,
+                         const int32_t *col, const double *val, const int32_t *tptr, const int32_t *tcol,
+                         const double *tval, unsigned flags, ks_mat **out) {
+  if (!ctx || !comm || !out || !ptr || comm->ctx != ctx) return KS_BAD_INPUT;
+  *out = nullptr;
+  const bool want_t = (flags & KS_MAT_TRANSPOSE) != 0;
+  if (want_t && !tptr) return set_error(ctx, KS_BAD_INPUT, "split rows with KS_MAT_TRANSPOSE need the rows of A^T");
+  if (n_global < 1 || n_global >= (1LL << 31) - 1 || r0 < 0 || r1 < r0 || r1 > n_global)
+    return set_error(ctx, KS_BAD_INPUT, "split rows: need 0 <= r0 <= r1 <= n_global < 2^31 - 1");
+  const long long nloc = r1 - r0;
+  auto check_rows = [&](const int32_t *p, const int32_t *c, const double *v) -> ks_status {
+    for (long long i = 0; i < nloc; i++)
+      if (p[i + 1] < p[i]) return set_error(ctx, KS_BAD_INPUT, "split rows: ptr must be non-decreasing");
+    if (p[nloc] > p[0] && (!c || !v)) return KS_BAD_INPUT;
+    for (long long j = 0; j < (long long)p[nloc] - p[0]; j++)
+      if (c[j] < 0 || c[j] >= n_global) return set_error(ctx, KS_BAD_INPUT, "column index out of range");
+    return KS_OK;
+  };
+  KS_CUDA(ctx, cudaSetDevice(ctx->device));
+  KS_TRY(check_rows(ptr, col, val));
+  if (want_t) KS_TRY(check_rows(tptr, tcol, tval));
+  // every rank's rows and windows: r0 r1 lo hi tlo thi
+  int64_t lo = r0, hi = r1, tlo = r0, thi = r1;
+  KS_TRY(ks_halo_window(r0, r1, ptr, col, &lo, &hi));
+  if (want_t) KS_TRY(ks_halo_window(r0, r1, tptr, tcol, &tlo, &thi));
+  const long long mine[6] = {r0, r1, lo, hi, tlo, thi};
+  std::vector<long long> all((size_t)comm->nranks * 6);
+  KS_TRY(comm->allgather_host(mine, 6, all.data()));
+  const int P = comm->nranks;
+  if (all[0] != 0 || all[(size_t)(P - 1) * 6 + 1] != n_global)
+    return set_error(ctx, KS_BAD_INPUT, "split rows: the ranks' rows must cover 0..n_global in rank order");
+  for (int q = 1; q < P; q++)
+    if (all[(size_t)q * 6] != all[(size_t)(q - 1) * 6 + 1])
+      return set_error(ctx, KS_BAD_INPUT, "split rows: the ranks' rows must be contiguous in rank order");
+  auto *d = new DistInfo();
+  d->comm = comm;
+  d->n_global = n_global;
+  d->r0 = r0;
+  d->r1 = r1;
+  d->lo = lo;
+  d->hi = hi;
+  d->tlo = tlo;
+  d->thi = thi;
+  d->ext_lo = std::min(lo, tlo);
+  d->ext_hi = std::max(hi, thi);
+  ks_mat *m = new ks_mat();
+  m->ctx = ctx;
+  m->flags = flags;
+  m->dist = d;
+  ks_status s = plan_of(ctx, all, P, comm->rank, 2, d->planA);
+  if (s == KS_OK && want_t) s = plan_of(ctx, all, P, comm->rank, 4, d->planT);
+  if (s == KS_OK) s = upload_rows(ctx, m->A, nloc, ptr, col, val, r0, lo, hi, flags);
+  if (s == KS_OK && want_t) {
+    s = upload_rows(ctx, m->T, nloc, tptr, tcol, tval, r0, tlo, thi, flags);
+    m->has_T = s == KS_OK;
+  }
+  if (s != KS_OK) {
+    ks_mat_destroy(m);
+    return s;
+  }
+  *out = m;
+  return KS_OK;
+}
+
+ks_status ks_mat_dist_info(const ks_mat *m, int64_t *n_global, int64_t *r0, int64_t *r1, int64_t *ext_lo,
+                           int64_t *ext_hi) {
+  if (!m) return KS_BAD_INPUT;
+  const DistInfo *d = m->dist;
+  if (n_global) *n_global = d ? d->n_global : m->A.n;
+  if (r0) *r0 = d ? d->r0 : 0;
+  if (r1) *r1 = d ? d->r1 : m->A.n;
+  if (ext_lo) *ext_lo = d ? d->ext_lo : 0;
+  if (ext_hi) *ext_hi = d ? d->ext_hi : m->A.n;
+  return KS_OK;
+}
+
 ks_status ks_mat_index_bytes(const ks_mat *m, int *a_bytes, int *t_bytes) {
   if (!m) return KS_BAD_INPUT;
   if (a_bytes) *a_bytes = m->A.col16 ? 2 : 4;
@@ -565,6 +689,7 @@ ks_status ks_mat_index_bytes(const ks_mat *m, int *a_bytes, int *t_bytes) {
 
 ks_status ks_mat_transpose_download(const ks_mat *m, int32_t *tptr, int32_t *trow, double *tval) {
   if (!m || !m->has_T) return m ? set_error(m->ctx, KS_BAD_INPUT, "matrix has no transpose") : KS_BAD_INPUT;
+  if (m->dist) return set_error(m->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");
   ks_ctx *ctx = m->ctx;
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (tptr) KS_CUDA(ctx, cudaMemcpy(tptr, m->T.ptr, sizeof(int) * (size_t)(m->T.n + 1), cudaMemcpyDeviceToHost));

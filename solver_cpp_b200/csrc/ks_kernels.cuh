@@ -7,6 +7,7 @@
 #include <type_traits>
 
 #include "ks_common.cuh"
+#include "ks_dist.cuh"
 #include "ks_spmv_tma.cuh"
 
 namespace ks {
@@ -218,13 +219,73 @@ inline int spmv_tma_ctas_per_sm(int device) {
   return per_sm[device & 63];
 }
 
+template <class Op>
+inline void launch_scalar(ks_ctx *ctx, const Op &op, Stop stop) {
+  launch_k(ctx, scalar_kernel<Op>, dim3(1), dim3(32), 0, op, stop);
+}
+
+// ------------------------------------------------------------------ split solves
+// In a row-split solve (ctx->red_comm set) a kernel's reductions cover this
+// rank's rows only. The kernel then leaves its sums in ctx->d_stage instead of
+// running its scalar step; the sums are added over the ranks on the stream,
+// and the scalar step runs afterwards on every rank with the same totals, so
+// every rank takes the same decisions.
+template <class Op>
+struct StageSums : Op {
+  double *stage;
+  __device__ void finish(const double (&s)[Op::ND > 0 ? Op::ND : 1]) const {
+#pragma unroll
+    for (int d = 0; d < Op::ND; d++) stage[d] = s[d];
+  }
+};
+
+template <class Op>
+struct FinishSummed {
+  Op op;
+  const double *stage;
+  __device__ void run() const {
+    double s[Op::ND > 0 ? Op::ND : 1];
+#pragma unroll
+    for (int d = 0; d < Op::ND; d++) s[d] = stage[d];
+    op.finish(s);
+  }
+};
+
+inline void note_dist(ks_ctx *ctx, ks_status s) {
+  if (s != KS_OK && ctx->dist_status == KS_OK) ctx->dist_status = s;
+}
+
+template <class Op, class F>
+inline void with_rank_sums(ks_ctx *ctx, const Op &op, Stop stop, F &&launch) {
+  if constexpr (Op::ND > 0) {
+    if (ctx->red_comm) {
+      StageSums<Op> w;
+      static_cast<Op &>(w) = op;
+      w.stage = ctx->d_stage;
+      launch(w);
+      note_dist(ctx, ctx->red_comm->allreduce(ctx->d_stage, Op::ND));
+      launch_scalar(ctx, FinishSummed<Op>{op, ctx->d_stage}, stop);
+      return;
+    }
+  }
+  launch(op);
+}
+
 template <int NV, class MT, class IT, class GX, class Epi>
-inline void launch_spmv_i(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
+inline void launch_spmv_k(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
                           int slot) {
   const int per_sm = spmv_tma_ctas_per_sm<NV, MT, IT, GX, Epi>(ctx->device);
   const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
   launch_k(ctx, spmv_tma_kernel<NV, MT, IT, GX, Epi>, dim3(grid), dim3(kThreads), spmv_tma_smem<MT, IT>(),
            tview<MT, IT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err);
+}
+
+template <int NV, class MT, class IT, class GX, class Epi>
+inline void launch_spmv_i(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi_in, Stop stop,
+                          int slot) {
+  with_rank_sums(ctx, epi_in, stop, [&](const auto &epi) {
+    launch_spmv_k<NV, MT, IT, GX, std::decay_t<decltype(epi)>>(ctx, A, g0, g1, epi, stop, slot);
+  });
 }
 
 // 16-bit column offsets when the matrix has them, else int32 columns.
@@ -249,11 +310,14 @@ inline void launch_spmv2(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x
 }
 
 template <class Op>
-inline void launch_vec(ks_ctx *ctx, long long n, const Op &op, Stop stop, int slot = 0) {
+inline void launch_vec(ks_ctx *ctx, long long n, const Op &op_in, Stop stop, int slot = 0) {
   long long need = (n + kThreads - 1) / kThreads;
   int grid = red_grid(ctx);
   if (need < grid) grid = (int)(need > 0 ? need : 1);
-  launch_k(ctx, vec_kernel<Op>, dim3(grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
+  with_rank_sums(ctx, op_in, stop, [&](const auto &op) {
+    using O = std::decay_t<decltype(op)>;
+    launch_k(ctx, vec_kernel<O>, dim3(grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
+  });
 }
 
 // k_hint: the number of basis vectors, or a bound when the kernel reads it
@@ -267,12 +331,10 @@ inline void launch_basis(ks_ctx *ctx, long long n, int k_hint, const Op &op, Sto
   const long long cap = k_hint >= 64 ? (long long)(ctx->partials_len / (Op::ND > 0 ? Op::ND : 1))
                                      : (long long)ctx->num_sms * 8;
   grid = std::max(1LL, std::min(grid, cap));
-  launch_k(ctx, basis_kernel<Op>, dim3((unsigned)grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
-}
-
-template <class Op>
-inline void launch_scalar(ks_ctx *ctx, const Op &op, Stop stop) {
-  launch_k(ctx, scalar_kernel<Op>, dim3(1), dim3(32), 0, op, stop);
+  with_rank_sums(ctx, op, stop, [&](const auto &o) {
+    using O = std::decay_t<decltype(o)>;
+    launch_k(ctx, basis_kernel<O>, dim3((unsigned)grid), dim3(kThreads), 0, o, n, stop, red_of(ctx, slot));
+  });
 }
 
 }  // namespace ks

@@ -166,6 +166,27 @@ struct PutArray {  // out[w * stride_w + i * stride_i] = value
   __device__ void put(int w, int i, double v) const { out[w * stride_w + i * stride_i] = v; }
 };
 
+// Split solves: the block dot leaves its results in the stage (w * k + i)
+// and, once they are summed over the ranks, a scalar step hands each to the
+// real epilogue.
+template <class Epi>
+struct StagePuts {
+  double *stage;
+  int k;
+  __device__ void put(int w, int i, double v) const { stage[(long long)w * k + i] = v; }
+};
+
+template <class Epi>
+struct PutSummed {
+  Epi epi;
+  const double *stage;
+  int nw, k;
+  __device__ void run() const {
+    for (int w = 0; w < nw; w++)
+      for (int i = 0; i < k; i++) epi.put(w, i, stage[(long long)w * k + i]);
+  }
+};
+
 template <int NW, class VT, class Epi>
 inline ks_status launch_block_dot(ks_ctx *ctx, const VT *V, long long ld, int k, const VT *W0,
                                   const VT *W1, long long n, const Epi &epi, Stop stop) {
@@ -177,6 +198,14 @@ inline ks_status launch_block_dot(ks_ctx *ctx, const VT *V, long long ld, int k,
   const long long need = (n + kThreads - 1) / kThreads;
   if (need < gx) gx = (int)std::max<long long>(need, 1);
   dim3 grid(groups, gx);
+  if (ctx->red_comm) {  // split solve: results summed over the ranks, then put
+    if (NW * k > kStageLen) return set_error(ctx, KS_BAD_INPUT, "block dot: too many results for a split solve");
+    launch_k(ctx, block_dot_kernel<NW, VT, StagePuts<Epi>>, grid, dim3(kThreads), 0, V, ld, k, W0, W1, n,
+             StagePuts<Epi>{ctx->d_stage, k}, stop, ctx->partials, ctx->counters + 16);
+    note_dist(ctx, ctx->red_comm->allreduce(ctx->d_stage, NW * k));
+    launch_scalar(ctx, PutSummed<Epi>{epi, ctx->d_stage, NW, k}, stop);
+    return KS_OK;
+  }
   launch_k(ctx, block_dot_kernel<NW, VT, Epi>, grid, dim3(kThreads), 0, V, ld, k, W0, W1, n, epi, stop,
            ctx->partials, ctx->counters + 16);
   return KS_OK;

@@ -2,6 +2,7 @@
 // operations, k-skip matrix powers and Gram values, adjoint pattern gather.
 #include <cmath>
 
+#include "ks_dist.cuh"
 #include "ks_ops.cuh"
 
 namespace ks {
@@ -64,6 +65,19 @@ ks_status ks_spmv_values(const ks_mat *mat, int trans, ks_precision values, cons
   const CsrDev &A = *pick(mat, trans);
   if (x->n < A.n || y->n < A.n || x->type != y->type)
     return set_error(ctx, KS_BAD_INPUT, "spmv: vector length or type mismatch");
+  if (mat->dist) {  // split rows: x into a window-sized buffer, halo from the peers
+    const DistInfo &d = *mat->dist;
+    const size_t es = elem_size(x->type);
+    void *buf = nullptr;
+    KS_TRY(pool_get(ctx, es * (size_t)d.ld() + 64, &buf));
+    char *xl = (char *)buf + d.off() * (long long)es;
+    const cudaError_t e = cudaMemcpyAsync(xl, x->d, es * (size_t)A.n, cudaMemcpyDeviceToDevice, ctx->stream);
+    ks_status s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "spmv copy");
+    if (s == KS_OK) s = d.comm->exchange(trans ? d.planT : d.planA, xl, es);
+    if (s == KS_OK) s = spmv_any(ctx, A, values, x->type, xl, y->d, Stop{nullptr, nullptr});
+    pool_release(ctx, buf);  // later users of the pool are queued behind this SpMV
+    return s;
+  }
   return spmv_any(ctx, A, values, x->type, x->d, y->d, Stop{nullptr, nullptr});
 }
 
@@ -219,6 +233,7 @@ extern "C" {
 
 ks_status ks_matpow(const ks_mat *mat, const ks_vec *r, const ks_vec *p, int k, ks_vec *Ar, ks_vec *Ap) {
   if (!mat || !r || !p || !Ar || !Ap || k < 0) return KS_BAD_INPUT;
+  if (mat->dist) return set_error(mat->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");
   ks_ctx *ctx = mat->ctx;
   const long long n = mat->A.n;
   if (r->type != KS_FP64 || p->type != KS_FP64 || Ar->type != KS_FP64 || Ap->type != KS_FP64 ||
@@ -270,6 +285,7 @@ ks_status ks_gram_bicg(const ks_vec *Ar, const ks_vec *Ap, const ks_vec *rs, con
 
 ks_status ks_pattern_grad(const ks_mat *mat, const ks_vec *lambda, const ks_vec *x, ks_vec *grad_val) {
   if (!mat || !lambda || !x || !grad_val) return KS_BAD_INPUT;
+  if (mat->dist) return set_error(mat->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");
   ks_ctx *ctx = mat->ctx;
   if (lambda->type != KS_FP64 || x->type != KS_FP64 || grad_val->type != KS_FP64 ||
       lambda->n != mat->A.n || x->n != mat->A.n || grad_val->n < mat->A.nnz)
@@ -283,6 +299,7 @@ ks_status ks_pattern_grad(const ks_mat *mat, const ks_vec *lambda, const ks_vec 
 ks_status ks_check_error(const ks_mat *mat, const ks_vec *b, const ks_vec *x, double *log10_ratio,
                          double *rel) {
   if (!mat || !b || !x || b->type != KS_FP64 || x->type != KS_FP64) return KS_BAD_INPUT;
+  if (mat->dist) return set_error(mat->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");  // ks_solve reports it
   ks_ctx *ctx = mat->ctx;
   launch_spmv<double, double>(ctx, mat->A, (const double *)x->d,
                               ResidEpi<double>{(const double *)b->d, nullptr, ctx->d_result},

@@ -104,11 +104,23 @@ struct Env {
   bool outer = false;  // drives host polling
   Params sp{};
   bool faithful = false;
-  long long n = 0;
+  long long n = 0;    // this rank's vector length
+  long long ld = 0;   // workspace slot length (n, or the window of a split solve)
+  long long off = 0;  // the vector's offset in its slot
   volatile int *hflag = nullptr;  // host view of st->host_done (outer only)
   int lookahead = 8;
+  // row-split solve: the transport and the halo plans of A and AT
+  ks_comm *comm = nullptr;
+  const HaloPlan *planA = nullptr, *planT = nullptr;
   Stop stop() const { return Stop{&st->k.done, outer_done}; }
+  // Fill the halo of an SpMV input from the peers (it is written, though
+  // the method treats the vector as read-only: the halo is not its data).
+  void halo(const CsrDev &M, const VT *x) const {
+    if (comm) note_dist(ctx, comm->exchange(&M == A ? *planA : *planT, (void *)x, sizeof(VT)));
+  }
 };
+
+__global__ void k_snapshot(const int *done, int *out) { *out = *(volatile const int *)done; }
 
 // Host-side bounded lookahead: after each issued iteration, wait for the one
 // `la` iterations back and read the mapped done flag.
@@ -117,8 +129,25 @@ struct Poller {
   volatile int *flag;
   int la;
   long long issued = 0;
+  // Row-split solve: every rank must stop issuing after the same iteration,
+  // or their collectives would no longer pair up. Every `la` iterations a
+  // one-thread kernel copies `done` into a mapped ring; the host decides from
+  // the copy one chunk back, which holds the same value on every rank.
+  bool step_split() {
+    issued++;
+    if (issued % la) return false;
+    const long long m = issued / la;
+    const int R = ctx->nflags;
+    ctx->launches++;
+    k_snapshot<<<1, 1, 0, ctx->stream>>>(ctx->poll_done, ctx->d_snap + (m % R));
+    cudaEventRecord(ctx->flag_events[m % R], ctx->stream);
+    if (m < 2) return false;
+    cudaEventSynchronize(ctx->flag_events[(m - 1) % R]);
+    return ((volatile int *)ctx->h_snap)[(m - 1) % R] != 0;
+  }
   bool step() {
     if (!flag) return false;
+    if (ctx->red_comm) return step_split();
     const int R = ctx->nflags;
     cudaEventRecord(ctx->flag_events[issued % R], ctx->stream);
     issued++;
@@ -134,6 +163,7 @@ struct Poller {
 // SpMV with an epilogue, dispatched on the vector type and value copy.
 template <class VT, class Epi>
 inline void mv(const Env<VT> &E, const CsrDev &M, const VT *x, const Epi &epi) {
+  E.halo(M, x);
   if constexpr (std::is_same<VT, double>::value) {
     launch_spmv<double, double>(E.ctx, M, x, epi, E.stop());
   } else {
@@ -444,10 +474,10 @@ inline bool defer_x(const Env<VT> &E, int method) {
 template <class VT>
 struct DirRing {
   VT *P;
-  long long n;
+  long long ld;  // slot stride
   int D;
   double *alpha;
-  VT *slot(long long L) const { return P + ((L - 1) % D) * n; }
+  VT *slot(long long L) const { return P + ((L - 1) % D) * ld; }
   double *aslot(long long L) const { return alpha + (L - 1) % D; }
 };
 
@@ -537,23 +567,28 @@ struct XpbyToOp {
 // After iteration L: apply the ring once it is full.
 template <class VT>
 inline void ring_step(const Env<VT> &E, const DirRing<VT> &R, VT *x, long long L) {
-  if (L % R.D == 0) launch_basis(E.ctx, E.n, R.D, FlushXOp<VT>{x, R.P, R.n, R.alpha, E.st}, E.stop());
+  if (L % R.D == 0) launch_basis(E.ctx, E.n, R.D, FlushXOp<VT>{x, R.P, R.ld, R.alpha, E.st}, E.stop());
 }
 
 // After the loop: apply what is pending. Runs after the method has stopped
 // (its own done flag set), so only the outer method's flag stops it.
 template <class VT>
 inline void ring_final(const Env<VT> &E, const DirRing<VT> &R, VT *x) {
-  launch_basis(E.ctx, E.n, R.D, FlushXOp<VT>{x, R.P, R.n, R.alpha, E.st}, Stop{nullptr, E.outer_done});
+  launch_basis(E.ctx, E.n, R.D, FlushXOp<VT>{x, R.P, R.ld, R.alpha, E.st}, Stop{nullptr, E.outer_done});
 }
 
+// Carves vectors out of one workspace block: slots of ld entries, the
+// vector's own entries at offset `off` (a row-split solve keeps its halo
+// around them; on one GPU ld = n, off = 0). Consecutive slots of one take()
+// form a basis with stride ld.
 template <class VT>
-struct Ws {  // carve n-length vectors out of one workspace block
+struct Ws {
   VT *base;
-  long long n;
+  long long ld;
+  long long off;
   int used = 0;
   VT *take(int count = 1) {
-    VT *p = base + (long long)used * n;
+    VT *p = base + (long long)used * ld + off;
     used += count;
     return p;
   }
@@ -573,11 +608,11 @@ ks_status init_state(const Env<VT> &E, const VT *b) {
 // removes 8 us.)
 template <class VT>
 ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
-  Ws<VT> W{ws, E.n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take();
   const bool defer = defer_x(E, KS_CG);
   const int D = defer ? dir_ring(E.sp) : 1;  // D = 1: p updated in place
-  DirRing<VT> R{W.take(D), E.n, D, dws};
+  DirRing<VT> R{W.take(D), E.ld, D, dws};
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CG});
@@ -665,11 +700,11 @@ struct Xpby2ToOp {
 
 template <class VT>
 ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
-  Ws<VT> W{ws, E.n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take(), *s = W.take();
   const bool defer = defer_x(E, KS_CR);
   const int D = defer ? dir_ring(E.sp) : 1;
-  DirRing<VT> R{W.take(D), E.n, D, dws};
+  DirRing<VT> R{W.take(D), E.ld, D, dws};
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CHECK});
@@ -735,11 +770,11 @@ struct Xpby2PlainOp {
 
 template <class VT>
 ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
-  Ws<VT> W{ws, E.n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *rs = W.take(), *ps = W.take(), *mvv = W.take();
   const bool defer = defer_x(E, KS_BICG);
   const int D = defer ? dir_ring(E.sp) : 1;
-  DirRing<VT> R{W.take(D), E.n, D, dws};
+  DirRing<VT> R{W.take(D), E.ld, D, dws};
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   // (r*, r) = (r, r) at the start
@@ -873,9 +908,9 @@ struct SetLoopOp {
 template <class VT>
 ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws,
                        InnerRunner<VT> *inner) {
-  const long long n = E.n;
+  const long long n = E.n, ld = E.ld;
   const int m = (int)E.sp.restart;
-  Ws<VT> W{ws, n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *Av = W.take(), *z = W.take();
   VT *P = W.take(m), *Q = W.take(m);
   double *qq = dws, *beta = dws + m;
@@ -898,7 +933,7 @@ ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws
     mv(E, *E.A, (const VT *)P, GcrQ0Epi<VT>{r, Q, qq, E.st});
     for (int k = 0; k < m; k++) {
       const bool last = (k == m - 1);
-      vec(E, GcrXrOp<VT>{x, r, P + (long long)k * n, Q + (long long)k * n, E.st, last ? 1 : 0});
+      vec(E, GcrXrOp<VT>{x, r, P + (long long)k * ld, Q + (long long)k * ld, E.st, last ? 1 : 0});
       issued_steps++;
       if (last) break;
       const VT *znew = r;
@@ -907,11 +942,11 @@ ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws
         znew = z;
       }
       mv(E, *E.A, znew, StoreEpi<VT, VT>{Av});
-      KS_TRY(launch_block_dot<1, VT>(E.ctx, Q, n, k + 1, Av, nullptr, n, GcrBetaPut{beta, qq, E.st},
+      KS_TRY(launch_block_dot<1, VT>(E.ctx, Q, ld, k + 1, Av, nullptr, n, GcrBetaPut{beta, qq, E.st},
                                      E.stop()));
       launch_basis(E.ctx, n, k + 1,
-                   GcrPQOp<VT>{P, Q, n, k + 1, beta, znew, Av, r, P + (long long)(k + 1) * n,
-                               Q + (long long)(k + 1) * n, qq + k + 1, E.st},
+                   GcrPQOp<VT>{P, Q, ld, k + 1, beta, znew, Av, r, P + (long long)(k + 1) * ld,
+                               Q + (long long)(k + 1) * ld, qq + k + 1, E.st},
                    E.stop());
       // Each step is one check of the loop counter, so the method has
       // stopped on the device after at most maxloop steps.
@@ -1080,10 +1115,10 @@ struct GmMarkFinal {
 template <class VT>
 ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws,
                          InnerRunner<VT> *inner) {
-  const long long n = E.n;
+  const long long n = E.n, ld = E.ld;
   const int m = (int)E.sp.restart;
   if (m < 2) return set_error(E.ctx, KS_BAD_INPUT, "GMRES needs restart >= 2");
-  Ws<VT> W{ws, n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *w = W.take(), *z = W.take();
   VT *V = W.take(m + 1);
   VT *Z = inner ? W.take(m) : nullptr;
@@ -1106,17 +1141,17 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
     vec(E, ScaleOp<VT>{r, V, &E.st->k.s[S_T]});
     launch_scalar(E.ctx, GmCycleOp{g, E.st}, E.stop());
     for (int k = 0; k < m - 1; k++) {
-      const VT *vk = V + (long long)k * n;
+      const VT *vk = V + (long long)k * ld;
       if (inner) {
-        inner->solve(vk, Z + (long long)k * n);
-        mv(E, *E.A, (const VT *)(Z + (long long)k * n), StoreEpi<VT, VT>{w});
+        inner->solve(vk, Z + (long long)k * ld);
+        mv(E, *E.A, (const VT *)(Z + (long long)k * ld), StoreEpi<VT, VT>{w});
       } else {
         mv(E, *E.A, vk, StoreEpi<VT, VT>{w});
       }
-      KS_TRY(launch_block_dot<1, VT>(E.ctx, V, n, k + 1, w, nullptr, n, GmPutH{g.H, m, k}, E.stop()));
-      launch_basis(E.ctx, n, k + 1, BlockAxpyOp<VT>{V, n, k + 1, g.H + k, m, w, &E.st->k.s[S_T], 1},
+      KS_TRY(launch_block_dot<1, VT>(E.ctx, V, ld, k + 1, w, nullptr, n, GmPutH{g.H, m, k}, E.stop()));
+      launch_basis(E.ctx, n, k + 1, BlockAxpyOp<VT>{V, ld, k + 1, g.H + k, m, w, &E.st->k.s[S_T], 1},
                    E.stop());  // s[T] = |w|
-      vec(E, ScaleOp<VT>{w, V + (long long)(k + 1) * n, &E.st->k.s[S_T]});
+      vec(E, ScaleOp<VT>{w, V + (long long)(k + 1) * ld, &E.st->k.s[S_T]});
       launch_scalar(E.ctx, GmGivensOp{g, E.st, k, k + 1 < m - 1 ? 1 : 0}, E.stop());
       issued++;
       if (E.outer && P.step()) {
@@ -1131,13 +1166,13 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
     if (stop_host) break;
     // end of cycle (gmres.cpp:409-421)
     launch_scalar(E.ctx, GmHyeOp{g, E.st, m - 1, 0}, E.stop());
-    launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, n, m - 1, g.y, x, E.st, 0, 0}, E.stop());
+    launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, ld, m - 1, g.y, x, E.st, 0, 0}, E.stop());
     if (E.outer && P.step()) break;
   }
   // The step that stopped the method (converged or maxloop) assembles x;
   // these kernels are gated by the stop reason, not by `done`.
   launch_scalar(E.ctx, GmHyeOp{g, E.st, -1, 1}, Stop{nullptr, E.outer_done});
-  launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, n, 0, g.y, x, E.st, 1, E.faithful ? 1 : 0},
+  launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, ld, 0, g.y, x, E.st, 1, E.faithful ? 1 : 0},
                Stop{nullptr, E.outer_done});
   launch_scalar(E.ctx, GmMarkFinal{E.st}, Stop{nullptr, E.outer_done});
   return KS_OK;
@@ -1258,8 +1293,10 @@ struct Store2 {
 
 template <class VT>
 void matpow_t(const Env<VT> &E, const VT *r, const VT *p, int k, VT *Ar, VT *Ap) {
-  const long long n = E.n;
+  const long long n = E.n, ld = E.ld;
   auto mv2 = [&](const VT *a, const VT *b2, VT *o0, VT *o1) {
+    E.halo(*E.A, a);
+    E.halo(*E.A, b2);
     if constexpr (std::is_same<VT, double>::value) {
       launch_spmv2<double, double>(E.ctx, *E.A, a, b2, Store2<VT>{o0, o1}, E.stop());
     } else {
@@ -1271,17 +1308,17 @@ void matpow_t(const Env<VT> &E, const VT *r, const VT *p, int k, VT *Ar, VT *Ap)
   };
   mv2(r, p, Ar, Ap);
   for (int i = 1; i < 2 * k + 1; i++)
-    mv2(Ar + (long long)(i - 1) * n, Ap + (long long)(i - 1) * n, Ar + (long long)i * n,
-        Ap + (long long)i * n);
-  mv(E, *E.A, (const VT *)(Ap + (long long)(2 * k) * n), StoreEpi<VT, VT>{Ap + (long long)(2 * k + 1) * n});
+    mv2(Ar + (long long)(i - 1) * ld, Ap + (long long)(i - 1) * ld, Ar + (long long)i * ld,
+        Ap + (long long)i * ld);
+  mv(E, *E.A, (const VT *)(Ap + (long long)(2 * k) * ld), StoreEpi<VT, VT>{Ap + (long long)(2 * k + 1) * ld});
 }
 
 template <class VT>
 ks_status run_kskipcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
-  const long long n = E.n;
+  const long long n = E.n, ld = E.ld;
   const int k = E.sp.kskip;
   if (k < 0) return set_error(E.ctx, KS_BAD_INPUT, "kskip must be >= 0");
-  Ws<VT> W{ws, n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *p = W.take(), *Av = W.take();
   VT *Ar = W.take(2 * k + 1), *Ap = W.take(2 * k + 2);
   double *G = dws, *coef = dws + 6 * k + 4;
@@ -1295,8 +1332,8 @@ ks_status run_kskipcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws)
     launch_scalar(E.ctx, KsCheckOp{E.st, nloop}, E.stop());
     matpow_t(E, r, p, k, Ar, Ap);
     if (k > 0)
-      KS_TRY(launch_block_dot<1, VT>(E.ctx, Ar, n, 2 * k, r, nullptr, n, PutArray{G, 0, 1}, E.stop()));
-    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ap, n, 2 * k + 2, r, p, n,
+      KS_TRY(launch_block_dot<1, VT>(E.ctx, Ar, ld, 2 * k, r, nullptr, n, PutArray{G, 0, 1}, E.stop()));
+    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ap, ld, 2 * k + 2, r, p, n,
                                    PutArray{G + 2 * k, 2 * k + 2, 1}, E.stop()));
     launch_scalar(E.ctx, KsCgRecOp{E.st, G, coef, k, E.sp.fix, E.faithful ? 0 : 1}, E.stop());
     for (int i = 0; i <= k; i++) {
@@ -1367,10 +1404,10 @@ struct KsRsEpi {  // r* = -a (A^T p*) + r*
 
 template <class VT>
 ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
-  const long long n = E.n;
+  const long long n = E.n, ld = E.ld;
   const int k = E.sp.kskip;
   if (k < 0) return set_error(E.ctx, KS_BAD_INPUT, "kskip must be >= 0");
-  Ws<VT> W{ws, n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *p = W.take(), *rs = W.take(), *ps = W.take(), *Av = W.take();
   VT *Ar = W.take(2 * k + 1), *Ap = W.take(2 * k + 2);
   double *G = dws, *coef = dws + 8 * k + 6;
@@ -1384,9 +1421,9 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
     launch_scalar(E.ctx, KsCheckOp{E.st, nloop}, E.stop());
     matpow_t(E, r, p, k, Ar, Ap);
     vec(E, GammaOp<VT>{rs, r, E.st});
-    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ar, n, 2 * k + 1, rs, ps, n, PutArray{G, 2 * k + 1, 1},
+    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ar, ld, 2 * k + 1, rs, ps, n, PutArray{G, 2 * k + 1, 1},
                                    E.stop()));
-    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ap, n, 2 * k + 2, rs, ps, n,
+    KS_TRY(launch_block_dot<2, VT>(E.ctx, Ap, ld, 2 * k + 2, rs, ps, n,
                                    PutArray{G + 4 * k + 2, 2 * k + 2, 1}, E.stop()));
     launch_scalar(E.ctx, KsBicgRecOp{E.st, G, coef, k}, E.stop());
     for (int i = 0; i <= k; i++) {
@@ -1497,7 +1534,7 @@ struct RzOp {  // rr2 = (r, z); beta = rr2 / rr; rr = rr2   (vpcg.cpp:733-745)
 
 template <class VT>
 ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT> *inner) {
-  Ws<VT> W{ws, E.n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *p = W.take(), *z = W.take(), *mvv = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
@@ -1545,7 +1582,7 @@ struct VpcrMvEpi {  // Av = A z; zaz(2) = (z, Av); init: Ap = Av, alpha from (Ap
 
 template <class VT>
 ks_status run_vpcr(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT> *inner) {
-  Ws<VT> W{ws, E.n};
+  Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *p = W.take(), *z = W.take(), *Av = W.take(), *Ap = W.take();
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
@@ -1657,7 +1694,21 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
 
   KS_CUDA(ctx, cudaSetDevice(ctx->device));
   const long long n = A->n;
+  const DistInfo *dist = mat->dist;
+  const long long ld = dist ? dist->ld() : n, off = dist ? dist->off() : 0;
   Alloc al{ctx, {}};
+  // A row-split solve sums every reduction over the ranks while it runs.
+  struct SplitScope {
+    ks_ctx *c;
+    SplitScope(ks_ctx *c_, ks_comm *comm) : c(c_) {
+      c->red_comm = comm;
+      c->dist_status = KS_OK;
+    }
+    ~SplitScope() {
+      c->red_comm = nullptr;
+      c->poll_done = nullptr;
+    }
+  } scope(ctx, dist ? dist->comm : nullptr);
   // device state (outer, inner) and history
   DevState *st = nullptr, *ist = nullptr;
   KS_TRY(al.get(2, &st));
@@ -1683,7 +1734,13 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
 
   // workspaces
   double *ws = nullptr, *dws = nullptr;
-  KS_TRY(al.get((size_t)(vec_count(outer, outer_sp, n, sizeof(double), ctx->l2_bytes) * n), &ws));
+  KS_TRY(al.get((size_t)(vec_count(outer, outer_sp, n, sizeof(double), ctx->l2_bytes) * ld), &ws));
+  double *xs = x;  // a split solve works on a windowed copy of x (restarts multiply x)
+  if (dist) {
+    KS_TRY(al.get((size_t)ld, &xs));
+    xs += off;
+  }
+  ctx->poll_done = &st->k.done;
   KS_TRY(al.get((size_t)dws_count(outer, outer_sp), &dws));
 
   Env<double> E;
@@ -1697,6 +1754,13 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   E.sp = outer_sp;
   E.faithful = prm->reference_defects != 0;
   E.n = n;
+  E.ld = ld;
+  E.off = off;
+  if (dist) {
+    E.comm = dist->comm;
+    E.planA = trans ? &dist->planT : &dist->planA;
+    E.planT = trans ? &dist->planA : &dist->planT;
+  }
   E.hflag = (volatile int *)ctx->h_flags;
   E.lookahead = prm->poll_interval > 0 ? prm->poll_interval : (vp ? 2 : 8);
   E.lookahead = std::min(E.lookahead, ctx->nflags - 1);  // event ring size
@@ -1718,7 +1782,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
       I.outer = false;
       I.sp = inner_sp;
       I.hflag = nullptr;
-      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp, n, sizeof(double), ctx->l2_bytes) * n), &IR.ws64));
+      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp, n, sizeof(double), ctx->l2_bytes) * ld), &IR.ws64));
     } else {
       Env<float> &I = IR.E32;
       I.ctx = ctx;
@@ -1732,17 +1796,33 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
       I.sp = inner_sp;
       I.faithful = E.faithful;
       I.n = n;
+      I.ld = ld;
+      I.off = off;
+      I.comm = E.comm;
+      I.planA = E.planA;
+      I.planT = E.planT;
       I.hflag = nullptr;
-      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp, n, sizeof(float), ctx->l2_bytes) * n), &IR.ws32));
-      KS_TRY(al.get((size_t)n, &IR.b32));
-      KS_TRY(al.get((size_t)n, &IR.z32));
+      KS_TRY(al.get((size_t)(vec_count(inner, inner_sp, n, sizeof(float), ctx->l2_bytes) * ld), &IR.ws32));
+      KS_TRY(al.get((size_t)ld, &IR.b32));
+      KS_TRY(al.get((size_t)ld, &IR.z32));
+      IR.b32 += off;
+      IR.z32 += off;
     }
   }
 
   KS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  ks_status s = run_method<double>(outer, E, b, x, ws, dws, vp ? &IR : nullptr);
+  ks_status s = run_method<double>(outer, E, b, xs, ws, dws, vp ? &IR : nullptr);
   if (s == KS_OK && vp) s = IR.status;
   KS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  if (s == KS_OK && dist) {
+    // true residual |b - A x| / |b| over all ranks (not gated by `done`: the
+    // method has stopped by now), then x out of the window
+    E.halo(*A, xs);
+    launch_spmv<double, double>(ctx, *A, (const double *)xs, ResidEpi<double>{b, nullptr, ctx->d_result},
+                                Stop{nullptr, nullptr});
+    KS_CUDA(ctx, cudaMemcpyAsync(x, xs, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  if (s == KS_OK && ctx->dist_status != KS_OK) s = ctx->dist_status;
   if (s != KS_OK) {
     cudaStreamSynchronize(ctx->stream);
     return s;
@@ -1803,6 +1883,12 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     rep->spmv_count = 0;
     rep->true_res_log10 = 0.0;
     rep->true_rel_res = 0.0;
+    if (dist) {  // summed over the ranks after the solve
+      double s2[2];
+      KS_CUDA(ctx, cudaMemcpy(s2, ctx->d_result, sizeof(s2), cudaMemcpyDeviceToHost));
+      rep->true_rel_res = std::sqrt(s2[0]) / std::sqrt(s2[1]);
+      rep->true_res_log10 = std::log10(rep->true_rel_res);
+    }
   }
   return st_code;
 }
@@ -1841,7 +1927,7 @@ ks_status ks_solve(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver in
   }
   ks_status s = solve_impl(ctx, mat, outer, inner, params, (const double *)b->d, (double *)x->d, hist_iter,
                            hist_err, hist_cap, report);
-  if (report && (s == KS_OK || s == KS_NOT_CONVERGED || s == KS_BREAKDOWN || s == KS_NAN_DETECTED)) {
+  if (report && !mat->dist && (s == KS_OK || s == KS_NOT_CONVERGED || s == KS_BREAKDOWN || s == KS_NAN_DETECTED)) {
     double lg = 0, rel = 0;
     const ks_mat *m = mat;
     if (params->transpose) {
@@ -1867,21 +1953,27 @@ ks_status ks_solve(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver in
 ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
                         const ks_params *params, const double *b, double *x, int64_t *hist_iter,
                         double *hist_err, int64_t hist_cap, ks_report *report) {
-  if (!ctx || !mat || !b || !x) return KS_BAD_INPUT;
-  ks_vec *vb = nullptr, *vx = nullptr;
-  KS_TRY(ks_vec_create(ctx, mat->A.n, KS_FP64, &vb));
-  ks_status s = ks_vec_create(ctx, mat->A.n, KS_FP64, &vx);
-  if (s == KS_OK) s = ks_vec_upload(vb, b);
-  ks_status r = s;
-  if (s == KS_OK) {
-    r = ks_solve(ctx, mat, outer, inner, params, vb, vx, hist_iter, hist_err, hist_cap, report);
+  if (!ctx || !mat || !b || !x || mat->ctx != ctx) return KS_BAD_INPUT;
+  // b and x live in the context's buffer pool between calls: no device
+  // allocation (and no synchronising free) per solve
+  const long long n = mat->A.n;
+  void *buf = nullptr;
+  KS_TRY(pool_get(ctx, sizeof(double) * (size_t)(2 * n) + 256, &buf));
+  ks_vec vb, vx;
+  vb.ctx = vx.ctx = ctx;
+  vb.n = vx.n = n;
+  vb.type = vx.type = KS_FP64;
+  vb.d = buf;
+  vx.d = (char *)buf + ((sizeof(double) * (size_t)n + 255) / 256) * 256;
+  ks_status r = ks_vec_upload(&vb, b);
+  if (r == KS_OK) {
+    r = ks_solve(ctx, mat, outer, inner, params, &vb, &vx, hist_iter, hist_err, hist_cap, report);
     if (r == KS_OK || r == KS_NOT_CONVERGED || r == KS_BREAKDOWN || r == KS_NAN_DETECTED) {
-      ks_status d = ks_vec_download(vx, x);
+      const ks_status d = ks_vec_download(&vx, x);
       if (d != KS_OK) r = d;
     }
   }
-  ks_vec_destroy(vb);
-  ks_vec_destroy(vx);
+  pool_release(ctx, buf);
   return r;
 }
 
@@ -1889,6 +1981,7 @@ ks_status ks_adjoint_grad(ks_ctx *ctx, const ks_mat *mat, ks_solver solver, ks_s
                           const ks_params *params, const ks_vec *x, const ks_vec *g, ks_vec *grad_b,
                           ks_vec *grad_val, ks_report *report) {
   if (!ctx || !mat || !x || !g || x->type != KS_FP64 || g->type != KS_FP64) return KS_BAD_INPUT;
+  if (mat->dist) return set_error(mat->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");
   ks_params p;
   if (params) p = *params;
   else ks_params_default(&p);

@@ -1,0 +1,136 @@
+"""GPU: row-split solves with ranks emulated on one GPU (ks_comm_create_local).
+
+Every rank runs on its own context and host thread, exactly as one process
+per GPU would, with the halo exchange done by device copies from the peer's
+vector and the reductions summed by a kernel in rank order. The split SpMV
+must equal the whole-matrix SpMV bit for bit (rows are complete on their
+rank), every rank must take the same decisions (identical histories and
+iteration counts), and the assembled solution must agree with the one-GPU
+solve: the dots are summed in another order, so to 1e-8 relative, with
+iteration counts within 2 %.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+from solver_cpp_b200.matrices import config_problem, transpose
+
+pytestmark = pytest.mark.gpu
+
+
+def _ranks(P, fn):
+    out, errors = [None] * P, []
+
+    def work(q):
+        try:
+            out[q] = fn(q)
+        except Exception as e:  # reported below, with the rank
+            errors.append((q, repr(e)))
+
+    ts = [threading.Thread(target=work, args=(q,)) for q in range(P)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=900)
+    assert not errors, errors
+    return out
+
+
+@pytest.fixture(scope="module")
+def split3(ks):
+    ctxs = [ks.Context(0) for _ in range(3)]
+    comms = ks.Comm.local(ctxs)
+    yield ctxs, comms
+    for c in comms:
+        c.close()
+    for c in ctxs:
+        c.close()
+
+
+@pytest.mark.parametrize("prob,align", [("poisson3d", 144), ("convdiff3d", 1), ("varcoef2d", 1)])
+def test_split_spmv_is_bitwise(ks, split3, oracle, prob, align):
+    ctxs, comms = split3
+    A, _, _ = config_problem(prob, 12 if "3d" in prob else 40)
+    rs = ks.partition_rows(A.n, 3, align)
+    x = np.random.default_rng(2).standard_normal(A.n)
+
+    def rank(q):
+        ctx = ctxs[q]
+        M = ks.SplitMatrix(ctx, comms[q], A, rs[q], rs[q + 1], transpose=True)
+        X, Y = ctx.vector(x[rs[q]:rs[q + 1]]), ctx.vector(n=M.n)
+        ks.spmv(M, X, Y)
+        y = Y.numpy()
+        ks.spmv(M, X, Y, trans=True)
+        return y, Y.numpy(), M.info()["index_bytes"]
+
+    res = _ranks(3, rank)
+    P = oracle.Problem(A)
+    assert np.array_equal(np.concatenate([r[0] for r in res]), oracle.spmv(P, x))
+    assert np.array_equal(np.concatenate([r[1] for r in res]), oracle.spmv(P, x, transpose=True))
+    assert all(r[2] == 2 for r in res)  # int16 offsets survive the split
+
+
+CASES = [
+    ("poisson3d", "CG", "NONE", {}),
+    ("poisson3d", "CG", "NONE", {"x_update": 2}),
+    ("poisson3d", "CR", "NONE", {}),
+    ("convdiff3d", "BICG", "NONE", {}),
+    ("convdiff3d", "GMRES", "NONE", {"R": 30}),
+    ("convdiff3d", "GCR", "NONE", {"R": 10}),
+    ("poisson3d", "KSKIPCG", "NONE", {"K": 2}),
+    ("convdiff3d", "KSKIPBICG", "NONE", {"K": 2}),
+    ("varcoef3d", "VPCG", "CG", {"l": 20, "e": 1e-30, "inner_precision": "fp32"}),
+    ("varcoef3d", "VPGMRES", "CG", {"R": 30, "l": 10, "e": 1e-30, "inner_precision": "fp32"}),
+]
+
+
+@pytest.mark.parametrize("prob,outer,inner,kw", CASES)
+def test_split_solve_matches_one_gpu(ks, ctx, split3, prob, outer, inner, kw):
+    ctxs, comms = split3
+    A, b, _ = config_problem(prob, 20)
+    tr = outer in ("BICG", "KSKIPBICG")
+    lowp = "inner_precision" in kw
+    ref = ks.solve(ctx, ctx.matrix(A, transpose=tr, fp32=lowp), outer, b, inner=inner, E=1e-10, **kw)
+    rs = ks.partition_rows(A.n, 3, 400)
+    AT = transpose(A) if tr else None
+
+    def rank(q):
+        c = ctxs[q]
+        M = ks.SplitMatrix(c, comms[q], A, rs[q], rs[q + 1], transpose=tr, fp32=lowp, AT=AT)
+        return ks.solve(c, M, outer, b[rs[q]:rs[q + 1]], inner=inner, E=1e-10, **kw)
+
+    res = _ranks(3, rank)
+    for r in res[1:]:  # every rank took the same decisions
+        assert r.status == res[0].status and r.loop == res[0].loop
+        assert np.array_equal(r.hist_err, res[0].hist_err)
+        assert r.true_rel_res == res[0].true_rel_res
+    r0 = res[0]
+    assert r0.status == ref.status == 0, (r0.status, ref.status)
+    assert abs(r0.loop - ref.loop) <= max(2, 0.02 * ref.loop), (r0.loop, ref.loop)
+    x = np.concatenate([r.x for r in res])
+    assert np.linalg.norm(x - ref.x) <= 1e-8 * np.linalg.norm(ref.x)
+    true = np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)
+    assert r0.true_rel_res == pytest.approx(true, rel=1e-6)
+    assert true < 2e-10
+
+
+def test_split_two_ranks_at_half(ks, oracle):
+    """Two ranks split at ceil(n/2), the reference's two-GPU split, on an odd n."""
+    A, b, _ = config_problem("poisson2d", 45)  # n = 2025
+    rs = ks.partition_rows(A.n, 2)
+    assert rs[1] == (A.n + 1) // 2
+    ctxs = [ks.Context(0) for _ in range(2)]
+    comms = ks.Comm.local(ctxs)
+    try:
+        res = _ranks(2, lambda q: ks.solve(ctxs[q], ks.SplitMatrix(ctxs[q], comms[q], A, rs[q], rs[q + 1]), "CG",
+                                           b[rs[q]:rs[q + 1]], E=1e-12))
+        o = oracle.solve(A, b, "CG", E=1e-12)
+        assert res[0].status == 0 and abs(res[0].loop - o["loop"]) <= 2
+        x = np.concatenate([r.x for r in res])
+        assert np.linalg.norm(x - o["x"]) <= 1e-9 * np.linalg.norm(o["x"])
+    finally:
+        for c in comms:
+            c.close()
+        for c in ctxs:
+            c.close()
