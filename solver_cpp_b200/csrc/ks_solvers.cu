@@ -601,6 +601,85 @@ ks_status init_state(const Env<VT> &E, const VT *b) {
   return KS_OK;
 }
 
+// ------------------------------------------------------------------ iteration issue
+// Systems small enough that an iteration's kernels take a few microseconds
+// are bound by launching: the host spends about as long on the three to five
+// launches of an iteration as the GPU spends running them. When every
+// iteration issues the same kernels with the same arguments (all device
+// state lives in KState), the iterations after the first chunk are replayed
+// from a CUDA graph holding kGraphChunk iterations, one host launch per chunk.
+// Kernels past the method's stop return at once, as they do without graphs.
+constexpr int kGraphChunk = 16;
+constexpr long long kGraphMaxN = 1 << 20;  // rows; larger systems are HBM-bound
+
+struct ChunkGraph {
+  ks_ctx *ctx;
+  cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;  // kernels per replay, for the launch count
+  ~ChunkGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  template <class F>
+  bool capture(F &&issue) {
+    const long long l0 = ctx->launches;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return false;
+    }
+    issue();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    kernels = ctx->launches - l0;
+    ctx->launches = l0;  // counted again at every replay
+    if (e != cudaSuccess || !g) {
+      (void)cudaGetLastError();
+      return false;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      exec = nullptr;
+      (void)cudaGetLastError();
+      return false;
+    }
+    return true;
+  }
+  void launch() {
+    cudaGraphLaunch(exec, ctx->stream);
+    ctx->launches += kernels;
+  }
+};
+
+// Issues iterations 1..maxloop: body(L) queues iteration L. `fixed`: every
+// iteration queues the same kernels with the same arguments.
+template <class VT, class F>
+inline void run_iterations(const Env<VT> &E, bool fixed, F &&body) {
+  Poller P{E.ctx, E.hflag, E.lookahead};
+  long long L = 1;
+  if (fixed && E.outer && !E.comm && E.n <= kGraphMaxN && E.sp.maxloop > 2 * kGraphChunk) {
+    // the first chunk is launched directly (it also sets up every kernel)
+    for (; L <= kGraphChunk; L++) {
+      body(L);
+      if (P.step()) return;
+    }
+    ChunkGraph G{E.ctx};
+    if (G.capture([&] {
+          for (int j = 0; j < kGraphChunk; j++) body(L);
+        })) {
+      Poller PC{E.ctx, E.hflag, 2};  // lookahead in chunks
+      for (; L <= E.sp.maxloop; L += kGraphChunk) {
+        G.launch();
+        if (PC.step()) return;
+      }
+      return;
+    }
+  }
+  for (; L <= E.sp.maxloop; L++) {
+    body(L);
+    if (E.outer && P.step()) return;
+  }
+}
+
 // cg::solve, three kernels per iteration with the x update deferred to the
 // direction ring. (Forming the next direction inside the SpMV's gather
 // instead of the separate update was measured slower on B200: gathering two
@@ -616,8 +695,7 @@ ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CG});
-  Poller P{E.ctx, E.hflag, E.lookahead};
-  for (long long L = 1; L <= E.sp.maxloop; L++) {
+  run_iterations(E, !defer, [&](long long L) {
     VT *p = R.slot(L);
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
     if (defer) {
@@ -627,8 +705,7 @@ ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
       vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 0});
     }
     vec(E, XpbyToOp<VT>{p, r, R.slot(L + 1), &E.st->k.s[S_BETA]});
-    if (E.outer && P.step()) break;
-  }
+  });
   if (defer) ring_final(E, R, x);
   return KS_OK;
 }
@@ -709,8 +786,7 @@ ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   if (!defer) vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CHECK});
   mv(E, *E.A, (const VT *)R.slot(1), CrStartMvEpi<VT>{r, q, s, E.st});
-  Poller P{E.ctx, E.hflag, E.lookahead};
-  for (long long L = 1; L <= E.sp.maxloop; L++) {
+  run_iterations(E, !defer, [&](long long L) {
     if (defer) {
       vec(E, RUpdOp<VT>{r, q, E.st, 1, R.aslot(L)});
       ring_step(E, R, x, L);
@@ -719,8 +795,7 @@ ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
     }
     mv(E, *E.A, (const VT *)r, CrMvEpi<VT>{r, s, E.st});
     vec(E, Xpby2ToOp<VT>{R.slot(L), r, R.slot(L + 1), q, s, E.st});
-    if (E.outer && P.step()) break;
-  }
+  });
   if (defer) ring_final(E, R, x);
   return KS_OK;
 }
@@ -779,8 +854,7 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   if (!defer) vec(E, ZeroOp<VT>{x});
   // (r*, r) = (r, r) at the start
   start_from_zero(E, StartEpi<VT>{b, r, rs, R.slot(1), ps, E.st, START_CG});
-  Poller P{E.ctx, E.hflag, E.lookahead};
-  for (long long L = 1; L <= E.sp.maxloop; L++) {
+  run_iterations(E, !defer, [&](long long L) {
     VT *p = R.slot(L);
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
     if (defer) {
@@ -791,8 +865,7 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
     }
     mv(E, *E.AT, (const VT *)ps, BicgMvTEpi<VT>{rs, r, E.st});
     vec(E, Xpby2PlainOp<VT>{p, r, R.slot(L + 1), ps, rs, &E.st->k.s[S_BETA]});
-    if (E.outer && P.step()) break;
-  }
+  });
   if (defer) ring_final(E, R, x);
   return KS_OK;
 }

@@ -7,7 +7,8 @@ must equal the whole-matrix SpMV bit for bit (rows are complete on their
 rank), every rank must take the same decisions (identical histories and
 iteration counts), and the assembled solution must agree with the one-GPU
 solve: the dots are summed in another order, so to 1e-8 relative, with
-iteration counts within 2 %.
+iteration counts within 2 % (10 % and 1e-6 for VPGMRES with an FP32 inner
+solve, whose outer iteration count moves with FP32-sized changes).
 """
 import threading
 
@@ -107,9 +108,14 @@ def test_split_solve_matches_one_gpu(ks, ctx, split3, prob, outer, inner, kw):
         assert r.true_rel_res == res[0].true_rel_res
     r0 = res[0]
     assert r0.status == ref.status == 0, (r0.status, ref.status)
-    assert abs(r0.loop - ref.loop) <= max(2, 0.02 * ref.loop), (r0.loop, ref.loop)
+    # An FP32 inner solve turns the reordered sums into FP32-sized changes of
+    # each preconditioned direction; flexible GMRES then needs a few more or
+    # fewer outer iterations (here 63 on one GPU, 67 split), so those cases
+    # get 10 % and 1e-6; the FP64 methods 2 % and 1e-8.
+    loose = lowp and outer == "VPGMRES"
+    assert abs(r0.loop - ref.loop) <= max(2, (0.10 if loose else 0.02) * ref.loop), (r0.loop, ref.loop)
     x = np.concatenate([r.x for r in res])
-    assert np.linalg.norm(x - ref.x) <= 1e-8 * np.linalg.norm(ref.x)
+    assert np.linalg.norm(x - ref.x) <= (1e-6 if loose else 1e-8) * np.linalg.norm(ref.x)
     true = np.linalg.norm(b - A.to_scipy() @ x) / np.linalg.norm(b)
     assert r0.true_rel_res == pytest.approx(true, rel=1e-6)
     assert true < 2e-10
