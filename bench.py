@@ -62,6 +62,8 @@ WORKLOADS = {
     # against plain FP64 GMRES with the same restart
     "c4_vpgmres": _w("varcoef3d", 160, "VPGMRES", dict(_VP20, inner_precision="fp32"), inner="CG",
                      plain=dict(outer="GMRES", params=dict(E=1e-10, L=20000)), spmv_values="fp32"),
+    # the reference's own CPU-runnable case: 2D Poisson 64^2, b = A*1 + noise
+    "c1_cg": _w("poisson2d", 64, "CG", dict(E=1e-10, L=10000), ref_args=["-S", "cg", "-E", "1e-10"]),
     "c2_cg": _w("poisson3d", 128, "CG", dict(E=1e-10, L=10000), ref_args=["-S", "cg", "-E", "1e-10"]),
     "c2_cr": _w("poisson3d", 128, "CR", dict(E=1e-10, L=10000), ref_args=["-S", "cr", "-E", "1e-10"]),
     "c2_kskipcg2": _w("poisson3d", 128, "KSKIPCG", dict(E=1e-10, L=10000, K=2)),
@@ -423,8 +425,8 @@ def cpu_baseline_port(A, b, W, res):
 #: iterations for VPCG), measured once by running oracle/_ref/Solver to
 #: convergence with 8 OpenMP threads: c4_mixed `-S vpcg -s cg -l 20 -e 1e-30
 #: -E 1e-10` 593 outer iterations (285.8 s); plain CG on the same system 5157
-#: (144.8 s); c2_cg `-S cg -E 1e-10` 530.
-REF_FULL_ITERATIONS = {"c4_mixed": 593, "c2_cg": 530}
+#: (144.8 s); c2_cg `-S cg -E 1e-10` 530; c1_cg 202 (the 64^2 golden run).
+REF_FULL_ITERATIONS = {"c4_mixed": 593, "c2_cg": 530, "c1_cg": 202}
 
 
 def run_reference(args, world, rank):
