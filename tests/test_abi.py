@@ -93,3 +93,26 @@ def test_ctx_without_device_reports_no_device(ks):
     assert lib.ks_ctx_create(0, C.byref(h)) == 9  # KS_NO_DEVICE
     with pytest.raises(ks.KrylovError):
         ks.Context(0)
+
+
+def test_bench_reference_arm_json(ks, tmp_path):
+    """bench.py --impl reference on the 64^2 CG case: the reference's own CPU
+    binary (built from its sources when the package was built) runs a bounded
+    sample and the line carries the contract's keys."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--workload", "c1_cg",
+                        "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["impl"] == "reference"
+    if "unavailable" in d:
+        pytest.skip(d["unavailable"])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "cpu_baseline", "e2e",
+              "config"):
+        assert k in d, k
+    assert d["value"] > 0 and d["cpu_baseline"]["kind"] == "reference" and d["config"]["workload"] == "c1_cg"
