@@ -321,15 +321,17 @@ inline void launch_vec(ks_ctx *ctx, long long n, const Op &op_in, Stop stop, int
 }
 
 // k_hint: the number of basis vectors, or a bound when the kernel reads it
-// from the device. Short chains run one full-occupancy wave of CTAs that
-// stride over the elements, which keeps the final reduction short; long
-// chains (measured: from 64 vectors) stream faster with one thread per
-// element, the reduction's cost then being small beside the pass.
+// from the device. Short chains run at least one full-occupancy wave of CTAs
+// and at most two elements per thread: fewer CTAs keep the final reduction
+// short, but an element's loads are one round trip that the next element
+// waits behind. Long chains (measured: from 64 vectors) stream fastest with
+// one thread per element, the reduction's cost then being small beside the
+// pass.
 template <class Op>
 inline void launch_basis(ks_ctx *ctx, long long n, int k_hint, const Op &op, Stop stop, int slot = 0) {
   long long grid = (n + kThreads - 1) / kThreads;
   const long long cap = k_hint >= 64 ? (long long)(ctx->partials_len / (Op::ND > 0 ? Op::ND : 1))
-                                     : (long long)ctx->num_sms * 8;
+                                     : std::max((long long)ctx->num_sms * 8, (grid + 1) / 2);
   grid = std::max(1LL, std::min(grid, cap));
   with_rank_sums(ctx, op, stop, [&](const auto &o) {
     using O = std::decay_t<decltype(o)>;
