@@ -137,6 +137,9 @@ __device__ __forceinline__ float mval<float, __nv_bfloat16>(__nv_bfloat16 v) {
   return __bfloat162float(v);
 }
 
+// Hint: bring the line holding p into L2 (no register, no fault on use).
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ---------------------------------------------------------------- PDL
 // Programmatic dependent launch: every kernel lets the next one in the stream
 // be scheduled at once (trigger) and waits for the previous one's results
@@ -197,22 +200,32 @@ __device__ __forceinline__ bool grid_sum_n(double (&v)[ND], double *partials,
   __syncthreads();
   if (!is_last) return false;
   __threadfence();
-  // Four independent running sums per thread keep four partial loads in
-  // flight; the order is still fixed.
+  // Several loads in flight per thread; the order is still fixed. Few
+  // values: four running sums per value. Many values (block dots): one
+  // running sum per value, all values' loads of one round issued together.
+  const unsigned B = blockDim.x;
+  if constexpr (ND >= 4) {
 #pragma unroll
-  for (int d = 0; d < ND; d++) {
-    const double *p = partials + (size_t)d * G;
-    const unsigned B = blockDim.x;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    unsigned i = threadIdx.x;
-    for (; i + 3 * B < G; i += 4 * B) {
-      s0 += __ldcg(p + i);
-      s1 += __ldcg(p + i + B);
-      s2 += __ldcg(p + i + 2 * B);
-      s3 += __ldcg(p + i + 3 * B);
+    for (int d = 0; d < ND; d++) v[d] = 0.0;
+    for (unsigned i = threadIdx.x; i < G; i += B) {
+#pragma unroll
+      for (int d = 0; d < ND; d++) v[d] += __ldcg(partials + (size_t)d * G + i);
     }
-    for (; i < G; i += B) s0 += __ldcg(p + i);
-    v[d] = (s0 + s1) + (s2 + s3);
+  } else {
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      const double *p = partials + (size_t)d * G;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      unsigned i = threadIdx.x;
+      for (; i + 3 * B < G; i += 4 * B) {
+        s0 += __ldcg(p + i);
+        s1 += __ldcg(p + i + B);
+        s2 += __ldcg(p + i + 2 * B);
+        s3 += __ldcg(p + i + 3 * B);
+      }
+      for (; i < G; i += B) s0 += __ldcg(p + i);
+      v[d] = (s0 + s1) + (s2 + s3);
+    }
   }
   block_sum<ND>(v);
   if (threadIdx.x == 0) *counter = 0u;

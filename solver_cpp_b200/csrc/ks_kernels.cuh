@@ -111,7 +111,16 @@ __global__ void __launch_bounds__(kThreads) basis_kernel(Op op, long long n, Sto
 #pragma unroll
   for (int b = 0; b < NB; b++) B[b] = op.base(b);
   const long long ld = op.ld;
-  for (long long j = (long long)blockIdx.x * kThreads + threadIdx.x; j < n; j += (long long)gridDim.x * kThreads) {
+  const long long estride = (long long)gridDim.x * kThreads;
+  for (long long j = (long long)blockIdx.x * kThreads + threadIdx.x; j < n; j += estride) {
+    // the next element's first chunk heads for L2 while this one runs
+    if (j + estride < n) {
+#pragma unroll
+      for (int u = 0; u < C; u++)
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+          if (u < k) prefetch_l2(B[b] + (long long)u * ld + j + estride);
+    }
     typename Op::St s = op.init(j);
     VT cur[C][NB], nxt[C][NB];
 #pragma unroll
@@ -322,11 +331,11 @@ inline void launch_vec(ks_ctx *ctx, long long n, const Op &op_in, Stop stop, int
 
 // k_hint: the number of basis vectors, or a bound when the kernel reads it
 // from the device. Short chains run at least one full-occupancy wave of CTAs
-// and at most two elements per thread: fewer CTAs keep the final reduction
-// short, but an element's loads are one round trip that the next element
-// waits behind. Long chains (measured: from 64 vectors) stream fastest with
-// one thread per element, the reduction's cost then being small beside the
-// pass.
+// and at most two elements per thread (measured best at 128^3: fewer CTAs
+// keep the final reduction short, but each element's loads are a round trip
+// the next element waits behind, even with its basis prefetched into L2).
+// Long chains (measured: from 64 vectors) stream fastest with one thread per
+// element, the reduction's cost then being small beside the pass.
 template <class Op>
 inline void launch_basis(ks_ctx *ctx, long long n, int k_hint, const Op &op, Stop stop, int slot = 0) {
   long long grid = (n + kThreads - 1) / kThreads;

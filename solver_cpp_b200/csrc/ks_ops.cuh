@@ -123,7 +123,7 @@ __global__ void pattern_grad_kernel(CsrK<double> A, const double *__restrict__ l
 // Each group is reduced deterministically with its own counter;
 // Epi::put(w, i, value) receives every result (thread 0 of the group's last CTA).
 template <int NW, class VT, class Epi>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, NW == 1 ? 4 : 2)
     block_dot_kernel(const VT *__restrict__ V, long long ld, int k,
                      const VT *__restrict__ W0, const VT *__restrict__ W1, long long n,
                      Epi epi, Stop stop, double *partials, unsigned *counters) {

@@ -207,8 +207,12 @@ struct NormBOp {  // s[BNORM] = |b|
   const VT *b;
   DevState *st;
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
-    const double v = widen(b[i]);
+  struct Regs {
+    VT b;
+  };
+  __device__ Regs load(long long i) const { return {b[i]}; }
+  __device__ void store(long long, const Regs &g, double (&acc)[1]) const {
+    const double v = widen(g.b);
     acc[0] = add_rn(acc[0], mul_rn(v, v));
   }
   __device__ void finish(const double (&s)[1]) const { st->k.s[S_BNORM] = sqrt(s[0]); }
@@ -227,7 +231,11 @@ struct CopyOp {
   const VT *a;
   VT *b;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const { b[i] = a[i]; }
+  struct Regs {
+    VT a;
+  };
+  __device__ Regs load(long long i) const { return {a[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const { b[i] = g.a; }
   __device__ void finish(const double (&)[1]) const {}
 };
 
@@ -901,11 +909,18 @@ struct GcrXrOp {
   DevState *st;
   int last;
   static constexpr int ND = 1;
-  __device__ void elem(long long i, double (&acc)[1]) const {
+  struct Regs {
+    VT x, p, q, r;
+  };
+  __device__ Regs load(long long i) const {
+    if (last) return {x[i], pk[i], (VT)0, (VT)0};
+    return {x[i], pk[i], qk[i], r[i]};
+  }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
     const VT a = (VT)rd(&st->k.s[S_ALPHA]);
-    x[i] = add_rn(mul_rn(a, pk[i]), x[i]);
+    x[i] = add_rn(mul_rn(a, g.p), g.x);
     if (!last) {
-      const VT ri = add_rn(mul_rn((VT)(-a), qk[i]), r[i]);
+      const VT ri = add_rn(mul_rn((VT)(-a), g.q), g.r);
       r[i] = ri;
       acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
     }
@@ -1047,9 +1062,11 @@ struct ScaleOp {  // out = a / t, t from slot (Scalar_x_div_a)
   VT *out;
   const double *t;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const {
-    out[i] = div_rn(a[i], (VT)rd(t));
-  }
+  struct Regs {
+    VT a;
+  };
+  __device__ Regs load(long long i) const { return {a[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const { out[i] = div_rn(g.a, (VT)rd(t)); }
   __device__ void finish(const double (&)[1]) const {}
 };
 
@@ -1455,10 +1472,14 @@ struct KsXrOp {  // x += a p; r -= a Av
   const VT *Av;
   const double *a;
   static constexpr int ND = 0;
-  __device__ void elem(long long i, double (&)[1]) const {
+  struct Regs {
+    VT x, p, r, av;
+  };
+  __device__ Regs load(long long i) const { return {x[i], p[i], r[i], Av[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const {
     const VT al = (VT)rd(a);
-    x[i] = add_rn(mul_rn(al, p[i]), x[i]);
-    r[i] = add_rn(mul_rn((VT)(-al), Av[i]), r[i]);
+    x[i] = add_rn(mul_rn(al, g.p), g.x);
+    r[i] = add_rn(mul_rn((VT)(-al), g.av), g.r);
   }
   __device__ void finish(const double (&)[1]) const {}
 };
