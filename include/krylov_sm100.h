@@ -329,8 +329,9 @@ ks_status ks_comm_info(const ks_comm *comm, int *nranks, int *rank);
  * indices; ptr holds r1 - r0 + 1 offsets of any base) and, with
  * KS_MAT_TRANSPOSE, the same rows of A^T (tptr/tcol/tval). Every rank calls
  * it with its own block, blocks contiguous in rank order (ks_partition_rows
- * gives one). ks_solve / ks_solve_host / ks_spmv on the result take vectors
- * of the local length r1 - r0 and run the split method: before each SpMV the
+ * gives one). ks_solve / ks_solve_host / ks_spmv / ks_adjoint_grad /
+ * ks_pattern_grad on the result take vectors of the local length r1 - r0
+ * (grad_val: the local nonzeros) and run the split method: before each SpMV the
  * halo of the input vector comes from the peers (ks_halo_plan), and every
  * reduction is summed over the ranks before its scalar step, so every rank
  * takes the same decisions. Replaces the reference's two-GPU split

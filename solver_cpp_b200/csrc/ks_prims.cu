@@ -285,14 +285,31 @@ ks_status ks_gram_bicg(const ks_vec *Ar, const ks_vec *Ap, const ks_vec *rs, con
 
 ks_status ks_pattern_grad(const ks_mat *mat, const ks_vec *lambda, const ks_vec *x, ks_vec *grad_val) {
   if (!mat || !lambda || !x || !grad_val) return KS_BAD_INPUT;
-  if (mat->dist) return set_error(mat->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");
   ks_ctx *ctx = mat->ctx;
   if (lambda->type != KS_FP64 || x->type != KS_FP64 || grad_val->type != KS_FP64 ||
       lambda->n != mat->A.n || x->n != mat->A.n || grad_val->n < mat->A.nnz)
     return set_error(ctx, KS_BAD_INPUT, "pattern_grad: FP64 vectors of n, n, nnz required");
-  pattern_grad_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(
-      view<double>(mat->A), (const double *)lambda->d, (const double *)x->d, (double *)grad_val->d);
-  KS_CUDA(ctx, cudaGetLastError());
+  const double *xs = (const double *)x->d;
+  void *buf = nullptr;
+  if (mat->dist) {  // split rows: the columns reach into the halo, so x goes into a window first
+    const DistInfo &d = *mat->dist;
+    KS_TRY(pool_get(ctx, sizeof(double) * (size_t)d.ld() + 64, &buf));
+    double *xl = (double *)buf + d.off();
+    const cudaError_t e =
+        cudaMemcpyAsync(xl, x->d, sizeof(double) * (size_t)mat->A.n, cudaMemcpyDeviceToDevice, ctx->stream);
+    ks_status s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "pattern_grad copy");
+    if (s == KS_OK) s = d.comm->exchange(d.planA, xl, sizeof(double));
+    if (s != KS_OK) {
+      pool_release(ctx, buf);
+      return s;
+    }
+    xs = xl;
+  }
+  pattern_grad_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(view<double>(mat->A), (const double *)lambda->d,
+                                                                  xs, (double *)grad_val->d);
+  const cudaError_t e = cudaGetLastError();
+  if (buf) pool_release(ctx, buf);  // later users of the pool are queued behind the gather
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pattern_grad");
   return KS_OK;
 }
 

@@ -1106,32 +1106,55 @@ struct GmPutH {  // H[i][k] = (w, V_i)
 // H[k+1][k] = |w| arrives in s[T] from the block AXPY; then the Givens
 // rotations of column k (gmres.cpp:384-399), count++ and, unless step k ends
 // the cycle, the stopping test at the top of step k+1.
-struct GmGivensOp {
+struct GmGivensOp {  // arguments of gm_givens_kernel
   GmArrays g;
   DevState *st;
   int k;
   int check_next;
-  __device__ void run() const {
-    const int m = g.m;
-    double *H = g.H;
-    H[(long long)(k + 1) * m + k] = st->k.s[S_T];
-    for (int i = 0; i <= k - 1; i++) {
-      const double t1 = H[(long long)i * m + k], t2 = H[(long long)(i + 1) * m + k];
-      H[(long long)i * m + k] = g.cs[i] * t1 - g.sn[i] * t2;
-      H[(long long)(i + 1) * m + k] = g.sn[i] * t1 + g.cs[i] * t2;
-    }
-    const double hkk = H[(long long)k * m + k], hk1 = H[(long long)(k + 1) * m + k];
-    const double a = sqrt(hkk * hkk + hk1 * hk1);
-    g.cs[k] = hkk / a;
-    g.sn[k] = -hk1 / a;
-    g.e[k + 1] = g.sn[k] * g.e[k];
-    g.e[k] = g.cs[k] * g.e[k];
-    H[(long long)k * m + k] = g.cs[k] * H[(long long)k * m + k] - g.sn[k] * H[(long long)(k + 1) * m + k];
-    H[(long long)(k + 1) * m + k] = 0.0;
-    st->k.loop += 1;
-    if (check_next) gm_check(g, st, k + 1);
-  }
 };
+
+// The Givens step of column k (gmres.cpp:384-399): H[k+1][k] = |w|, the k
+// earlier rotations applied in order, the new rotation, e updated, count++
+// and, unless step k ends the cycle, the stopping test of step k+1. The
+// column and the rotations are staged in shared memory by the whole CTA, so
+// the chain of k dependent rotations reads shared memory, not global memory.
+__global__ void __launch_bounds__(kThreads) gm_givens_kernel(GmGivensOp op, Stop stop) {
+  extern __shared__ double gsm[];  // column k (k + 2), cs (k), sn (k)
+  pdl_wait();
+  if (stop()) return;
+  const int k = op.k, m = op.g.m;
+  double *H = op.g.H;
+  double *col = gsm, *cs = gsm + (k + 2), *sn = cs + k;
+  for (int i = threadIdx.x; i <= k + 1; i += blockDim.x) col[i] = H[(long long)i * m + k];
+  for (int i = threadIdx.x; i < k; i += blockDim.x) {
+    cs[i] = op.g.cs[i];
+    sn[i] = op.g.sn[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    DevState *st = op.st;
+    col[k + 1] = st->k.s[S_T];
+    for (int i = 0; i <= k - 1; i++) {
+      const double t1 = col[i], t2 = col[i + 1];
+      col[i] = cs[i] * t1 - sn[i] * t2;
+      col[i + 1] = sn[i] * t1 + cs[i] * t2;
+    }
+    const double hkk = col[k], hk1 = col[k + 1];
+    const double a = sqrt(hkk * hkk + hk1 * hk1);
+    const double ck = hkk / a, sk = -hk1 / a;
+    op.g.cs[k] = ck;
+    op.g.sn[k] = sk;
+    op.g.e[k + 1] = sk * op.g.e[k];
+    op.g.e[k] = ck * op.g.e[k];
+    col[k] = ck * col[k] - sk * col[k + 1];
+    col[k + 1] = 0.0;
+    st->k.loop += 1;
+    if (op.check_next) gm_check(op.g, st, k + 1);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i <= k + 1; i += blockDim.x) H[(long long)i * m + k] = col[i];
+  pdl_trigger();
+}
 
 // Back substitution y = H^{-1} e on the leading size x size block
 // (blas::Hye, blas.cpp:303-314). size < 0: take size from the stop step.
@@ -1242,7 +1265,8 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
       launch_basis(E.ctx, n, k + 1, BlockAxpyOp<VT>{V, ld, k + 1, g.H + k, m, w, &E.st->k.s[S_T], 1},
                    E.stop());  // s[T] = |w|
       vec(E, ScaleOp<VT>{w, V + (long long)(k + 1) * ld, &E.st->k.s[S_T]});
-      launch_scalar(E.ctx, GmGivensOp{g, E.st, k, k + 1 < m - 1 ? 1 : 0}, E.stop());
+      launch_k(E.ctx, gm_givens_kernel, dim3(1), dim3(kThreads), sizeof(double) * (size_t)(3 * k + 2),
+               GmGivensOp{g, E.st, k, k + 1 < m - 1 ? 1 : 0}, E.stop());
       issued++;
       if (E.outer && P.step()) {
         stop_host = true;
@@ -2075,7 +2099,6 @@ ks_status ks_adjoint_grad(ks_ctx *ctx, const ks_mat *mat, ks_solver solver, ks_s
                           const ks_params *params, const ks_vec *x, const ks_vec *g, ks_vec *grad_b,
                           ks_vec *grad_val, ks_report *report) {
   if (!ctx || !mat || !x || !g || x->type != KS_FP64 || g->type != KS_FP64) return KS_BAD_INPUT;
-  if (mat->dist) return set_error(mat->ctx, KS_UNIMPLEMENTED, "not available for split-row matrices");
   ks_params p;
   if (params) p = *params;
   else ks_params_default(&p);

@@ -140,3 +140,38 @@ def test_split_two_ranks_at_half(ks, oracle):
             c.close()
         for c in ctxs:
             c.close()
+
+
+@pytest.mark.parametrize("prob,solver", [("varcoef2d", "CG"), ("convdiff2d", "BICG")])
+def test_split_adjoint_gradient(ks, ctx, split3, prob, solver):
+    """Adjoint gradients on split rows (the transposed solve and the pattern
+    gather, whose columns reach into the halo) against the one-GPU ones."""
+    ctxs, comms = split3
+    A, b, _ = config_problem(prob, 48)
+    xstar = np.random.default_rng(6).standard_normal(A.n)
+    kw = dict(E=1e-12, L=20000)
+    M = ctx.matrix(A, transpose=True)
+    fw = ks.solve(ctx, M, solver, b, **kw)
+    X, G = ctx.vector(fw.x), ctx.vector(fw.x - xstar)
+    GB, GV = ctx.vector(n=A.n), ctx.vector(n=A.nnz)
+    assert ks.adjoint_grad(ctx, M, solver, X, G, GB, GV, **kw)[0] == 0
+    gb_ref, gv_ref = GB.numpy(), GV.numpy()
+    rs = ks.partition_rows(A.n, 3, 48)
+    AT = transpose(A)
+
+    def rank(q):
+        c = ctxs[q]
+        r0, r1 = rs[q], rs[q + 1]
+        Ms = ks.SplitMatrix(c, comms[q], A, r0, r1, transpose=True, AT=AT)
+        x = ks.solve(c, Ms, solver, b[r0:r1], **kw).x
+        Xl, Gl = c.vector(x), c.vector(x - xstar[r0:r1])
+        GBl, GVl = c.vector(n=Ms.n), c.vector(n=max(Ms.nnz, 1))
+        st, _ = ks.adjoint_grad(c, Ms, solver, Xl, Gl, GBl, GVl, **kw)
+        return st, GBl.numpy(), GVl.numpy()[:Ms.nnz]
+
+    res = _ranks(3, rank)
+    assert all(r[0] == 0 for r in res)
+    gb = np.concatenate([r[1] for r in res])
+    gv = np.concatenate([r[2] for r in res])
+    assert np.linalg.norm(gb - gb_ref) <= 1e-8 * np.linalg.norm(gb_ref)
+    assert np.linalg.norm(gv - gv_ref) <= 1e-8 * np.linalg.norm(gv_ref)
