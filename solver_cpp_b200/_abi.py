@@ -43,7 +43,7 @@ MAT_BF16 = 4
 MAT_INDEX32 = 8
 
 
-ABI_VERSION = 2  # KS_ABI_VERSION of the header these structures mirror
+ABI_VERSION = 3  # KS_ABI_VERSION of the header these structures mirror
 
 
 class Params(C.Structure):
@@ -54,6 +54,7 @@ class Params(C.Structure):
         ("inner_kskip", C.c_int32), ("inner_fix", C.c_int32),
         ("inner_precision", C.c_int32), ("reference_defects", C.c_int32),
         ("transpose", C.c_int32), ("poll_interval", C.c_int32), ("x_update", C.c_int32),
+        ("cluster_solve", C.c_int32),
     ]
 
 

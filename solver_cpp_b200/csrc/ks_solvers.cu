@@ -15,6 +15,8 @@
 #include <cstring>
 
 #include "ks_ops.cuh"
+#include "ks_state.cuh"
+#include "ks_resident.cuh"
 
 namespace ks {
 
@@ -23,65 +25,6 @@ ks_status spmv_any(ks_ctx *ctx, const CsrDev &A, ks_precision vals, ks_precision
 ks_status matpow(ks_ctx *ctx, const CsrDev &A, const double *r, const double *p, int k, double *Ar,
                  double *Ap, Stop stop);
 
-// ------------------------------------------------------------------ state
-enum Slot : int {
-  S_BNORM = 0,
-  S_EPS = 1,
-  S_RR = 2,     // (r,r) / (r*,r) / (r,z) / (r,s) / zaz: the carried product
-  S_ALPHA = 3,
-  S_BETA = 4,
-  S_T = 5,      // GMRES: current norm
-  S_GAMMA = 6,  // k-skip
-};
-enum Aux : int { A_MAXLOOP = 0, A_RECORD = 1, A_SPMV = 2, A_CONVK = 3, A_FINAL = 4, A_KIDX = 5, A_PENDING = 6, A_XZERO = 7 };
-
-struct DevState {  // KState plus the host-mapped mirror of `done`
-  KState k;
-  int *host_done;
-};
-
-__device__ __forceinline__ void set_done(DevState *st, int code) {
-  st->k.done = code;
-  if (st->host_done) *(volatile int *)st->host_done = code;
-}
-
-__device__ __forceinline__ void record(DevState *st, long long label, double err) {
-  if (!st->k.aux[A_RECORD]) return;
-  const long long h = st->k.hlen++;
-  if (h < st->k.hcap) {
-    st->k.hist_err[h] = err;
-    st->k.hist_it[h] = label;
-  }
-}
-
-// Stopping test at the top of iteration L of the CG-type loops
-// (cg.cpp:184-198): loop ends after maxloop iterations, records, compares.
-__device__ __forceinline__ void check_top(DevState *st, long long L, double err) {
-  st->k.loop = L;
-  if (L > st->k.aux[A_MAXLOOP]) {
-    set_done(st, kMaxLoop);
-    return;
-  }
-  record(st, L, err);
-  if (err <= st->k.s[S_EPS])
-    set_done(st, kConverged);
-  else if (err != err)
-    set_done(st, kNaN);
-}
-
-// a / b of a recurrence; a zero or non-finite result stops the method.
-__device__ __forceinline__ double rdiv(DevState *st, double a, double b) {
-  if (b == 0.0) {
-    set_done(st, kBreakdown);
-    return 0.0;
-  }
-  const double q = div_rn(a, b);
-  if (!isfinite(q)) set_done(st, kNaN);
-  return q;
-}
-
-__device__ __forceinline__ double rd(const double *p) { return __ldg(p); }
-
 // ------------------------------------------------------------------ env
 struct Params {
   long long maxloop;
@@ -89,7 +32,8 @@ struct Params {
   long long restart;
   int kskip;
   int fix;
-  int x_update = 0;  // ks_params.x_update
+  int x_update = 0;       // ks_params.x_update
+  int cluster_solve = 0;  // ks_params.cluster_solve
 };
 
 template <class VT>
@@ -693,8 +637,35 @@ inline void run_iterations(const Env<VT> &E, bool fixed, F &&body) {
 // instead of the separate update was measured slower on B200: gathering two
 // vectors per nonzero cost 15 us per SpMV at 128^3, the update kernel it
 // removes 8 us.)
+// Small systems (up to kResMaxRows rows, one GPU, FP64; ks_params.cluster_solve
+// 0): the whole solve as one launch of one thread-block cluster
+// (ks_resident.cuh). Returns false,
+// having launched nothing, when the system does not qualify or no cluster of
+// the needed shape fits on the device.
+inline bool run_cg_resident(const Env<double> &E, const double *b, double *x, ks_status *s) {
+  if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A->val) return false;
+  const ResShape sh = resident_shape(E.n);
+  if (!sh.C) return false;
+  const CsrDev &A = *E.A;
+  const ResCgArgs a{A.ptr, A.col, A.col16, A.val, b, x, E.st, (int)E.n, sh.shift};
+  bool fits = false;
+  if (res_cg(sh, A.col16 != nullptr, E.ctx->stream, a, true, &fits) != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  E.ctx->launches++;
+  const cudaError_t e = res_cg(sh, A.col16 != nullptr, E.ctx->stream, a, false, nullptr);
+  *s = e == cudaSuccess ? KS_OK : cuda_fail(E.ctx, e, "cluster-resident CG launch");
+  return true;
+}
+
 template <class VT>
 ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
+  if constexpr (std::is_same<VT, double>::value) {
+    ks_status s = KS_OK;
+    if (run_cg_resident(E, b, x, &s)) return s;
+  }
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take();
   const bool defer = defer_x(E, KS_CG);
@@ -1798,10 +1769,12 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     return set_error(ctx, KS_BAD_INPUT, "low-precision inner BiCG needs the transpose's value copy");
 
   Params outer_sp{prm->outer_maxloop, prm->outer_eps, prm->outer_restart, prm->outer_kskip, prm->outer_fix,
-                  prm->x_update};
+                  prm->x_update, prm->cluster_solve};
   Params inner_sp{prm->inner_maxloop, prm->inner_eps, prm->inner_restart, prm->inner_kskip, prm->inner_fix,
-                  prm->x_update};
+                  prm->x_update, prm->cluster_solve};
   if (prm->x_update < 0 || prm->x_update > 2) return set_error(ctx, KS_BAD_INPUT, "x_update must be 0, 1 or 2");
+  if (prm->cluster_solve < 0 || prm->cluster_solve > 1)
+    return set_error(ctx, KS_BAD_INPUT, "cluster_solve must be 0 or 1");
   if ((outer == KS_GCR || outer == KS_GMRES || outer == KS_VPGCR || outer == KS_VPGMRES) &&
       (outer_sp.restart < 1 || outer_sp.restart > 1024))
     return set_error(ctx, KS_BAD_INPUT, "restart must be in [1, 1024]");

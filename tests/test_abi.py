@@ -34,7 +34,7 @@ def test_abi_version_and_status_strings(ks):
     from solver_cpp_b200 import _abi
 
     lib = ks.lib()
-    assert lib.ks_abi_version() == _abi.ABI_VERSION == 2  # 2: ks_params.x_update
+    assert lib.ks_abi_version() == _abi.ABI_VERSION == 3  # 2: ks_params.x_update; 3: cluster_solve
     assert b"not converged" in lib.ks_status_string(2)
     assert b"not implemented" in lib.ks_status_string(99)
 

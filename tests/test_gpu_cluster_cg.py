@@ -1,0 +1,99 @@
+"""GPU: CG on small systems as one thread-block-cluster launch.
+
+Up to 32768 rows (one GPU, FP64) CG runs as a single launch of one cluster
+of up to 16 CTAs (ks_params.cluster_solve 0, the default); cluster_solve 1
+selects the kernel-per-step engine used for larger systems. Both paths do the
+same element-wise arithmetic and differ only in the order in which the dot
+products add their terms, so each must reproduce the reference's golden
+histories under the same criterion (golden_cases.check_history), agree with
+the other to rounding, and report the same iteration counts, verdicts and
+maxloop behaviour as the oracle.
+"""
+import numpy as np
+import pytest
+
+from golden_cases import check_history, index, load, oracle_envelope
+from solver_cpp_b200.matrices import config_problem
+
+pytestmark = pytest.mark.gpu
+
+CG_CASES = sorted(c for c, m in index().items() if m["outer"] == "CG")
+
+
+@pytest.mark.parametrize("cluster_solve", [0, 1])
+@pytest.mark.parametrize("cid", CG_CASES)
+def test_cg_golden_history_on_both_paths(ks, ctx, cid, cluster_solve):
+    meta, g = load(cid)
+    A, b, _ = config_problem(meta["problem"], meta["grid"])
+    M = ctx.matrix(A)
+    r = ks.solve(ctx, M, "CG", b, cluster_solve=cluster_solve, **meta["params"])
+    assert r.converged == meta["converged"]
+    check_history(r.hist_iter, r.hist_err, g["hist_iter"], g["hist_err"], g["envelope"], r.loop, meta["loop"],
+                  meta["loop_range"])
+    assert round(r.true_res_log10, 1) == pytest.approx(meta["true_res_log10"], abs=0.21)
+
+
+# grid edges giving n = 1, 25, 961 (not a multiple of 32), 2025, 16384, 32761
+# and 32768 (the largest single-cluster system: 16 CTAs of 2048 rows), and
+# 33124 (above the limit: the engine runs it in either mode)
+SHAPES = [("poisson2d", 1), ("poisson2d", 5), ("poisson2d", 31), ("poisson2d", 45), ("poisson2d", 128),
+          ("poisson2d", 181), ("poisson3d", 32), ("poisson2d", 182)]
+
+
+@pytest.mark.parametrize("prob,g", SHAPES)
+def test_cluster_and_engine_agree(ks, ctx, prob, g):
+    A, b, _ = config_problem(prob, g)
+    M = ctx.matrix(A)
+    r0 = ks.solve(ctx, M, "CG", b, E=1e-12, L=5000, cluster_solve=0)
+    r1 = ks.solve(ctx, M, "CG", b, E=1e-12, L=5000, cluster_solve=1)
+    assert r0.status == r1.status == 0
+    assert abs(r0.loop - r1.loop) <= max(1, r1.loop // 100)
+    assert np.linalg.norm(r0.x - r1.x) <= 1e-10 * np.linalg.norm(r1.x)
+    m = min(len(r0.hist_err), len(r1.hist_err)) // 2  # the first half agrees closely
+    assert np.allclose(r0.hist_err[:m], r1.hist_err[:m], rtol=1e-8, atol=0)
+    assert r0.true_rel_res < 2e-12
+    if A.n > 32768:  # both ran the engine: identical
+        assert np.array_equal(r0.x, r1.x) and r0.loop == r1.loop
+
+
+def test_cluster_int32_columns_and_device_vectors(ks, ctx):
+    """Columns kept as int32 (KS_MAT_INDEX32) and as 16-bit offsets give the
+    same solve bit for bit; device vectors give the host path's x."""
+    A, b, _ = config_problem("varcoef3d", 16)
+    r16 = ks.solve(ctx, ctx.matrix(A), "CG", b, E=1e-10)
+    M32 = ctx.matrix(A, index32=True)
+    assert M32.info()["index_bytes"] == 4
+    r32 = ks.solve(ctx, M32, "CG", b, E=1e-10)
+    assert np.array_equal(r16.x, r32.x) and np.array_equal(r16.hist_err, r32.hist_err)
+    B, X = ctx.vector(b), ctx.vector(n=A.n)
+    rd = ks.solve(ctx, M32, "CG", B, x=X, E=1e-10)
+    assert rd.converged and np.array_equal(X.numpy(), r32.x)
+    r2 = ks.solve(ctx, M32, "CG", b, E=1e-10)  # repeat: deterministic
+    assert np.array_equal(r2.x, r32.x) and np.array_equal(r2.hist_err, r32.hist_err)
+
+
+@pytest.mark.parametrize("L", [0, 1, 7, 255, 256, 257, 300])
+def test_cluster_maxloop_and_history_flushes(ks, ctx, oracle, L):
+    """The history is kept in shared memory and written out every 256 entries
+    and at the end: maxloop values around that boundary must give the
+    oracle's loop count, labels and verdict, and a history within the
+    reference-envelope criterion."""
+    A, b, _ = config_problem("varcoef2d", 40)
+    M = ctx.matrix(A)
+    r = ks.solve(ctx, M, "CG", b, L=L, E=1e-30)
+    o, env, lr = oracle_envelope(oracle, A, b, "CG", L=L, E=1e-30)
+    assert r.status == o["status"] == 2
+    assert r.loop == o["loop"]
+    assert np.array_equal(r.hist_iter, o["hist_iter"])
+    if L > 0:  # L = 0 stops before the first entry
+        check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
+    e = ks.solve(ctx, M, "CG", b, L=L, E=1e-30, cluster_solve=1)
+    assert np.array_equal(e.hist_iter, r.hist_iter)
+    assert np.linalg.norm(e.x - r.x) <= 1e-9 * max(np.linalg.norm(e.x), 1e-300)
+
+
+def test_cluster_solve_rejects_bad_value(ks, ctx):
+    A, b, _ = config_problem("poisson2d", 8)
+    with pytest.raises(ks.KrylovError) as e:
+        ks.solve(ctx, ctx.matrix(A), "CG", b, cluster_solve=2)
+    assert e.value.status == 5
