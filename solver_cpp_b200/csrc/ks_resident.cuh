@@ -10,8 +10,8 @@
 //    CTA's shared memory, through distributed shared memory for another CTA's
 //    rows. The matrix stays in global memory; its slice is read through L1,
 //    where it stays between iterations.
-//  * A reduction is a block sum, one cluster barrier, then the C block sums
-//    read and added in a fixed order. Every thread of every CTA adds the same values in the
+//  * A reduction is a block sum sent to every CTA of the cluster, then the C
+//    block sums added in rank order. Every CTA adds the same values in the
 //    same order, so all compute the same alpha, beta and stopping decision and
 //    leave the loop together; only rank 0's first thread writes the device
 //    state (loop counter, history, done code).
@@ -20,15 +20,19 @@
 // updates) is the kernel-per-step engine's, operation for operation; only the
 // order in which the dot products add their partial sums differs.
 //
-// Nothing here spins: a CTA waits only at the cluster's hardware barrier,
-// which every CTA of the cluster reaches (they are co-scheduled by the launch
-// and all take the same branch at every decision).
+// The CTAs are co-scheduled by the cluster launch and take the same branch at
+// every decision. A CTA waits at the cluster's hardware barrier twice (after
+// setting up, before leaving) and otherwise only on its own mbarrier for the
+// other CTAs' block sums, a wait bounded in time: if it runs out the CTA sets
+// the context's error flag and leaves the loop, and so do the others at
+// their next wait.
 #pragma once
 
 #include <cooperative_groups.h>
 
 #include <algorithm>
 
+#include "ks_spmv_tma.cuh"
 #include "ks_state.cuh"
 
 namespace ks {
@@ -123,33 +127,107 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-// Sum over the cluster of one value per thread; every thread of every CTA
-// returns the same total: the block sums are added by warp 0 of each CTA, and
-// after the cluster barrier warp 0 of every CTA adds the same C block sums in
-// the same butterfly and hands the total to its CTA through `tot`. (One warp
-// per CTA reads the other CTAs' sums: a read by every warp would queue
-// hundreds of distributed-shared-memory requests at each CTA's slot.) `red`
-// alternates between two slots: another CTA may still be reading this call's
-// slot when this CTA starts the next reduction, but not two reductions on (a
-// cluster barrier lies between).
-__device__ __forceinline__ double cluster_sum(cgx::cluster_group cl, double v, double *warp_s, double *red,
-                                              double *tot, int C) {
+// Exchange area of one CTA for the cluster reductions: every CTA's block sum
+// (two slots, used by alternate reductions), one mbarrier per slot, and the
+// outcome of the wait for the CTA.
+struct ResXchg {
+  double red[2][kResMaxCluster];
+  uint64_t bar[2];
+  int ok;
+  double tot;
+};
+
+__device__ __forceinline__ void xchg_init(cgx::cluster_group cl, ResXchg *xg) {
+  if (threadIdx.x == 0) {
+    mbar_init(&xg->bar[0], 1);
+    mbar_init(&xg->bar[1], 1);
+    mbar_fence_init();
+  }
+  cl.sync();  // every CTA's barriers are initialised before any CTA sends to them
+}
+
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Sum number m (0, 1, 2, ...) over the cluster of one value per thread.
+// Warp 0 of each CTA adds its CTA's warp sums and stores the block sum into
+// slot m % 2 of every CTA's exchange area with st.async, which completes 8
+// bytes on that CTA's mbarrier of the slot (a release at cluster scope, so the
+// CTA's earlier shared-memory writes, ordered before it by __syncthreads, are
+// visible to the receiver once its wait returns). Every thread then runs
+// `shadow` (work that needs neither the sum nor other CTAs' data) while the
+// block sums travel; thread 0 expects 8 C bytes per use of the barrier and
+// waits for them (bounded by kWaitLimitNs) and adds the C block sums in rank
+// order, the same on every CTA. Returns false in every thread of the CTA if
+// the wait ran out.
+//
+// Slot reuse: a CTA sends sum m + 2 only after completing sum m + 1, which
+// needs every CTA's block sum m + 1, which each CTA computes only after it
+// has read sum m; so sum m + 2 never lands on a slot or barrier phase still
+// in use. (A block sum may land before the receiver's own expect for that
+// phase; the transaction count then runs negative until it does.)
+template <class F>
+__device__ __forceinline__ bool cluster_sum(double v, double *warp_s, ResXchg *xg, int m, int C, int rank,
+                                            double *out, F &&shadow) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+  const int s = m & 1;
+  const uint32_t parity = (uint32_t)((m >> 1) & 1);
   v = group_sum<32>(v);
   if (lane == 0) warp_s[w] = v;
   __syncthreads();
   if (w == 0) {
-    const double t = group_sum<32>(lane < nw ? warp_s[lane] : 0.0);
-    if (lane == 0) *red = t;
+    // every group of 8 or 16 lanes adds the same warp sums, so every lane that
+    // sends holds the same block sum
+    double t;
+    if (nw > 16) {
+      t = group_sum<32>(warp_s[lane]);
+    } else if (nw > 8) {
+      const int g = lane & 15;
+      t = group_sum<16>(g < nw ? warp_s[g] : 0.0);
+    } else {
+      const int g = lane & 7;
+      t = group_sum<8>(g < nw ? warp_s[g] : 0.0);
+    }
+    if (lane == 0) mbar_expect_tx(&xg->bar[s], 8u * (uint32_t)C);
+    if (lane < C) {
+      uint32_t ra, rb;
+      asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(smem_u32(&xg->red[s][rank])), "r"(lane));
+      asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(smem_u32(&xg->bar[s])), "r"(lane));
+      asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(ra),
+                   "l"(__double_as_longlong(t)), "r"(rb)
+                   : "memory");
+    }
   }
-  cl.sync();
-  if (w == 0) {
-    const double u = group_sum<32>(lane < C ? *cl.map_shared_rank(red, (unsigned)lane) : 0.0);
-    if (lane == 0) *tot = u;
+  shadow();
+  if (threadIdx.x == 0) {
+    bool ok = mbar_try_wait_cluster(&xg->bar[s], parity);
+    if (!ok) {
+      const unsigned long long t0 = global_ns();
+      while (!(ok = mbar_try_wait_cluster(&xg->bar[s], parity)))
+        if (global_ns() - t0 > kWaitLimitNs) break;
+    }
+    xg->ok = ok ? 1 : 0;
+    if (ok) {
+      double u = 0.0;
+      for (int c = 0; c < C; c++) u += xg->red[s][c];  // rank order
+      xg->tot = u;
+    }
   }
   __syncthreads();
-  return *tot;
+  *out = xg->tot;
+  return xg->ok != 0;
 }
+
+__device__ __forceinline__ void no_shadow() {}
 
 struct ResCgArgs {
   const int *ptr;
@@ -159,27 +237,31 @@ struct ResCgArgs {
   const double *b;
   double *x;
   DevState *st;  // reset by InitOp before the launch
+  int *err;      // set if a bounded wait ran out
   int n;
   int shift;  // rows per CTA = 2^shift
 };
 
 // cg::solve (cg.cpp:148-240) from x = 0 to the stopping test, in one launch,
-// with two cluster barriers per iteration. The CTAs publish r (not p): the
-// SpMV of iteration L forms p_L = beta p_{L-1} + r_L for every column it
-// gathers, from the owner's p_{L-1} and r_L, with the operations of the
-// direction update (so the value equals the owner's p_L bit for bit), while
-// each CTA writes its own p_L into the other of two p buffers. The reduction
-// barrier after the x/r update then also publishes r_{L+1} and p_L, and the
-// separate barrier after the direction update is not needed. x, r and p live
-// in the CTA's shared memory (a thread reads and writes only its own rows of
-// x); q, needed across the (p,q) reduction, in registers.
+// with two cluster reductions per iteration and no other synchronisation
+// between CTAs. The CTAs publish r (not p): the SpMV of iteration L forms
+// p_L = beta p_{L-1} + r_L for every column it gathers, from the owner's
+// p_{L-1} and r_L, with the operations of the direction update (so the value
+// equals the owner's p_L bit for bit), while each CTA writes its own p_L into
+// the other of two p buffers. The reduction after the x/r update then also
+// publishes r_{L+1} and p_L. x, r and p live in the CTA's shared memory (a
+// thread reads and writes only its own rows of x); q, needed across the (p,q)
+// reduction, in registers. With one row per thread the values the next SpMV
+// gathers (up to kResPre per row) are loaded right after that reduction, so
+// their latency overlaps the beta division and the stopping test.
+constexpr int kResPre = 7;
+
 template <int R, bool I16>
 __global__ void __launch_bounds__(kResThreads, 1) k_cg_resident(const ResCgArgs a) {
   cgx::cluster_group cl = cgx::this_cluster();
   extern __shared__ double dyn_s[];  // slices of x, r, p (two buffers)
   __shared__ double warp_s[32];
-  __shared__ double red_s[2];
-  __shared__ double tot_s;
+  __shared__ ResXchg xg;
   __shared__ double hist_e[kResHist];
   __shared__ long long hist_i[kResHist];
   const int C = (int)cl.num_blocks();
@@ -190,7 +272,9 @@ __global__ void __launch_bounds__(kResThreads, 1) k_cg_resident(const ResCgArgs 
   const int r0 = rank << a.shift;
   ResScal S{a.st, rank == 0 && threadIdx.x == 0, a.st->k.s[S_EPS], a.st->k.aux[A_MAXLOOP], hist_e, hist_i};
   S.begin();
-  int red_i = 0;
+  xchg_init(cl, &xg);
+  int m = 0;  // reductions so far
+  bool ok = true;
   double q[R];
   double acc = 0.0;
 #pragma unroll
@@ -206,62 +290,138 @@ __global__ void __launch_bounds__(kResThreads, 1) k_cg_resident(const ResCgArgs 
     p_s0[li] = ri;  // p_0 := r_1 with beta_0 = 0 gives p_1 = 0*r_1 + r_1 = r_1 (r finite here)
     q[k] = 0.0;
   }
+  // the gather of one row (R == 1): its first kResPre columns' p_{L-1}, r_L
+  // and matrix values; the rest of a longer row is read in the SpMV itself
+  const int i1 = r0 + (int)threadIdx.x;
+  const bool row1 = R == 1 && i1 < a.n;
+  int j0 = 0, j1 = 0;
+  if (row1) {
+    j0 = __ldg(a.ptr + i1);
+    j1 = __ldg(a.ptr + i1 + 1);
+  }
+  double pv[kResPre], rv[kResPre], av[kResPre];
+  auto gather = [&](const double *p_old) {
+#pragma unroll
+    for (int t = 0; t < kResPre; t++) {
+      if (row1 && t < j1 - j0) {
+        const int j = j0 + t;
+        const int c = I16 ? i1 + (int)__ldg(a.col16 + j) : __ldg(a.col + j);
+        const int o = c >> a.shift, lc = c & mask;
+        const double *pp = p_old + lc, *rq = r_s + lc;
+        if (o != rank) {  // another CTA's row: its shared memory, through the cluster
+          pp = cl.map_shared_rank(pp, (unsigned)o);
+          rq = cl.map_shared_rank(rq, (unsigned)o);
+        }
+        pv[t] = *pp;
+        rv[t] = *rq;
+        av[t] = __ldg(a.val + j);
+      }
+    }
+  };
   // |b|^2 and (r,r) are the same sum, r being b
-  double rr = cluster_sum(cl, acc, warp_s, red_s + (red_i++ & 1), &tot_s, C);
+  double rr = 0.0;
+  ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &rr, no_shadow);
+  if (R == 1) gather(p_s0);
   const double bnorm = sqrt(rr);
   if (S.writer) a.st->k.s[S_BNORM] = bnorm;
-  S.check_top(1, sqrt(rr) / bnorm);
-  double beta = 0.0;
+  // The stopping test of iteration L (on (r_L, r_L)) runs in the shadow of
+  // the next (p,q) reduction: the SpMV of iteration L runs before the test
+  // and is discarded if the test stops the method (it changes only p_new and
+  // q, which are then unused). The verdicts and the history are the
+  // kernel-per-step engine's.
+  double rr_chk = rr;
   long long L = 1;
-  while (S.done == kRunning) {
+  double beta = 0.0, alpha = 0.0;
+  while (ok) {
     const double *p_old = (L & 1) ? p_s0 : p_s1;  // p_{L-1}
     double *p_new = (L & 1) ? p_s1 : p_s0;        // p_L
     // p_L = beta p_{L-1} + r_L; q = A p_L; (p,q) -> alpha
     acc = 0.0;
-#pragma unroll
-    for (int k = 0; k < R; k++) {
-      const int li = threadIdx.x + k * T, i = r0 + li;
-      if (i < a.n) {
+    if (R == 1) {
+      if (row1) {
+        const int li = (int)threadIdx.x;
         const double pk = add_rn(mul_rn(beta, p_old[li]), r_s[li]);
         p_new[li] = pk;
-        const int j0 = __ldg(a.ptr + i), j1 = __ldg(a.ptr + i + 1);
-        double s = 0.0;
-#pragma unroll 4
-        for (int j = j0; j < j1; j++) {
-          const int c = I16 ? i + (int)__ldg(a.col16 + j) : __ldg(a.col + j);
+        double sum = 0.0;
+#pragma unroll
+        for (int t = 0; t < kResPre; t++)
+          if (t < j1 - j0) sum = add_rn(sum, mul_rn(av[t], add_rn(mul_rn(beta, pv[t]), rv[t])));
+        for (int j = j0 + kResPre; j < j1; j++) {
+          const int c = I16 ? i1 + (int)__ldg(a.col16 + j) : __ldg(a.col + j);
           const int o = c >> a.shift, lc = c & mask;
           const double *pp = p_old + lc, *rq = r_s + lc;
-          if (o != rank) {  // another CTA's row: its shared memory, through the cluster
+          if (o != rank) {
             pp = cl.map_shared_rank(pp, (unsigned)o);
             rq = cl.map_shared_rank(rq, (unsigned)o);
           }
-          s = add_rn(s, mul_rn(__ldg(a.val + j), add_rn(mul_rn(beta, *pp), *rq)));
+          sum = add_rn(sum, mul_rn(__ldg(a.val + j), add_rn(mul_rn(beta, *pp), *rq)));
         }
-        q[k] = s;
-        acc = add_rn(acc, mul_rn(pk, s));
+        q[0] = sum;
+        acc = add_rn(0.0, mul_rn(pk, sum));
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < R; k++) {
+        const int li = threadIdx.x + k * T, i = r0 + li;
+        if (i < a.n) {
+          const double pk = add_rn(mul_rn(beta, p_old[li]), r_s[li]);
+          p_new[li] = pk;
+          const int jb = __ldg(a.ptr + i), je = __ldg(a.ptr + i + 1);
+          double sum = 0.0;
+#pragma unroll 4
+          for (int j = jb; j < je; j++) {
+            const int c = I16 ? i + (int)__ldg(a.col16 + j) : __ldg(a.col + j);
+            const int o = c >> a.shift, lc = c & mask;
+            const double *pp = p_old + lc, *rq = r_s + lc;
+            if (o != rank) {
+              pp = cl.map_shared_rank(pp, (unsigned)o);
+              rq = cl.map_shared_rank(rq, (unsigned)o);
+            }
+            sum = add_rn(sum, mul_rn(__ldg(a.val + j), add_rn(mul_rn(beta, *pp), *rq)));
+          }
+          q[k] = sum;
+          acc = add_rn(acc, mul_rn(pk, sum));
+        }
       }
     }
-    const double pq = cluster_sum(cl, acc, warp_s, red_s + (red_i++ & 1), &tot_s, C);
-    const double alpha = S.rdiv(rr, pq);
+    double pq = 0.0;
+    if (!(ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &pq,
+                           [&] { S.check_top(L, sqrt(rr_chk) / bnorm); })))
+      break;
+    if (S.done != kRunning) break;  // iteration L does not run
+    alpha = S.rdiv(rr, pq);
     if (S.done != kRunning) break;
-    // x += alpha p; r -= alpha q (published); (r,r) -> beta; stopping test
+    // r -= alpha q (published); (r,r) -> beta; x += alpha p in the shadow
     acc = 0.0;
 #pragma unroll
     for (int k = 0; k < R; k++) {
       const int li = threadIdx.x + k * T, i = r0 + li;
       if (i < a.n) {
-        x_s[li] = add_rn(mul_rn(alpha, p_new[li]), x_s[li]);
         const double rk = add_rn(mul_rn(-alpha, q[k]), r_s[li]);
         r_s[li] = rk;
         acc = add_rn(acc, mul_rn(rk, rk));
       }
     }
-    const double rr2 = cluster_sum(cl, acc, warp_s, red_s + (red_i++ & 1), &tot_s, C);
+    double rr2 = 0.0;
+    if (!(ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &rr2, [&] {
+#pragma unroll
+          for (int k = 0; k < R; k++) {
+            const int li = threadIdx.x + k * T, i = r0 + li;
+            if (i < a.n) x_s[li] = add_rn(mul_rn(alpha, p_new[li]), x_s[li]);
+          }
+        })))
+      break;
+    if (R == 1) gather(p_new);  // for iteration L + 1, whose p_L is p_new
     beta = S.rdiv(rr2, rr);
     rr = rr2;
-    S.check_top(L + 1, sqrt(rr2) / bnorm);
+    rr_chk = rr2;
     L++;
+    if (S.done != kRunning) {  // beta's division stopped the method: the test still runs
+      S.check_top(L, sqrt(rr_chk) / bnorm);
+      break;
+    }
   }
+  if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
 #pragma unroll
   for (int k = 0; k < R; k++) {
     const int li = threadIdx.x + k * T, i = r0 + li;

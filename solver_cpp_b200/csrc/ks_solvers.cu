@@ -647,7 +647,7 @@ inline bool run_cg_resident(const Env<double> &E, const double *b, double *x, ks
   const ResShape sh = resident_shape(E.n);
   if (!sh.C) return false;
   const CsrDev &A = *E.A;
-  const ResCgArgs a{A.ptr, A.col, A.col16, A.val, b, x, E.st, (int)E.n, sh.shift};
+  const ResCgArgs a{A.ptr, A.col, A.col16, A.val, b, x, E.st, E.ctx->d_err, (int)E.n, sh.shift};
   bool fits = false;
   if (res_cg(sh, A.col16 != nullptr, E.ctx->stream, a, true, &fits) != cudaSuccess || !fits) {
     (void)cudaGetLastError();
