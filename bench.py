@@ -361,6 +361,15 @@ def run_ours(args, world, rank, local):
         e2e = {"value": ems / 1e3, "unit": "s", "h2d_bytes_per_step": 8 * nl,
                "d2h_bytes_per_step": 8 * nl + 16 * int(rep.hist_len) + 64}
 
+    # CG on up to 32768 rows runs as one thread-block-cluster launch: its time
+    # per iteration (device events around the solve, from the report)
+    if W["outer"] == "CG" and not split and nl <= 32768 and adj is None and res.loop > 1:
+        roofline["solve_kernel"] = {
+            "kernel": "k_cg_resident (whole solve, one thread-block cluster)",
+            "solve_ms": round(res.solve_seconds * 1e3, 4),
+            "us_per_iteration": round(res.solve_seconds * 1e6 / (res.loop - 1), 3),
+            "bound": "latency of the two cross-SM reductions per iteration (inputs in L1 / shared memory)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and adj is None:
         cpu = cpu_baseline_port(A, b, W, res)
