@@ -176,13 +176,22 @@ def barrier(world):
         dist.barrier()
 
 
-def spmv_bytes(n, nnz, values, index_bytes=4):
-    """Algorithmic bytes of one SpMV: values + column indices (int32, or the
-    int16 row offsets the library stores when they fit) + int32 row offsets
-    + x read once + y written once."""
+def spmv_bytes(n, nnz, values, index_bytes=4, diagonals=0):
+    """Algorithmic bytes of one SpMV. CSR: values + column indices (int32, or
+    the int16 row offsets the library stores when they fit) + int32 row
+    offsets + x read once + y written once. Diagonal copy (`diagonals` > 0):
+    the diagonals' values (zeros where a row has no entry) + one mask byte
+    per row + x read once + y written once."""
     vb = {"fp64": 8, "fp32": 4, "bf16": 2}[values]
     xb = 8 if values == "fp64" else 4
+    if diagonals:
+        return diagonals * n * vb + n + xb * n + xb * n
     return nnz * (vb + index_bytes) + 4 * (n + 1) + xb * n + xb * n
+
+
+def layout_key(info):
+    """Short name of the layout the SpMV reads: d<diagonals> or i<index bytes>."""
+    return f"d{info['diagonals']}" if info.get("diagonals") else f"i{info['index_bytes']}"
 
 
 def run_ours(args, world, rank, local):
@@ -303,22 +312,23 @@ def run_ours(args, world, rank, local):
         s1.record(stream)
     torch.cuda.synchronize()
     spmv_ms = s0.elapsed_time(s1) / reps
-    ib = M.info()["index_bytes"]
-    alg = spmv_bytes(nl, nnzl, vals, ib)
+    minfo = M.info()
+    ib, nd = minfo["index_bytes"], minfo["diagonals"]
+    alg = spmv_bytes(nl, nnzl, vals, ib, nd)
     peak, peak_kind = load_peaks()
     achieved = alg / (spmv_ms / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "spmv_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(f"{args.workload}:{vals}:i{ib}")
+            traffic = json.load(open(tf)).get(f"{args.workload}:{vals}:{layout_key(minfo)}")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": f"spmv_{vals}",
-                "alg_bytes_per_launch": alg, "index_bytes": ib, "launch_ms": round(spmv_ms, 5),
+                "alg_bytes_per_launch": alg, "layout": layout_key(minfo), "launch_ms": round(spmv_ms, 5),
                 "peak_kind": peak_kind}
-    fp64_bytes = spmv_bytes(nl, nnzl, "fp64", ib)
+    fp64_bytes = spmv_bytes(nl, nnzl, "fp64", ib, nd)
     if vals != "fp64":  # also the FP64 SpMV of the outer loop
         x64, y64 = ctx.vector(np.random.default_rng(0).standard_normal(nl)), ctx.vector(n=nl)
         ks.spmv(M, x64, y64)
@@ -518,8 +528,10 @@ def spmv_only(args):
     ctx = ks.Context(0)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
-    M = ctx.matrix(A, fp32=args.spmv_only == "fp32", bf16=args.spmv_only == "bf16", index32=args.index32)
-    ib = M.info()["index_bytes"]
+    M = ctx.matrix(A, fp32=args.spmv_only == "fp32", bf16=args.spmv_only == "bf16", index32=args.index32,
+                   diag=not args.csr)
+    info = M.info()
+    ib, nd = info["index_bytes"], info["diagonals"]
     dt = ks.FP64 if args.spmv_only == "fp64" else ks.FP32
     vcode = {"fp64": ks.FP64, "fp32": ks.FP32, "bf16": ks.BF16}[args.spmv_only]
     X = ctx.vector(np.random.default_rng(0).standard_normal(A.n), dtype=dt)
@@ -535,11 +547,12 @@ def spmv_only(args):
         e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    alg = spmv_bytes(A.n, A.nnz, args.spmv_only, ib)
+    alg = spmv_bytes(A.n, A.nnz, args.spmv_only, ib, nd)
     peak, kind = load_peaks()
     gbs = alg / (ms / 1e3) / 1e9
     print(json.dumps({"kernel": f"spmv_{args.spmv_only}", "workload": args.workload, "n": A.n, "nnz": A.nnz,
-                      "index_bytes": ib, "alg_bytes": alg, "ms": round(ms, 5), "gbs": round(gbs, 1), "peak": peak,
+                      "layout": layout_key(info), "index_bytes": ib, "diagonals": nd, "alg_bytes": alg,
+                      "ms": round(ms, 5), "gbs": round(gbs, 1), "peak": peak,
                       "frac": round(gbs / peak, 4), "peak_kind": kind}))
     M.close()
     ctx.close()
@@ -606,6 +619,7 @@ def main():
     ap.add_argument("--spmv-only", choices=["fp64", "fp32", "bf16"], default=None,
                     help="time only the SpMV kernel on the workload's matrix (profiling)")
     ap.add_argument("--index32", action="store_true", help="with --spmv-only: int32 column indices")
+    ap.add_argument("--csr", action="store_true", help="with --spmv-only: CSR only (no diagonal copy)")
     ap.add_argument("--split", action="store_true",
                     help="with --gpus N > 1: split the one system's rows over the ranks (strong scaling) "
                          "instead of one replica per rank")

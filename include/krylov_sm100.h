@@ -88,6 +88,13 @@ int ks_abi_version(void);
  * index bytes of banded and stencil matrices; results are identical. This
  * flag keeps the int32 columns instead. */
 #define KS_MAT_INDEX32 8u
+/* By default a matrix whose rows hold their columns at no more than 8
+ * distinct offsets from the row (stencils, banded matrices), each row in
+ * increasing column order, with the diagonals at least 3/4 full, also keeps
+ * a diagonal copy (values diagonal-major, one presence mask byte per row),
+ * which the SpMV reads instead of the CSR arrays: no column indices at all,
+ * coalesced reads of x. Results are identical. This flag keeps CSR only. */
+#define KS_MAT_NO_DIAG 16u
 
 /* Upload a host CSR matrix (collection::CudaCopy_Part1,
  * solver_collection.cpp:932-942) and build the row-block schedule of the
@@ -109,6 +116,9 @@ ks_status ks_mat_info(const ks_mat *mat, int64_t *n, int64_t *nnz,
 /* Bytes per column index the SpMV reads for A (2 or 4) and for A^T (0 when
  * there is no transpose). No counterpart in the reference. */
 ks_status ks_mat_index_bytes(const ks_mat *mat, int *a_bytes, int *t_bytes);
+/* Diagonals of the diagonal copy of A and of A^T (0: the SpMV reads CSR). No
+ * counterpart in the reference. */
+ks_status ks_mat_diagonals(const ks_mat *mat, int *a_diagonals, int *t_diagonals);
 /* Copy the device-built transpose back (CSR of A^T: tptr[n+1], trow[nnz],
  * tval[nnz]), i.e. the CSC arrays the reference's CSR2CSC returns. */
 ks_status ks_mat_transpose_download(const ks_mat *mat, int32_t *tptr,

@@ -84,8 +84,8 @@ class Context:
     def set_stream(self, stream_ptr):
         _check(lib().ks_ctx_set_stream(self.handle, C.c_void_p(stream_ptr)), self.handle, "set_stream")
 
-    def matrix(self, A: CSR, transpose=False, fp32=False, bf16=False, index32=False) -> "Matrix":
-        return Matrix(self, A, transpose=transpose, fp32=fp32, bf16=bf16, index32=index32)
+    def matrix(self, A: CSR, transpose=False, fp32=False, bf16=False, index32=False, diag=True) -> "Matrix":
+        return Matrix(self, A, transpose=transpose, fp32=fp32, bf16=bf16, index32=index32, diag=diag)
 
     def vector(self, data=None, n=None, dtype=FP64) -> "Vector":
         return Vector(self, data=data, n=n, dtype=dtype)
@@ -94,16 +94,17 @@ class Context:
 class Matrix:
     """Device CSR matrix (``ks_mat``), optionally with its transpose and
     FP32 / BF16 value copies. ``index32`` keeps int32 column indices in the
-    SpMV instead of the 16-bit row offsets used when they fit."""
+    SpMV instead of the 16-bit row offsets used when they fit; ``diag=False``
+    keeps CSR only (no diagonal copy of a stencil matrix)."""
 
-    def __init__(self, ctx: Context, A: CSR, transpose=False, fp32=False, bf16=False, index32=False):
+    def __init__(self, ctx: Context, A: CSR, transpose=False, fp32=False, bf16=False, index32=False, diag=True):
         self.ctx = ctx
         self.n, self.nnz = A.n, A.nnz
         ptr = np.ascontiguousarray(A.ptr, dtype=np.int32)
         col = np.ascontiguousarray(A.col, dtype=np.int32)
         val = np.ascontiguousarray(A.val, dtype=np.float64)
         flags = (_abi.MAT_TRANSPOSE if transpose else 0) | (_abi.MAT_FP32 if fp32 else 0) | (
-            _abi.MAT_BF16 if bf16 else 0) | (_abi.MAT_INDEX32 if index32 else 0)
+            _abi.MAT_BF16 if bf16 else 0) | (_abi.MAT_INDEX32 if index32 else 0) | (0 if diag else _abi.MAT_NO_DIAG)
         h = C.c_void_p()
         _check(lib().ks_csr_upload(ctx.handle, self.n, self.nnz, _ptr(ptr), _ptr(col), _ptr(val), flags,
                                    C.byref(h)), ctx.handle, "ks_csr_upload")
@@ -126,8 +127,10 @@ class Matrix:
         _check(lib().ks_mat_info(self.handle, C.byref(n), C.byref(nnz), C.byref(rb)), self.ctx.handle, "info")
         a, t = C.c_int(), C.c_int()
         _check(lib().ks_mat_index_bytes(self.handle, C.byref(a), C.byref(t)), self.ctx.handle, "index_bytes")
+        da, dt = C.c_int(), C.c_int()
+        _check(lib().ks_mat_diagonals(self.handle, C.byref(da), C.byref(dt)), self.ctx.handle, "diagonals")
         return {"n": n.value, "nnz": nnz.value, "row_blocks": rb.value, "index_bytes": a.value,
-                "t_index_bytes": t.value}
+                "t_index_bytes": t.value, "diagonals": da.value, "t_diagonals": dt.value}
 
     def transpose_arrays(self):
         tptr = np.zeros(self.n + 1, dtype=np.int32)
@@ -463,7 +466,7 @@ class SplitMatrix(Matrix):
     solves on it take and return vectors of the local length r1 - r0."""
 
     def __init__(self, ctx: Context, comm: Comm, A: CSR, r0: int, r1: int, transpose=False, fp32=False,
-                 bf16=False, index32=False, AT: CSR | None = None):
+                 bf16=False, index32=False, AT: CSR | None = None, diag=True):
         self.ctx = ctx
         self.comm = comm
         self.r0, self.r1, self.n_global = int(r0), int(r1), A.n
@@ -483,7 +486,7 @@ class SplitMatrix(Matrix):
             tc = np.ascontiguousarray(T.col[k0:k1], dtype=np.int32)
             tv = np.ascontiguousarray(T.val[k0:k1], dtype=np.float64)
         flags = (_abi.MAT_TRANSPOSE if transpose else 0) | (_abi.MAT_FP32 if fp32 else 0) | (
-            _abi.MAT_BF16 if bf16 else 0) | (_abi.MAT_INDEX32 if index32 else 0)
+            _abi.MAT_BF16 if bf16 else 0) | (_abi.MAT_INDEX32 if index32 else 0) | (0 if diag else _abi.MAT_NO_DIAG)
         h = C.c_void_p()
         _check(lib().ks_dist_upload(ctx.handle, comm.handle, A.n, self.r0, self.r1, _ptr(ptr),
                                     _ptr(col) if col.size else None, _ptr(val) if val.size else None,

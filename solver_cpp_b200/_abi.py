@@ -41,6 +41,7 @@ MAT_TRANSPOSE = 1
 MAT_FP32 = 2
 MAT_BF16 = 4
 MAT_INDEX32 = 8
+MAT_NO_DIAG = 16
 
 
 ABI_VERSION = 3  # KS_ABI_VERSION of the header these structures mirror
@@ -88,6 +89,7 @@ SIGNATURES = [
     ("ks_mat_destroy", C.c_int, [_VP]),
     ("ks_mat_info", C.c_int, [_VP, _PI64, _PI64, _PI64]),
     ("ks_mat_index_bytes", C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("ks_mat_diagonals", C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("ks_mat_transpose_download", C.c_int, [_VP, _VP, _VP, _VP]),
     ("ks_vec_create", C.c_int, [_VP, _I64, C.c_int, C.POINTER(_VP)]),
     ("ks_vec_wrap", C.c_int, [_VP, _I64, C.c_int, _VP, C.POINTER(_VP)]),

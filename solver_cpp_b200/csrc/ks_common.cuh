@@ -21,6 +21,7 @@ constexpr int kPad = 8;             // tail padding of col/val arrays (elements)
 constexpr int kMaxDots = 8;         // simultaneous reductions in one kernel
 constexpr int kBlockDotGroup = 8;   // tall-skinny dots per pass
 constexpr int kMaxGroups = 128;     // block-dot groups in one launch (1024 dots)
+constexpr int kMaxDiag = 8;         // diagonals of a matrix's diagonal copy (8-bit row masks)
 
 // ---------------------------------------------------------------- state
 // Device-resident scalar state of one running Krylov method. Every scalar of
@@ -78,6 +79,21 @@ struct CsrDev {
   int *rb = nullptr;  // row-block boundaries, nrb + 1 entries
   int4 *rbi = nullptr;  // per row block: first row, end row, first nonzero, end nonzero
   int nrb = 0;
+  // Diagonal copy of a stencil-like matrix, read by the SpMV instead of the
+  // CSR arrays: every row holds its columns at offsets (col - row) from a set
+  // of dia_nd <= kMaxDiag offsets, dia_off ascending. Values are stored
+  // diagonal-major, dia_val[d * n + i] (0 where row i has no entry on
+  // diagonal d), and bit d of dia_mask[i] is set where it has one. Kept only
+  // when every row lists its columns in increasing order (so a row summed
+  // diagonal by diagonal is summed in its CSR order) and the diagonals are at
+  // least 3/4 full; dia_nd = 0 otherwise or with KS_MAT_NO_DIAG.
+  int dia_nd = 0;
+  int dia_off[kMaxDiag] = {};
+  int dia_cmin = 0, dia_cmax = 0;  // columns of x the diagonals may reach
+  double *dia_val = nullptr;
+  float *dia_val32 = nullptr;
+  __nv_bfloat16 *dia_val16 = nullptr;
+  unsigned char *dia_mask = nullptr;
 };
 
 template <class MT>

@@ -1,5 +1,6 @@
 // Context, matrices, vectors and the primitive operations of the C ABI.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -230,7 +231,142 @@ __global__ void k_col16(const int *__restrict__ ptr, const int *__restrict__ col
   if (bad) atomicOr(flags, bad);
 }
 
+// Diagonal copy (CsrDev::dia_*), pass 1: the distinct offsets col - row of
+// the matrix, collected in a per-CTA set in shared memory and merged into the
+// global set `offs` (kMaxDiag slots, kDiagEmpty where free). flags |= 1 for a
+// row whose columns are not strictly increasing, |= 2 for more than kMaxDiag
+// distinct offsets.
+constexpr int kDiagEmpty = INT_MIN;
+
+__device__ __forceinline__ bool diag_insert(int *set, int d) {
+  for (int s = 0; s < kMaxDiag; s++) {
+    int v = *(volatile int *)&set[s];
+    if (v == kDiagEmpty) {
+      v = atomicCAS(&set[s], kDiagEmpty, d);
+      if (v == kDiagEmpty) return true;
+    }
+    if (v == d) return true;
+  }
+  return false;
+}
+
+__global__ void k_dia_scan(const int *__restrict__ ptr, const int *__restrict__ col, int n, int *offs, int *flags) {
+  __shared__ int s_off[kMaxDiag];
+  __shared__ int s_flags;
+  if (threadIdx.x < kMaxDiag) s_off[threadIdx.x] = kDiagEmpty;
+  if (threadIdx.x == 0) s_flags = 0;
+  __syncthreads();
+  int bad = 0;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    const int j0 = ptr[r], j1 = ptr[r + 1];
+    int last = kDiagEmpty;
+    for (int j = j0; j < j1; j++) {
+      const int c = col[j];
+      if (j > j0 && c <= col[j - 1]) bad |= 1;
+      const int d = c - (int)r;
+      if (d == last) continue;
+      if (diag_insert(s_off, d))
+        last = d;
+      else
+        bad |= 2;
+    }
+  }
+  if (bad) atomicOr(&s_flags, bad);
+  __syncthreads();
+  if (threadIdx.x < kMaxDiag) {
+    const int d = s_off[threadIdx.x];
+    if (d != kDiagEmpty && !diag_insert(offs, d)) atomicOr(flags, 2);
+  }
+  if (threadIdx.x == 0 && s_flags) atomicOr(flags, s_flags);
+}
+
+struct DiagOffsets {
+  int nd;
+  int off[kMaxDiag];
+};
+
+// Pass 2: values diagonal-major (dval zeroed beforehand) and the row masks.
+__global__ void k_dia_fill(const int *__restrict__ ptr, const int *__restrict__ col,
+                           const double *__restrict__ val, int n, DiagOffsets o, double *__restrict__ dval,
+                           unsigned char *__restrict__ mask) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    unsigned m = 0;
+    for (int j = ptr[r]; j < ptr[r + 1]; j++) {
+      const int d = col[j] - (int)r;
+      for (int k = 0; k < o.nd; k++) {
+        if (o.off[k] == d) {
+          dval[(long long)k * n + r] = val[j];
+          m |= 1u << k;
+          break;
+        }
+      }
+    }
+    mask[r] = (unsigned char)m;
+  }
+}
+
+static void free_dia(CsrDev &A) {
+  cudaFree(A.dia_val);
+  cudaFree(A.dia_val32);
+  cudaFree(A.dia_val16);
+  cudaFree(A.dia_mask);
+  A.dia_val = nullptr;
+  A.dia_val32 = nullptr;
+  A.dia_val16 = nullptr;
+  A.dia_mask = nullptr;
+  A.dia_nd = 0;
+}
+
+// Builds the diagonal copy when the matrix qualifies (CsrDev::dia_*); leaves
+// dia_nd = 0 otherwise. Value copies follow the CSR ones (FP32, BF16).
+static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long long cmin, long long cmax) {
+  if (A.n < 1 || A.nnz < 1) return KS_OK;
+  const int g = ctx->num_sms * 8;
+  int *d_buf = nullptr;  // kMaxDiag offsets, then the flags
+  KS_CUDA(ctx, cudaMalloc(&d_buf, sizeof(int) * (kMaxDiag + 1)));
+  int h_buf[kMaxDiag + 1];
+  for (int k = 0; k < kMaxDiag; k++) h_buf[k] = kDiagEmpty;
+  h_buf[kMaxDiag] = 0;
+  cudaError_t e = cudaMemcpyAsync(d_buf, h_buf, sizeof(h_buf), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    k_dia_scan<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.n, d_buf, d_buf + kMaxDiag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_buf, d_buf, sizeof(h_buf), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_buf);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "diagonal scan");
+  if (h_buf[kMaxDiag]) return KS_OK;  // unordered rows or too many diagonals: CSR only
+  DiagOffsets o{};
+  for (int k = 0; k < kMaxDiag; k++)
+    if (h_buf[k] != kDiagEmpty) o.off[o.nd++] = h_buf[k];
+  std::sort(o.off, o.off + o.nd);
+  if (o.nd < 1 || 4 * A.nnz < 3LL * o.nd * A.n) return KS_OK;  // diagonals less than 3/4 full
+  const long long len = (long long)o.nd * A.n;
+  KS_CUDA(ctx, cudaMalloc(&A.dia_val, sizeof(double) * (size_t)len));
+  KS_CUDA(ctx, cudaMalloc(&A.dia_mask, (size_t)A.n));
+  KS_CUDA(ctx, cudaMemsetAsync(A.dia_val, 0, sizeof(double) * (size_t)len, ctx->stream));
+  k_dia_fill<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.val, A.n, o, A.dia_val, A.dia_mask);
+  if (flags & KS_MAT_FP32) {
+    KS_CUDA(ctx, cudaMalloc(&A.dia_val32, sizeof(float) * (size_t)len));
+    k_to_f32<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val32, len);
+  }
+  if (flags & KS_MAT_BF16) {
+    KS_CUDA(ctx, cudaMalloc(&A.dia_val16, sizeof(__nv_bfloat16) * (size_t)len));
+    k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val16, len);
+  }
+  KS_CUDA(ctx, cudaGetLastError());
+  A.dia_nd = o.nd;
+  for (int k = 0; k < kMaxDiag; k++) A.dia_off[k] = k < o.nd ? o.off[k] : 0;
+  A.dia_cmin = (int)cmin;
+  A.dia_cmax = (int)cmax;
+  return KS_OK;
+}
+
 static void free_csr(CsrDev &A) {
+  free_dia(A);
   cudaFree(A.ptr);
   cudaFree(A.col);
   cudaFree(A.col16);
@@ -302,6 +438,7 @@ static ks_status finish_csr(ks_ctx *ctx, CsrDev &A, const int32_t *host_ptr, uns
     k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.val, A.val16, tot);
   }
   KS_CUDA(ctx, cudaGetLastError());
+  if (!(flags & KS_MAT_NO_DIAG)) KS_TRY(build_diagonals(ctx, A, flags, cmin, cmax));
   // rb and rbi are host vectors going out of scope: the copies must complete first.
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return KS_OK;
@@ -684,6 +821,13 @@ ks_status ks_mat_index_bytes(const ks_mat *m, int *a_bytes, int *t_bytes) {
   if (!m) return KS_BAD_INPUT;
   if (a_bytes) *a_bytes = m->A.col16 ? 2 : 4;
   if (t_bytes) *t_bytes = m->has_T ? (m->T.col16 ? 2 : 4) : 0;
+  return KS_OK;
+}
+
+ks_status ks_mat_diagonals(const ks_mat *m, int *a_diagonals, int *t_diagonals) {
+  if (!m) return KS_BAD_INPUT;
+  if (a_diagonals) *a_diagonals = m->A.dia_nd;
+  if (t_diagonals) *t_diagonals = m->has_T ? m->T.dia_nd : 0;
   return KS_OK;
 }
 

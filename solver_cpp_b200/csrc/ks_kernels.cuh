@@ -8,6 +8,7 @@
 
 #include "ks_common.cuh"
 #include "ks_dist.cuh"
+#include "ks_spmv_dia.cuh"
 #include "ks_spmv_tma.cuh"
 
 namespace ks {
@@ -280,6 +281,77 @@ inline void with_rank_sums(ks_ctx *ctx, const Op &op, Stop stop, F &&launch) {
   launch(op);
 }
 
+template <class MT>
+inline const MT *dia_values_of(const CsrDev &A);
+template <>
+inline const double *dia_values_of<double>(const CsrDev &A) {
+  return A.dia_val;
+}
+template <>
+inline const float *dia_values_of<float>(const CsrDev &A) {
+  return A.dia_val32;
+}
+template <>
+inline const __nv_bfloat16 *dia_values_of<__nv_bfloat16>(const CsrDev &A) {
+  return A.dia_val16;
+}
+
+template <class MT>
+inline DiaT<MT> dview(const CsrDev &A) {
+  DiaT<MT> d;
+  d.val = dia_values_of<MT>(A);
+  d.mask = A.dia_mask;
+  d.n = A.n;
+  d.nd = A.dia_nd;
+  d.cmin = A.dia_cmin;
+  d.cmax = A.dia_cmax;
+  for (int k = 0; k < kMaxDiag; k++) d.off[k] = A.dia_off[k];
+  return d;
+}
+
+template <int NV, int NDG, class MT, class GX, class Epi>
+inline int spmv_dia_ctas_per_sm(int device) {
+  static std::atomic<unsigned long long> configured{0};
+  static int per_sm[64] = {0};
+  const unsigned long long bit = 1ull << (device & 63);
+  if (!(configured.load() & bit)) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, spmv_dia_kernel<NV, NDG, MT, GX, Epi>, kThreads, 0) !=
+            cudaSuccess ||
+        b < 1)
+      b = 1;
+    per_sm[device & 63] = std::min(b, 8);
+    configured.fetch_or(bit);
+  }
+  return per_sm[device & 63];
+}
+
+template <int NV, int NDG, class MT, class GX, class Epi>
+inline void launch_spmv_dn(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
+                           int slot) {
+  const long long need = ((long long)A.n + kThreads - 1) / kThreads;
+  const long long wave = (long long)ctx->num_sms * spmv_dia_ctas_per_sm<NV, NDG, MT, GX, Epi>(ctx->device);
+  const int grid = (int)std::max<long long>(1, std::min(need, wave));
+  launch_k(ctx, spmv_dia_kernel<NV, NDG, MT, GX, Epi>, dim3(grid), dim3(kThreads), 0, dview<MT>(A), g0, g1, epi,
+           stop, red_of(ctx, slot));
+}
+
+// SpMV over the diagonal copy: one thread per row, one resident wave of CTAs;
+// 5 and 7 diagonals (2-D and 3-D stencils) compiled for their count.
+template <int NV, class MT, class GX, class Epi>
+inline void launch_spmv_d(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi_in, Stop stop,
+                          int slot) {
+  with_rank_sums(ctx, epi_in, stop, [&](const auto &epi) {
+    using E = std::decay_t<decltype(epi)>;
+    if (A.dia_nd == 7)
+      launch_spmv_dn<NV, 7, MT, GX, E>(ctx, A, g0, g1, epi, stop, slot);
+    else if (A.dia_nd == 5)
+      launch_spmv_dn<NV, 5, MT, GX, E>(ctx, A, g0, g1, epi, stop, slot);
+    else
+      launch_spmv_dn<NV, 0, MT, GX, E>(ctx, A, g0, g1, epi, stop, slot);
+  });
+}
+
 template <int NV, class MT, class IT, class GX, class Epi>
 inline void launch_spmv_k(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
                           int slot) {
@@ -297,11 +369,14 @@ inline void launch_spmv_i(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &
   });
 }
 
-// 16-bit column offsets when the matrix has them, else int32 columns.
+// The diagonal copy when the matrix has one for these values, else CSR with
+// 16-bit column offsets when it has them, else CSR with int32 columns.
 template <int NV, class MT, class GX, class Epi>
 inline void launch_spmv_g(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &g1, const Epi &epi, Stop stop,
                           int slot = 0) {
-  if (A.col16)
+  if (A.dia_nd && dia_values_of<MT>(A))
+    launch_spmv_d<NV, MT, GX, Epi>(ctx, A, g0, g1, epi, stop, slot);
+  else if (A.col16)
     launch_spmv_i<NV, MT, short, GX, Epi>(ctx, A, g0, g1, epi, stop, slot);
   else
     launch_spmv_i<NV, MT, int, GX, Epi>(ctx, A, g0, g1, epi, stop, slot);

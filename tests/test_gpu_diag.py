@@ -1,0 +1,125 @@
+"""GPU: the diagonal copy of stencil matrices.
+
+A matrix whose rows hold their columns at no more than 8 distinct offsets
+from the row, in increasing column order, with the diagonals at least 3/4
+full, keeps a diagonal copy that the SpMV reads instead of CSR (no column
+indices). A row summed diagonal by diagonal is summed in its CSR order, so
+the SpMV must equal the reference's (the oracle's) bit for bit in FP64, equal
+the CSR kernel's bit for bit in FP32 and BF16, and every method must give the
+same history and solution bit for bit on either layout. Matrices that do not
+qualify keep CSR only and give the oracle's SpMV.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from solver_cpp_b200.matrices import CSR, config_problem
+
+pytestmark = pytest.mark.gpu
+
+STENCILS = [("poisson2d", 40, 5), ("poisson3d", 12, 7), ("convdiff3d", 12, 7), ("varcoef3d", 12, 7),
+            ("varcoef2d", 40, 5), ("convdiff2d", 40, 5)]
+
+
+def _csr(M):
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    return CSR(M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data.astype(np.float64))
+
+
+@pytest.mark.parametrize("prob,g,nd", STENCILS)
+def test_stencils_get_a_diagonal_copy(ks, ctx, prob, g, nd):
+    A, _, _ = config_problem(prob, g)
+    info = ctx.matrix(A, transpose=True).info()
+    assert info["diagonals"] == nd and info["t_diagonals"] == nd
+    assert ctx.matrix(A, transpose=True, diag=False).info()["diagonals"] == 0
+
+
+@pytest.mark.parametrize("prob,g,nd", STENCILS)
+def test_diagonal_spmv_is_bitwise(ks, ctx, oracle, prob, g, nd):
+    A, _, _ = config_problem(prob, g)
+    P = oracle.Problem(A)
+    x = np.random.default_rng(11).standard_normal(A.n)
+    D = ctx.matrix(A, transpose=True, fp32=True, bf16=True)
+    S = ctx.matrix(A, transpose=True, fp32=True, bf16=True, diag=False)
+    X, Y = ctx.vector(x), ctx.vector(n=A.n)
+    for trans in (False, True):
+        ks.spmv(D, X, Y, trans=trans)
+        assert np.array_equal(Y.numpy(), oracle.spmv(P, x, transpose=trans))
+    X32 = ctx.vector(x.astype(np.float32), dtype=ks.FP32)
+    Yd, Ys = ctx.vector(n=A.n, dtype=ks.FP32), ctx.vector(n=A.n, dtype=ks.FP32)
+    for vals in (ks.FP32, ks.BF16):
+        ks.spmv(D, X32, Yd, values=vals)
+        ks.spmv(S, X32, Ys, values=vals)
+        assert np.array_equal(Yd.numpy(), Ys.numpy()), vals
+
+
+def _nine_point(g):
+    T = sp.diags([-1.0, 2.5, -1.0], [-1, 0, 1], shape=(g, g))
+    return sp.kron(T, T) + sp.identity(g * g)  # 9 diagonals
+
+
+def _unsorted(A):
+    """Same matrix with the first two entries of every row of >= 2 entries swapped."""
+    col, val = A.col.copy(), A.val.copy()
+    for i in range(A.n):
+        j = A.ptr[i]
+        if A.ptr[i + 1] - j >= 2:
+            col[j], col[j + 1] = col[j + 1], col[j]
+            val[j], val[j + 1] = val[j + 1], val[j]
+    return CSR(A.ptr.copy(), col, val)
+
+
+def _sparse_far_diagonal(n):
+    M = sp.lil_matrix((n, n))
+    M.setdiag(4.0)
+    for i in range(0, n - 700, 97):  # a few entries far off the diagonal: two diagonals, half empty
+        M[i, i + 700] = -1.0
+    return M.tocsr()
+
+
+@pytest.mark.parametrize("case", ["nine_point", "unsorted", "random", "half_empty"])
+def test_non_stencils_keep_csr(ks, ctx, oracle, case):
+    if case == "nine_point":
+        A = _csr(_nine_point(30))
+    elif case == "unsorted":
+        A = _unsorted(config_problem("poisson2d", 30)[0])
+    elif case == "random":
+        rng = np.random.default_rng(4)
+        R = sp.random(900, 900, density=0.01, random_state=rng, format="csr") + 10 * sp.identity(900)
+        A = _csr(R)
+    else:
+        A = _csr(_sparse_far_diagonal(2000))
+    M = ctx.matrix(A)
+    assert M.info()["diagonals"] == 0
+    x = np.random.default_rng(5).standard_normal(A.n)
+    X, Y = ctx.vector(x), ctx.vector(n=A.n)
+    ks.spmv(M, X, Y)
+    assert np.array_equal(Y.numpy(), oracle.spmv(oracle.Problem(A), x))
+
+
+SOLVES = [
+    ("poisson3d", "CG", "NONE", {"cluster_solve": 1}),
+    ("poisson3d", "CR", "NONE", {}),
+    ("convdiff3d", "BICG", "NONE", {}),
+    ("convdiff3d", "GMRES", "NONE", {"R": 10}),
+    ("convdiff3d", "GCR", "NONE", {"R": 5}),
+    ("poisson3d", "KSKIPCG", "NONE", {"K": 2}),
+    ("convdiff3d", "KSKIPBICG", "NONE", {"K": 2}),
+    ("varcoef3d", "VPCG", "CG", {"l": 20, "e": 1e-30, "inner_precision": "fp32"}),
+    ("varcoef3d", "VPCG", "CG", {"l": 20, "e": 1e-30, "inner_precision": "bf16"}),
+    ("varcoef3d", "VPGMRES", "CG", {"R": 20, "l": 10, "e": 1e-30, "inner_precision": "fp32"}),
+]
+
+
+@pytest.mark.parametrize("prob,outer,inner,kw", SOLVES)
+def test_solves_identical_on_both_layouts(ks, ctx, prob, outer, inner, kw):
+    A, b, _ = config_problem(prob, 16)
+    res = []
+    for diag in (True, False):
+        M = ctx.matrix(A, transpose=True, fp32=True, bf16=True, diag=diag)
+        assert (M.info()["diagonals"] > 0) == diag
+        res.append(ks.solve(ctx, M, outer, b, inner=inner, E=1e-10, L=3000, **kw))
+    d, c = res
+    assert d.status == c.status and d.loop == c.loop
+    assert np.array_equal(d.hist_err, c.hist_err) and np.array_equal(d.x, c.x)
