@@ -413,9 +413,12 @@ inline int dir_ring(const Params &sp) {
   return (int)std::max<long long>(1, std::min<long long>(kDirRing, sp.maxloop));
 }
 
-// Direction slots a method allocates: the ring, or the single in-place p.
+// Direction slots a method allocates: the ring, or the single in-place p
+// (two for CG and BiCG, whose SpMV may form the next direction from the
+// previous one while writing it: run_cg, run_bicg; they use the second only
+// then).
 inline int dir_slots(int method, const Params &sp, long long n, size_t elem, size_t l2) {
-  return defer_x(method, sp, n, elem, l2) ? dir_ring(sp) : 1;
+  return defer_x(method, sp, n, elem, l2) ? dir_ring(sp) : (method == KS_CG || method == KS_BICG ? 2 : 1);
 }
 
 template <class VT>
@@ -603,7 +606,10 @@ struct ChunkGraph {
 };
 
 // Issues iterations 1..maxloop: body(L) queues iteration L. `fixed`: every
-// iteration queues the same kernels with the same arguments.
+// iteration after the first queues the same kernels, with arguments that
+// repeat with a period dividing kGraphChunk (CG alternates two direction
+// slots), so a chunk captured at iteration L replays as iterations
+// L + kGraphChunk, L + 2 kGraphChunk, ...
 template <class VT, class F>
 inline void run_iterations(const Env<VT> &E, bool fixed, F &&body) {
   Poller P{E.ctx, E.hflag, E.lookahead};
@@ -616,7 +622,7 @@ inline void run_iterations(const Env<VT> &E, bool fixed, F &&body) {
     }
     ChunkGraph G{E.ctx};
     if (G.capture([&] {
-          for (int j = 0; j < kGraphChunk; j++) body(L);
+          for (int j = 0; j < kGraphChunk; j++) body(L + j);
         })) {
       Poller PC{E.ctx, E.hflag, 2};  // lookahead in chunks
       for (; L <= E.sp.maxloop; L += kGraphChunk) {
@@ -632,11 +638,73 @@ inline void run_iterations(const Env<VT> &E, bool fixed, F &&body) {
   }
 }
 
-// cg::solve, three kernels per iteration with the x update deferred to the
-// direction ring. (Forming the next direction inside the SpMV's gather
-// instead of the separate update was measured slower on B200: gathering two
-// vectors per nonzero cost 15 us per SpMV at 128^3, the update kernel it
-// removes 8 us.)
+// SpMV input formed on the fly: the CG direction p_L[c] = beta p_{L-1}[c] +
+// r_L[c], with the direction update's operations (XpbyToOp), so every value
+// read equals the one the update would have stored, bit for bit.
+template <class VT>
+struct GDir {
+  const VT *__restrict__ pold;
+  const VT *__restrict__ r;
+  const double *beta;
+  VT b;
+  __device__ __forceinline__ GDir prep() const {
+    GDir g = *this;
+    g.b = (VT)rd(beta);
+    return g;
+  }
+  template <class AT>
+  __device__ __forceinline__ AT get(int c) const {
+    return (AT)add_rn(mul_rn(b, __ldg(pold + c)), __ldg(r + c));
+  }
+};
+
+// q = A p with p formed in the SpMV's reads (GDir): the row's own p_L is
+// stored for the x update and the next iteration; (p,q) -> alpha (CgMvEpi).
+template <class VT>
+struct CgMvDirEpi {
+  using acc_t = VT;
+  const VT *pold;
+  const VT *r;
+  VT *p;
+  VT *q;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    const VT b = (VT)rd(&st->k.s[S_BETA]);
+    const VT pi = add_rn(mul_rn(b, pold[i]), r[i]);
+    p[i] = pi;
+    q[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(pi), widen(v)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], s[0]);
+  }
+};
+
+// SpMV with its input read through a gather GX (mv: a plain vector).
+template <class VT, class GX, class Epi>
+inline void mv_g(const Env<VT> &E, const CsrDev &M, const GX &gx, const Epi &epi) {
+  if constexpr (std::is_same<VT, double>::value) {
+    launch_spmv_g<1, double, GX, Epi>(E.ctx, M, gx, gx, epi, E.stop());
+  } else {
+    if (E.mvals == KS_BF16)
+      launch_spmv_g<1, __nv_bfloat16, GX, Epi>(E.ctx, M, gx, gx, epi, E.stop());
+    else
+      launch_spmv_g<1, float, GX, Epi>(E.ctx, M, gx, gx, epi, E.stop());
+  }
+}
+
+// cg::solve, with the x update deferred to the direction ring where the
+// vectors do not fit in L2. On systems of up to kGraphMaxN rows whose SpMV
+// reads a diagonal copy, the SpMV forms the direction p = beta p + r itself
+// from the previous direction and r (GDir) and stores its own rows of p: two
+// kernels per iteration instead of three, which pays where the iteration is
+// bound by its kernel boundaries (512^2 adjoint CG workload on B200: 0.198 ->
+// 0.168 s). On larger systems reading two vectors per diagonal costs more
+// than the update kernel it removes (160^3 FP32 inner CG: 3.4 us more per
+// iteration), and with CSR the gather of two vectors per nonzero does too
+// (128^3: 15 us more per SpMV against 8 us saved), so they keep the separate
+// direction update.
 // Small systems (up to kResMaxRows rows, one GPU, FP64; ks_params.cluster_solve
 // 0): the whole solve as one launch of one thread-block cluster
 // (ks_resident.cuh). Returns false,
@@ -669,21 +737,30 @@ ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take();
   const bool defer = defer_x(E, KS_CG);
-  const int D = defer ? dir_ring(E.sp) : 1;  // D = 1: p updated in place
+  const bool fused = E.A->dia_nd > 0 && !E.comm && E.n <= kGraphMaxN && (!defer || dir_ring(E.sp) >= 2);
+  // without the ring: p in place, or two alternating slots when the SpMV forms
+  // p (a second slot would crowd the vectors of a large system out of L2)
+  const int D = defer ? dir_ring(E.sp) : (fused ? 2 : 1);
   DirRing<VT> R{W.take(D), E.ld, D, dws};
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, R.slot(1), nullptr, nullptr, E.st, START_CG});
   run_iterations(E, !defer, [&](long long L) {
     VT *p = R.slot(L);
-    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
+    if (fused) {
+      // iteration 1: beta = 0 and p_0 := r, so p_1 = 0 r + r = r (r finite)
+      const VT *pold = L == 1 ? r : R.slot(L + D - 1);
+      mv_g(E, *E.A, GDir<VT>{pold, r, &E.st->k.s[S_BETA], (VT)0}, CgMvDirEpi<VT>{pold, r, p, q, E.st});
+    } else {
+      mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, q, E.st});
+    }
     if (defer) {
       vec(E, RUpdOp<VT>{r, q, E.st, 0, R.aslot(L)});
       ring_step(E, R, x, L);
     } else {
       vec(E, XrUpdOp<VT>{x, r, p, q, E.st, 0});
     }
-    vec(E, XpbyToOp<VT>{p, r, R.slot(L + 1), &E.st->k.s[S_BETA]});
+    if (!fused) vec(E, XpbyToOp<VT>{p, r, R.slot(L + 1), &E.st->k.s[S_BETA]});
   });
   if (defer) ring_final(E, R, x);
   return KS_OK;
@@ -822,12 +899,43 @@ struct Xpby2PlainOp {
   __device__ void finish(const double (&)[1]) const {}
 };
 
+// Ap with p formed in the SpMV's reads (GDir, as in CG): the row's own p_L
+// is stored, and p*_L = beta p*_{L-1} + r*_L formed and stored in place (only
+// row i reads entry i here); (p*, Ap) -> alpha (CgMvEpi on p*).
+template <class VT>
+struct BicgMvDirEpi {
+  using acc_t = VT;
+  const VT *pold;
+  const VT *r;
+  VT *p;
+  VT *ps;
+  const VT *rs;
+  VT *ap;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    const VT b = (VT)rd(&st->k.s[S_BETA]);
+    p[i] = add_rn(mul_rn(b, pold[i]), r[i]);
+    const VT psi = add_rn(mul_rn(b, ps[i]), rs[i]);
+    ps[i] = psi;
+    ap[i] = v;
+    acc[0] = add_rn(acc[0], mul_rn(widen(psi), widen(v)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], s[0]);
+  }
+};
+
+// bicg::solve. On systems of up to kGraphMaxN rows with a diagonal copy the
+// A-SpMV forms both directions (as run_cg does for p), and the separate
+// direction update is gone: three kernels per iteration instead of four.
 template <class VT>
 ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *rs = W.take(), *ps = W.take(), *mvv = W.take();
   const bool defer = defer_x(E, KS_BICG);
-  const int D = defer ? dir_ring(E.sp) : 1;
+  const bool fused = E.A->dia_nd > 0 && !E.comm && E.n <= kGraphMaxN && (!defer || dir_ring(E.sp) >= 2);
+  const int D = defer ? dir_ring(E.sp) : (fused ? 2 : 1);  // as in run_cg
   DirRing<VT> R{W.take(D), E.ld, D, dws};
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
@@ -835,7 +943,14 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   start_from_zero(E, StartEpi<VT>{b, r, rs, R.slot(1), ps, E.st, START_CG});
   run_iterations(E, !defer, [&](long long L) {
     VT *p = R.slot(L);
-    mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
+    if (fused) {
+      // iteration 1: beta = 0, p_0 := r and p*_0 = r: p_1 = r, p*_1 = r* (r finite)
+      const VT *pold = L == 1 ? r : R.slot(L + D - 1);
+      mv_g(E, *E.A, GDir<VT>{pold, r, &E.st->k.s[S_BETA], (VT)0},
+           BicgMvDirEpi<VT>{pold, r, p, ps, rs, mvv, E.st});
+    } else {
+      mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
+    }
     if (defer) {
       vec(E, RUpdOp<VT>{r, mvv, E.st, 1, R.aslot(L)});
       ring_step(E, R, x, L);
@@ -843,7 +958,7 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
       vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
     }
     mv(E, *E.AT, (const VT *)ps, BicgMvTEpi<VT>{rs, r, E.st});
-    vec(E, Xpby2PlainOp<VT>{p, r, R.slot(L + 1), ps, rs, &E.st->k.s[S_BETA]});
+    if (!fused) vec(E, Xpby2PlainOp<VT>{p, r, R.slot(L + 1), ps, rs, &E.st->k.s[S_BETA]});
   });
   if (defer) ring_final(E, R, x);
   return KS_OK;
