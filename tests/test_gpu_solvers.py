@@ -109,17 +109,22 @@ def test_device_vectors_path(ks, ctx):
     assert r.converged and np.array_equal(X.numpy(), h.x)
 
 
+@pytest.mark.parametrize("diag", [True, False])
 @pytest.mark.parametrize("name", ["CG", "CR", "BICG"])
-def test_deferred_solution_update_at_ring_boundaries(ks, ctx, oracle, name):
+def test_deferred_solution_update_at_ring_boundaries(ks, ctx, oracle, name, diag):
     """CG, CR and BiCG apply x += alpha p either every iteration or through a
     ring of 32 directions (x_update 1 / 2; 0 picks by L2 fit). Stopping
     before, at and after a full ring (and at maxloop = the ring size) must
-    leave the same x bit for bit, and the x of the per-iteration update."""
+    leave the same x bit for bit, and the x of the per-iteration update. On
+    the diagonal copy (this size) CG and BiCG form the direction inside the
+    SpMV, on CSR they run a separate direction update. CG runs the
+    kernel-per-step engine here (cluster_solve 1)."""
     A, b, _ = config_problem("convdiff3d" if name == "BICG" else "poisson3d", 24)
-    M = _mat(ctx, A)
+    M = ctx.matrix(A, transpose=True, diag=diag)
+    kw = {"cluster_solve": 1} if name == "CG" else {}
     for L in (1, 5, 31, 32, 33, 64, 65, 90):
-        r1 = ks.solve(ctx, M, name, b, L=L, E=1e-30, x_update=1)
-        r2 = ks.solve(ctx, M, name, b, L=L, E=1e-30, x_update=2)
+        r1 = ks.solve(ctx, M, name, b, L=L, E=1e-30, x_update=1, **kw)
+        r2 = ks.solve(ctx, M, name, b, L=L, E=1e-30, x_update=2, **kw)
         assert np.array_equal(r1.x, r2.x) and np.array_equal(r1.hist_err, r2.hist_err), (name, L)
         o = oracle.solve(A, b, name, L=L, E=1e-30)
         assert r2.loop == o["loop"] and r2.status == o["status"] == 2, (name, L)
