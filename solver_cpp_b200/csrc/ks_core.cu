@@ -345,18 +345,21 @@ static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long lo
   std::sort(o.off, o.off + o.nd);
   if (o.nd < 1 || 4 * A.nnz < 3LL * o.nd * A.n) return KS_OK;  // diagonals less than 3/4 full
   const long long len = (long long)o.nd * A.n;
-  KS_CUDA(ctx, cudaMalloc(&A.dia_val, sizeof(double) * (size_t)len));
-  KS_CUDA(ctx, cudaMalloc(&A.dia_mask, (size_t)A.n));
+  // The copy is an optimisation: if the device cannot hold it, CSR serves.
+  auto got = [&](cudaError_t a) {
+    if (a == cudaSuccess) return true;
+    (void)cudaGetLastError();
+    free_dia(A);
+    return false;
+  };
+  if (!got(cudaMalloc(&A.dia_val, sizeof(double) * (size_t)len)) || !got(cudaMalloc(&A.dia_mask, (size_t)A.n)))
+    return KS_OK;
+  if ((flags & KS_MAT_FP32) && !got(cudaMalloc(&A.dia_val32, sizeof(float) * (size_t)len))) return KS_OK;
+  if ((flags & KS_MAT_BF16) && !got(cudaMalloc(&A.dia_val16, sizeof(__nv_bfloat16) * (size_t)len))) return KS_OK;
   KS_CUDA(ctx, cudaMemsetAsync(A.dia_val, 0, sizeof(double) * (size_t)len, ctx->stream));
   k_dia_fill<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.val, A.n, o, A.dia_val, A.dia_mask);
-  if (flags & KS_MAT_FP32) {
-    KS_CUDA(ctx, cudaMalloc(&A.dia_val32, sizeof(float) * (size_t)len));
-    k_to_f32<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val32, len);
-  }
-  if (flags & KS_MAT_BF16) {
-    KS_CUDA(ctx, cudaMalloc(&A.dia_val16, sizeof(__nv_bfloat16) * (size_t)len));
-    k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val16, len);
-  }
+  if (A.dia_val32) k_to_f32<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val32, len);
+  if (A.dia_val16) k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val16, len);
   KS_CUDA(ctx, cudaGetLastError());
   A.dia_nd = o.nd;
   for (int k = 0; k < kMaxDiag; k++) A.dia_off[k] = k < o.nd ? o.off[k] : 0;
