@@ -1,6 +1,6 @@
 // SpMV over the diagonal copy of a stencil-like matrix (sm_100a).
 //
-// The configurations' matrices (5- and 7-point stencils, upwind
+// Matrices of structured grids (5- and 7-point stencils, upwind
 // convection-diffusion) hold every row's columns at a handful of fixed
 // offsets from the row. Stored diagonal-major, the SpMV needs no column
 // indices or row offsets at all: per nonzero only its value (plus one mask
