@@ -233,10 +233,11 @@ typedef struct {
   int32_t x_update;        /* CG, CR, BiCG: 0 auto, 1 x += alpha p every
                               iteration, 2 deferred through a ring of 32
                               directions (same x bit for bit)              */
-  int32_t cluster_solve;   /* CG on at most 32768 rows (one GPU): 0 auto, the
-                              whole solve in one launch of one thread-block
-                              cluster where the device can hold it; 1 never
-                              (one kernel per step, as for larger systems) */
+  int32_t cluster_solve;   /* CG and BiCG on at most 32768 rows (one GPU): 0
+                              auto, the whole solve in one launch of one
+                              thread-block cluster where the device can hold
+                              it; 1 never (one kernel per step, as for larger
+                              systems)                                      */
 } ks_params;
 
 typedef struct {

@@ -112,9 +112,12 @@ class Matrix:
         self.flags = flags
 
     def close(self):
-        if self.handle:
+        # A matrix outliving its context (e.g. held by a traceback past the
+        # context's close) has nothing left to free: the context released the
+        # device with it, and the C call would read the freed context.
+        if self.handle and self.ctx.handle:
             lib().ks_mat_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -182,9 +185,9 @@ class Vector:
         return lib().ks_vec_device_ptr(self.handle)
 
     def close(self):
-        if self.handle:
+        if self.handle and self.ctx.handle:  # as Matrix.close
             lib().ks_vec_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -456,9 +459,9 @@ class Comm:
         return [cls(C.c_void_p(out[q]), ctxs[q]) for q in range(P)]
 
     def close(self):
-        if self.handle:
+        if self.handle and self.ctx.handle:  # as Matrix.close
             lib().ks_comm_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
 
 class SplitMatrix(Matrix):

@@ -1,4 +1,4 @@
-// Small systems solved inside one thread-block cluster.
+// Small systems solved inside one thread-block cluster (CG, BiCG).
 //
 // Up to 32K rows the kernels of a CG iteration (cg.cpp:184-240) each take a
 // few microseconds and the loop is bound by its kernel boundaries (launch,
@@ -127,14 +127,16 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-// Exchange area of one CTA for the cluster reductions: every CTA's block sum
+constexpr int kResMaxSums = 2;  // values one cluster reduction carries
+
+// Exchange area of one CTA for the cluster reductions: every CTA's block sums
 // (two slots, used by alternate reductions), one mbarrier per slot, and the
 // outcome of the wait for the CTA.
 struct ResXchg {
-  double red[2][kResMaxCluster];
+  double red[2][kResMaxSums][kResMaxCluster];
   uint64_t bar[2];
   int ok;
-  double tot;
+  double tot[kResMaxSums];
 };
 
 __device__ __forceinline__ void xchg_init(cgx::cluster_group cl, ResXchg *xg) {
@@ -158,53 +160,67 @@ __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, uint32_t pa
   return ok != 0;
 }
 
-// Sum number m (0, 1, 2, ...) over the cluster of one value per thread.
-// Warp 0 of each CTA adds its CTA's warp sums and stores the block sum into
-// slot m % 2 of every CTA's exchange area with st.async, which completes 8
-// bytes on that CTA's mbarrier of the slot (a release at cluster scope, so the
-// CTA's earlier shared-memory writes, ordered before it by __syncthreads, are
-// visible to the receiver once its wait returns). Every thread then runs
-// `shadow` (work that needs neither the sum nor other CTAs' data) while the
-// block sums travel; thread 0 expects 8 C bytes per use of the barrier and
-// waits for them (bounded by kWaitLimitNs) and adds the C block sums in rank
-// order, the same on every CTA. Returns false in every thread of the CTA if
-// the wait ran out.
+// Sums number m (0, 1, 2, ...) over the cluster of NV values per thread.
+// Warp 0 of each CTA adds its CTA's warp sums and stores the NV block sums
+// into slot m % 2 of every CTA's exchange area with st.async, each store
+// completing 8 bytes on that CTA's mbarrier of the slot (a release at cluster
+// scope, so the CTA's earlier shared-memory writes, ordered before it by
+// __syncthreads, are visible to the receiver once its wait returns). Every
+// thread then runs `shadow` (work that needs neither the sums nor other CTAs'
+// data) while the block sums travel; thread 0 expects 8 NV C bytes per use of
+// the barrier and waits for them (bounded by kWaitLimitNs) and adds the C
+// block sums of each value in rank order, the same on every CTA. warp_s holds
+// NV x 32 doubles. Returns false in every thread of the CTA if the wait ran
+// out.
 //
-// Slot reuse: a CTA sends sum m + 2 only after completing sum m + 1, which
-// needs every CTA's block sum m + 1, which each CTA computes only after it
-// has read sum m; so sum m + 2 never lands on a slot or barrier phase still
+// Slot reuse: a CTA sends sums m + 2 only after completing sums m + 1, which
+// need every CTA's block sums m + 1, which each CTA computes only after it
+// has read sums m; so sums m + 2 never land on a slot or barrier phase still
 // in use. (A block sum may land before the receiver's own expect for that
 // phase; the transaction count then runs negative until it does.)
-template <class F>
-__device__ __forceinline__ bool cluster_sum(double v, double *warp_s, ResXchg *xg, int m, int C, int rank,
-                                            double *out, F &&shadow) {
+template <int NV, class F>
+__device__ __forceinline__ bool cluster_sums(double (&v)[NV], double *warp_s, ResXchg *xg, int m, int C, int rank,
+                                             F &&shadow) {
+  static_assert(NV >= 1 && NV <= kResMaxSums, "values per cluster reduction");
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
   const int s = m & 1;
   const uint32_t parity = (uint32_t)((m >> 1) & 1);
-  v = group_sum<32>(v);
-  if (lane == 0) warp_s[w] = v;
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    v[k] = group_sum<32>(v[k]);
+    if (lane == 0) warp_s[k * 32 + w] = v[k];
+  }
   __syncthreads();
   if (w == 0) {
     // every group of 8 or 16 lanes adds the same warp sums, so every lane that
-    // sends holds the same block sum
-    double t;
-    if (nw > 16) {
-      t = group_sum<32>(warp_s[lane]);
-    } else if (nw > 8) {
-      const int g = lane & 15;
-      t = group_sum<16>(g < nw ? warp_s[g] : 0.0);
-    } else {
-      const int g = lane & 7;
-      t = group_sum<8>(g < nw ? warp_s[g] : 0.0);
+    // sends holds the same block sums
+    double t[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      if (nw > 16) {
+        t[k] = group_sum<32>(warp_s[k * 32 + lane]);
+      } else if (nw > 8) {
+        const int g = lane & 15;
+        t[k] = group_sum<16>(g < nw ? warp_s[k * 32 + g] : 0.0);
+      } else {
+        const int g = lane & 7;
+        t[k] = group_sum<8>(g < nw ? warp_s[k * 32 + g] : 0.0);
+      }
     }
-    if (lane == 0) mbar_expect_tx(&xg->bar[s], 8u * (uint32_t)C);
+    if (lane == 0) mbar_expect_tx(&xg->bar[s], 8u * (uint32_t)(NV * C));
     if (lane < C) {
-      uint32_t ra, rb;
-      asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(smem_u32(&xg->red[s][rank])), "r"(lane));
+      uint32_t rb;
       asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(smem_u32(&xg->bar[s])), "r"(lane));
-      asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(ra),
-                   "l"(__double_as_longlong(t)), "r"(rb)
-                   : "memory");
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        uint32_t ra;
+        asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                     : "=r"(ra)
+                     : "r"(smem_u32(&xg->red[s][k][rank])), "r"(lane));
+        asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];" ::"r"(ra),
+                     "l"(__double_as_longlong(t[k])), "r"(rb)
+                     : "memory");
+      }
     }
   }
   shadow();
@@ -217,14 +233,28 @@ __device__ __forceinline__ bool cluster_sum(double v, double *warp_s, ResXchg *x
     }
     xg->ok = ok ? 1 : 0;
     if (ok) {
-      double u = 0.0;
-      for (int c = 0; c < C; c++) u += xg->red[s][c];  // rank order
-      xg->tot = u;
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        double u = 0.0;
+        for (int c = 0; c < C; c++) u += xg->red[s][k][c];  // rank order
+        xg->tot[k] = u;
+      }
     }
   }
   __syncthreads();
-  *out = xg->tot;
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = xg->tot[k];
   return xg->ok != 0;
+}
+
+// One value: the sum in *out.
+template <class F>
+__device__ __forceinline__ bool cluster_sum(double v, double *warp_s, ResXchg *xg, int m, int C, int rank,
+                                            double *out, F &&shadow) {
+  double a[1] = {v};
+  const bool ok = cluster_sums<1>(a, warp_s, xg, m, C, rank, shadow);
+  *out = a[0];
+  return ok;
 }
 
 __device__ __forceinline__ void no_shadow() {}
@@ -260,7 +290,7 @@ template <int R, bool I16>
 __global__ void __launch_bounds__(kResThreads, 1) k_cg_resident(const ResCgArgs a) {
   cgx::cluster_group cl = cgx::this_cluster();
   extern __shared__ double dyn_s[];  // slices of x, r, p (two buffers)
-  __shared__ double warp_s[32];
+  __shared__ double warp_s[kResMaxSums * 32];
   __shared__ ResXchg xg;
   __shared__ double hist_e[kResHist];
   __shared__ long long hist_i[kResHist];
@@ -431,6 +461,168 @@ __global__ void __launch_bounds__(kResThreads, 1) k_cg_resident(const ResCgArgs 
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
+struct ResBicgArgs {
+  const int *ptr, *col;  // A
+  const short *col16;
+  const double *val;
+  const int *tptr, *tcol;  // A^T
+  const short *tcol16;
+  const double *tval;
+  const double *b;
+  double *x;
+  DevState *st;  // reset by InitOp before the launch
+  int *err;      // set if a bounded wait ran out
+  int n;
+  int shift;  // rows per CTA = 2^shift
+};
+
+// Row i of M times the direction formed on the fly, beta d_old + v, from the
+// owners' slices (this CTA's shared memory, or another CTA's through the
+// cluster); the direction update's operations, the row's CSR order.
+template <bool I16>
+__device__ __forceinline__ double row_times_dir(cgx::cluster_group cl, const int *ptr, const int *col,
+                                                const short *col16, const double *val, int i, int shift,
+                                                int rank, double beta, const double *d_old, const double *v_s) {
+  const int mask = (1 << shift) - 1;
+  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
+  double s = 0.0;
+#pragma unroll 4
+  for (int j = j0; j < j1; j++) {
+    const int c = I16 ? i + (int)__ldg(col16 + j) : __ldg(col + j);
+    const int o = c >> shift, lc = c & mask;
+    const double *pp = d_old + lc, *vq = v_s + lc;
+    if (o != rank) {
+      pp = cl.map_shared_rank(pp, (unsigned)o);
+      vq = cl.map_shared_rank(vq, (unsigned)o);
+    }
+    s = add_rn(s, mul_rn(__ldg(val + j), add_rn(mul_rn(beta, *pp), *vq)));
+  }
+  return s;
+}
+
+// bicg::solve (bicg.cpp:162-277) from x = 0 to the stopping test, in one
+// launch (as k_cg_resident; x, r, r* and two buffers each of p and p* in
+// shared memory). Per iteration both SpMVs, q = A p and t = A^T p*, form
+// their directions in their reads from the published r and r*; then two
+// cluster reductions: (p*, q) -> alpha, with the stopping test of the
+// previous iteration in its shadow, and ((r,r), (r*,r)) after r -= alpha q,
+// r* -= alpha t, with x += alpha p in its shadow. The decisions come in the
+// kernel-per-step engine's order: the stopping test on (r,r), then beta =
+// (r*,r)/(r*,r)_old; when beta's division stops the method the test still
+// runs and its verdict wins, as there.
+template <int R, bool IA16, bool IT16>
+__global__ void __launch_bounds__(kResThreads, 1) k_bicg_resident(const ResBicgArgs a) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  extern __shared__ double dyn_s[];  // slices of x, r, r*, p (two), p* (two)
+  __shared__ double warp_s[kResMaxSums * 32];
+  __shared__ ResXchg xg;
+  __shared__ double hist_e[kResHist];
+  __shared__ long long hist_i[kResHist];
+  const int C = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
+  const int rp = 1 << a.shift;
+  double *x_s = dyn_s, *r_s = dyn_s + rp, *rs_s = dyn_s + 2 * rp;
+  double *p_s0 = dyn_s + 3 * rp, *p_s1 = dyn_s + 4 * rp, *ps_s0 = dyn_s + 5 * rp, *ps_s1 = dyn_s + 6 * rp;
+  const int T = blockDim.x;
+  const int r0 = rank << a.shift;
+  ResScal S{a.st, rank == 0 && threadIdx.x == 0, a.st->k.s[S_EPS], a.st->k.aux[A_MAXLOOP], hist_e, hist_i};
+  S.begin();
+  xchg_init(cl, &xg);
+  int m = 0;
+  bool ok = true;
+  double q[R], t[R];
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    const int li = threadIdx.x + k * T, i = r0 + li;
+    double ri = 0.0;
+    if (i < a.n) {
+      ri = sub_rn(a.b[i], 0.0);  // b - A*0 with x = 0; r* = r (bicg.cpp:181-183)
+      acc = add_rn(acc, mul_rn(ri, ri));
+    }
+    x_s[li] = 0.0;
+    r_s[li] = ri;
+    rs_s[li] = ri;
+    p_s0[li] = ri;  // p_0 := r_1, p*_0 := r*_1 with beta_0 = 0: p_1 = r_1, p*_1 = r*_1
+    ps_s0[li] = ri;
+    q[k] = t[k] = 0.0;
+  }
+  // |b|^2, (r,r) and (r*,r) are the same sum, r* and r being b
+  double rr = 0.0;
+  ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &rr, no_shadow);
+  const double bnorm = sqrt(rr);
+  if (S.writer) a.st->k.s[S_BNORM] = bnorm;
+  double rr_chk = rr;  // (r,r) of the pending stopping test
+  long long L = 1;
+  double beta = 0.0, alpha = 0.0;
+  while (ok) {
+    const double *p_old = (L & 1) ? p_s0 : p_s1, *ps_old = (L & 1) ? ps_s0 : ps_s1;
+    double *p_new = (L & 1) ? p_s1 : p_s0, *ps_new = (L & 1) ? ps_s1 : ps_s0;
+    // p = beta p + r, p* = beta p* + r*; q = A p, t = A^T p*; (p*, q) -> alpha
+    acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int li = threadIdx.x + k * T, i = r0 + li;
+      if (i < a.n) {
+        p_new[li] = add_rn(mul_rn(beta, p_old[li]), r_s[li]);
+        const double psk = add_rn(mul_rn(beta, ps_old[li]), rs_s[li]);
+        ps_new[li] = psk;
+        q[k] = row_times_dir<IA16>(cl, a.ptr, a.col, a.col16, a.val, i, a.shift, rank, beta, p_old, r_s);
+        t[k] = row_times_dir<IT16>(cl, a.tptr, a.tcol, a.tcol16, a.tval, i, a.shift, rank, beta, ps_old, rs_s);
+        acc = add_rn(acc, mul_rn(psk, q[k]));
+      }
+    }
+    double pq = 0.0;
+    if (!(ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &pq,
+                           [&] { S.check_top(L, sqrt(rr_chk) / bnorm); })))
+      break;
+    if (S.done != kRunning) break;  // iteration L does not run
+    alpha = S.rdiv(rr, pq);
+    if (S.done != kRunning) break;
+    // r -= alpha q; r* -= alpha t (published); (r,r), (r*,r); x += alpha p in the shadow
+    double sums[2] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int li = threadIdx.x + k * T, i = r0 + li;
+      if (i < a.n) {
+        const double rk = add_rn(mul_rn(-alpha, q[k]), r_s[li]);
+        const double rsk = add_rn(mul_rn(-alpha, t[k]), rs_s[li]);
+        r_s[li] = rk;
+        rs_s[li] = rsk;
+        sums[0] = add_rn(sums[0], mul_rn(rk, rk));
+        sums[1] = add_rn(sums[1], mul_rn(rsk, rk));
+      }
+    }
+    if (!(ok = cluster_sums<2>(sums, warp_s, &xg, m++, C, rank, [&] {
+#pragma unroll
+          for (int k = 0; k < R; k++) {
+            const int li = threadIdx.x + k * T, i = r0 + li;
+            if (i < a.n) x_s[li] = add_rn(mul_rn(alpha, p_new[li]), x_s[li]);
+          }
+        })))
+      break;
+    rr_chk = sums[0];
+    L++;
+    // the stopping test on (r,r) runs first in the engine; it is deferred to
+    // the next reduction's shadow here, so beta's division comes first, and
+    // when that stops the method the test runs at once (its verdict wins)
+    beta = S.rdiv(sums[1], rr);
+    rr = sums[1];
+    if (S.done != kRunning) {
+      S.check_top(L, sqrt(rr_chk) / bnorm);
+      break;
+    }
+  }
+  if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    const int li = threadIdx.x + k * T, i = r0 + li;
+    if (i < a.n) a.x[i] = x_s[li];
+  }
+  S.end();
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
 // ---------------------------------------------------------------- host side
 struct ResShape {
   int C = 0;      // CTAs (0: the system is too large)
@@ -492,6 +684,62 @@ inline cudaError_t res_cg_launch(const ResShape &sh, cudaStream_t s, const ResCg
     return cudaSuccess;
   }
   return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+template <int R, bool IA16, bool IT16>
+inline cudaError_t res_bicg_launch(const ResShape &sh, cudaStream_t s, const ResBicgArgs &a, bool probe_only,
+                                   bool *fits) {
+  auto kern = k_bicg_resident<R, IA16, IT16>;
+  const size_t smem = (7 * sizeof(double)) << sh.shift;  // x, r, r*, two p and two p* slices
+  if (sh.C > 8) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)sh.C);
+  cfg.blockDim = dim3((unsigned)sh.T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)sh.C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  if (probe_only) {
+    int clusters = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+    *fits = e == cudaSuccess && clusters >= 1;
+    if (e != cudaSuccess) (void)cudaGetLastError();
+    return cudaSuccess;
+  }
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+template <int R>
+inline cudaError_t res_bicg_r(const ResShape &sh, bool ia16, bool it16, cudaStream_t s, const ResBicgArgs &a,
+                              bool probe_only, bool *fits) {
+  if (ia16)
+    return it16 ? res_bicg_launch<R, true, true>(sh, s, a, probe_only, fits)
+                : res_bicg_launch<R, true, false>(sh, s, a, probe_only, fits);
+  return it16 ? res_bicg_launch<R, false, true>(sh, s, a, probe_only, fits)
+              : res_bicg_launch<R, false, false>(sh, s, a, probe_only, fits);
+}
+
+// As res_cg, for BiCG (columns of A and of A^T as int16 offsets or int32).
+inline cudaError_t res_bicg(const ResShape &sh, bool ia16, bool it16, cudaStream_t s, const ResBicgArgs &a,
+                            bool probe_only, bool *fits) {
+  switch (sh.R) {
+    case 1: return res_bicg_r<1>(sh, ia16, it16, s, a, probe_only, fits);
+    case 2: return res_bicg_r<2>(sh, ia16, it16, s, a, probe_only, fits);
+    case 4: return res_bicg_r<4>(sh, ia16, it16, s, a, probe_only, fits);
+  }
+  return cudaErrorInvalidValue;
 }
 
 // probe_only: sets *fits to whether one cluster of this shape can be resident

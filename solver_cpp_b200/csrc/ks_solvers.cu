@@ -926,11 +926,38 @@ struct BicgMvDirEpi {
   }
 };
 
+// BiCG on small systems as one thread-block-cluster launch (as
+// run_cg_resident).
+inline bool run_bicg_resident(const Env<double> &E, const double *b, double *x, ks_status *s) {
+  if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A->val || !E.AT || !E.AT->val)
+    return false;
+  const ResShape sh = resident_shape(E.n);
+  if (!sh.C) return false;
+  const CsrDev &A = *E.A, &T = *E.AT;
+  const ResBicgArgs a{A.ptr, A.col,  A.col16, A.val, T.ptr,         T.col,      T.col16,
+                      T.val, b,      x,       E.st,  E.ctx->d_err, (int)E.n, sh.shift};
+  bool fits = false;
+  const bool ia16 = A.col16 != nullptr, it16 = T.col16 != nullptr;
+  if (res_bicg(sh, ia16, it16, E.ctx->stream, a, true, &fits) != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  E.ctx->launches++;
+  const cudaError_t e = res_bicg(sh, ia16, it16, E.ctx->stream, a, false, nullptr);
+  *s = e == cudaSuccess ? KS_OK : cuda_fail(E.ctx, e, "cluster-resident BiCG launch");
+  return true;
+}
+
 // bicg::solve. On systems of up to kGraphMaxN rows with a diagonal copy the
 // A-SpMV forms both directions (as run_cg does for p), and the separate
 // direction update is gone: three kernels per iteration instead of four.
 template <class VT>
 ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
+  if constexpr (std::is_same<VT, double>::value) {
+    ks_status s = KS_OK;
+    if (run_bicg_resident(E, b, x, &s)) return s;
+  }
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *rs = W.take(), *ps = W.take(), *mvv = W.take();
   const bool defer = defer_x(E, KS_BICG);

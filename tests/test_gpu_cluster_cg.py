@@ -1,7 +1,7 @@
-"""GPU: CG on small systems as one thread-block-cluster launch.
+"""GPU: CG and BiCG on small systems as one thread-block-cluster launch.
 
-Up to 32768 rows (one GPU, FP64) CG runs as a single launch of one cluster
-of up to 16 CTAs (ks_params.cluster_solve 0, the default); cluster_solve 1
+Up to 32768 rows (one GPU, FP64) CG and BiCG run as a single launch of one
+cluster of up to 16 CTAs (ks_params.cluster_solve 0, the default); cluster_solve 1
 selects the kernel-per-step engine used for larger systems. Both paths do the
 same element-wise arithmetic and differ only in the order in which the dot
 products add their terms, so each must reproduce the reference's golden
@@ -97,3 +97,60 @@ def test_cluster_solve_rejects_bad_value(ks, ctx):
     with pytest.raises(ks.KrylovError) as e:
         ks.solve(ctx, ctx.matrix(A), "CG", b, cluster_solve=2)
     assert e.value.status == 5
+
+
+# ------------------------------------------------------------------ BiCG
+BICG_CASES = sorted(c for c, m in index().items() if m["outer"] == "BICG")
+
+
+@pytest.mark.parametrize("cluster_solve", [0, 1])
+@pytest.mark.parametrize("cid", BICG_CASES)
+def test_bicg_golden_history_on_both_paths(ks, ctx, cid, cluster_solve):
+    meta, g = load(cid)
+    A, b, _ = config_problem(meta["problem"], meta["grid"])
+    M = ctx.matrix(A, transpose=True)
+    r = ks.solve(ctx, M, "BICG", b, cluster_solve=cluster_solve, **meta["params"])
+    assert r.converged == meta["converged"]
+    check_history(r.hist_iter, r.hist_err, g["hist_iter"], g["hist_err"], g["envelope"], r.loop, meta["loop"],
+                  meta["loop_range"])
+    assert round(r.true_res_log10, 1) == pytest.approx(meta["true_res_log10"], abs=0.21)
+
+
+# BiCG departs from itself under a change of summation order much sooner than
+# CG. On the small systems both paths are held to the oracle's envelope; on
+# the larger ones (the oracle's own chunked sums differ by 1e-4 within the
+# first half of the 128^2 history and its iteration counts spread over
+# 428-463; at 182^2 the engine converged in 608 iterations, the oracle in 693)
+# to convergence with a true residual near the oracle's (BiCG stops on its
+# recurrence residual, and the true one lies above it by as much in the
+# oracle: 1.2e-11 at 128^2).
+BICG_SHAPES = [("convdiff2d", 1, True), ("convdiff2d", 5, True), ("convdiff2d", 31, True),
+               ("convdiff2d", 45, True), ("convdiff2d", 128, False), ("convdiff2d", 181, False),
+               ("convdiff3d", 32, False), ("convdiff2d", 182, False)]
+
+
+@pytest.mark.parametrize("prob,g,strict", BICG_SHAPES)
+def test_bicg_cluster_and_engine_against_oracle(ks, ctx, oracle, prob, g, strict):
+    A, b, _ = config_problem(prob, g)
+    M = ctx.matrix(A, transpose=True)
+    o, env, lr = oracle_envelope(oracle, A, b, "BICG", E=1e-12, L=5000)
+    o_true = np.linalg.norm(b - A.to_scipy() @ o["x"]) / np.linalg.norm(b)
+    for cs in (0, 1):
+        r = ks.solve(ctx, M, "BICG", b, E=1e-12, L=5000, cluster_solve=cs)
+        assert r.status == o["status"] == 0, (cs, r.status)
+        if strict:
+            check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
+        assert r.true_rel_res < 3 * max(o_true, 1e-12), (cs, r.true_rel_res, o_true)
+
+
+@pytest.mark.parametrize("L", [0, 1, 7, 255, 256, 257])
+def test_bicg_cluster_maxloop_and_history_flushes(ks, ctx, oracle, L):
+    A, b, _ = config_problem("convdiff2d", 40)
+    M = ctx.matrix(A, transpose=True)
+    r = ks.solve(ctx, M, "BICG", b, L=L, E=1e-30)
+    o, env, lr = oracle_envelope(oracle, A, b, "BICG", L=L, E=1e-30)
+    assert r.status == o["status"] == 2
+    assert r.loop == o["loop"]
+    assert np.array_equal(r.hist_iter, o["hist_iter"])
+    if L > 0:
+        check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
