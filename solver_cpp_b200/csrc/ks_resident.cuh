@@ -651,11 +651,12 @@ inline ResShape resident_shape(long long n) {
   return sh;
 }
 
-template <int R, bool I16>
-inline cudaError_t res_cg_launch(const ResShape &sh, cudaStream_t s, const ResCgArgs &a, bool probe_only,
-                                 bool *fits) {
-  auto kern = k_cg_resident<R, I16>;
-  const size_t smem = (4 * sizeof(double)) << sh.shift;  // x, r and two p slices
+// Launches `kern` over one cluster of shape sh with `smem` bytes of dynamic
+// shared memory; probe_only: sets *fits to whether one such cluster can be
+// resident on the device and launches nothing.
+template <class Args>
+inline cudaError_t res_launch(void (*kern)(Args), const ResShape &sh, size_t smem, cudaStream_t s,
+                              const Args &a, bool probe_only, bool *fits) {
   if (sh.C > 8) {
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
@@ -686,39 +687,18 @@ inline cudaError_t res_cg_launch(const ResShape &sh, cudaStream_t s, const ResCg
   return cudaLaunchKernelEx(&cfg, kern, a);
 }
 
+template <int R, bool I16>
+inline cudaError_t res_cg_launch(const ResShape &sh, cudaStream_t s, const ResCgArgs &a, bool probe_only,
+                                 bool *fits) {
+  // x, r and two p slices
+  return res_launch(k_cg_resident<R, I16>, sh, (4 * sizeof(double)) << sh.shift, s, a, probe_only, fits);
+}
+
 template <int R, bool IA16, bool IT16>
 inline cudaError_t res_bicg_launch(const ResShape &sh, cudaStream_t s, const ResBicgArgs &a, bool probe_only,
                                    bool *fits) {
-  auto kern = k_bicg_resident<R, IA16, IT16>;
-  const size_t smem = (7 * sizeof(double)) << sh.shift;  // x, r, r*, two p and two p* slices
-  if (sh.C > 8) {
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return e;
-  }
-  if (smem > 48 * 1024) {
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)sh.C);
-  cfg.blockDim = dim3((unsigned)sh.T);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = (unsigned)sh.C;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  if (probe_only) {
-    int clusters = 0;
-    const cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
-    *fits = e == cudaSuccess && clusters >= 1;
-    if (e != cudaSuccess) (void)cudaGetLastError();
-    return cudaSuccess;
-  }
-  return cudaLaunchKernelEx(&cfg, kern, a);
+  // x, r, r*, two p and two p* slices
+  return res_launch(k_bicg_resident<R, IA16, IT16>, sh, (7 * sizeof(double)) << sh.shift, s, a, probe_only, fits);
 }
 
 template <int R>
