@@ -233,7 +233,7 @@ typedef struct {
   int32_t x_update;        /* CG, CR, BiCG: 0 auto, 1 x += alpha p every
                               iteration, 2 deferred through a ring of 32
                               directions (same x bit for bit)              */
-  int32_t cluster_solve;   /* CG and BiCG on at most 32768 rows (one GPU): 0
+  int32_t cluster_solve;   /* CG, CR, BiCG on at most 32768 rows (one GPU): 0
                               auto, the whole solve in one launch of one
                               thread-block cluster where the device can hold
                               it; 1 never (one kernel per step, as for larger

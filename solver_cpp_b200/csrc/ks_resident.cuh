@@ -1,4 +1,4 @@
-// Small systems solved inside one thread-block cluster (CG, BiCG).
+// Small systems solved inside one thread-block cluster (CG, CR, BiCG).
 //
 // Up to 32K rows the kernels of a CG iteration (cg.cpp:184-240) each take a
 // few microseconds and the loop is bound by its kernel boundaries (launch,
@@ -623,6 +623,153 @@ __global__ void __launch_bounds__(kResThreads, 1) k_bicg_resident(const ResBicgA
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
+// Row i of M times the vector v, read from the owners' slices (this CTA's
+// shared memory, or another CTA's through the cluster), in the row's CSR order.
+template <bool I16>
+__device__ __forceinline__ double row_times(cgx::cluster_group cl, const int *ptr, const int *col,
+                                            const short *col16, const double *val, int i, int shift, int rank,
+                                            const double *v_s) {
+  const int mask = (1 << shift) - 1;
+  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
+  double s = 0.0;
+#pragma unroll 4
+  for (int j = j0; j < j1; j++) {
+    const int c = I16 ? i + (int)__ldg(col16 + j) : __ldg(col + j);
+    const int o = c >> shift, lc = c & mask;
+    const double *vq = v_s + lc;
+    if (o != rank) vq = cl.map_shared_rank(vq, (unsigned)o);
+    s = add_rn(s, mul_rn(__ldg(val + j), *vq));
+  }
+  return s;
+}
+
+// cr::solve (cr.cpp:152-263) from x = 0 to the stopping test, in one launch
+// (as k_cg_resident; x and r in shared memory, p, q = A p and s = A r of the
+// thread's rows in registers). The SpMV reads r only, so r is the one vector
+// the CTAs publish; an iteration has three cluster reductions, in the
+// engine's order: (r,r) after x += alpha p, r -= alpha q (the stopping test;
+// it also publishes r), (r,s) after s = A r (beta), and (q,q) after p = beta
+// p + r, q = beta q + s (alpha).
+template <int R, bool I16>
+__global__ void __launch_bounds__(kResThreads, 1) k_cr_resident(const ResCgArgs a) {
+  cgx::cluster_group cl = cgx::this_cluster();
+  extern __shared__ double dyn_s[];  // slices of x and r
+  __shared__ double warp_s[kResMaxSums * 32];
+  __shared__ ResXchg xg;
+  __shared__ double hist_e[kResHist];
+  __shared__ long long hist_i[kResHist];
+  const int C = (int)cl.num_blocks();
+  const int rank = (int)cl.block_rank();
+  const int rp = 1 << a.shift;
+  double *x_s = dyn_s, *r_s = dyn_s + rp;
+  const int T = blockDim.x;
+  const int r0 = rank << a.shift;
+  ResScal S{a.st, rank == 0 && threadIdx.x == 0, a.st->k.s[S_EPS], a.st->k.aux[A_MAXLOOP], hist_e, hist_i};
+  S.begin();
+  xchg_init(cl, &xg);
+  int m = 0;
+  bool ok = true;
+  double p[R], q[R], sv[R];
+  double acc = 0.0;
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    const int li = threadIdx.x + k * T, i = r0 + li;
+    double ri = 0.0;
+    if (i < a.n) {
+      ri = sub_rn(a.b[i], 0.0);  // b - A*0 with x = 0; p = r (cr.cpp:79-86)
+      acc = add_rn(acc, mul_rn(ri, ri));
+    }
+    x_s[li] = 0.0;
+    r_s[li] = ri;
+    p[k] = ri;
+    q[k] = sv[k] = 0.0;
+  }
+  // |b|^2 and (r,r) are the same sum, r being b; the reduction also publishes r
+  double rr = 0.0;
+  ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &rr, no_shadow);
+  const double bnorm = sqrt(rr);
+  if (S.writer) a.st->k.s[S_BNORM] = bnorm;
+  if (ok) S.check_top(1, sqrt(rr) / bnorm);
+  double rs = 0.0, alpha = 0.0, beta = 0.0;
+  if (ok && S.done == kRunning) {
+    // q = A p (p = r), s = q; (r,s) and (q,q) -> rs, alpha
+    double sums[2] = {0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int i = r0 + threadIdx.x + k * T;
+      if (i < a.n) {
+        const double v = row_times<I16>(cl, a.ptr, a.col, a.col16, a.val, i, a.shift, rank, r_s);
+        q[k] = v;
+        sv[k] = v;
+        sums[0] = add_rn(sums[0], mul_rn(p[k], v));
+        sums[1] = add_rn(sums[1], mul_rn(v, v));
+      }
+    }
+    ok = cluster_sums<2>(sums, warp_s, &xg, m++, C, rank, no_shadow);
+    if (ok) {
+      rs = sums[0];
+      alpha = S.rdiv(sums[0], sums[1]);
+    }
+  }
+  long long L = 1;
+  while (ok && S.done == kRunning) {
+    // x += alpha p; r -= alpha q (published); (r,r) -> stopping test
+    acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int li = threadIdx.x + k * T, i = r0 + li;
+      if (i < a.n) {
+        x_s[li] = add_rn(mul_rn(alpha, p[k]), x_s[li]);
+        const double rk = add_rn(mul_rn(-alpha, q[k]), r_s[li]);
+        r_s[li] = rk;
+        acc = add_rn(acc, mul_rn(rk, rk));
+      }
+    }
+    double rr2 = 0.0;
+    if (!(ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &rr2, no_shadow))) break;
+    S.check_top(L + 1, sqrt(rr2) / bnorm);
+    L++;
+    if (S.done != kRunning) break;
+    // s = A r; (r,s) -> beta
+    acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int li = threadIdx.x + k * T, i = r0 + li;
+      if (i < a.n) {
+        sv[k] = row_times<I16>(cl, a.ptr, a.col, a.col16, a.val, i, a.shift, rank, r_s);
+        acc = add_rn(acc, mul_rn(r_s[li], sv[k]));
+      }
+    }
+    double rs2 = 0.0;
+    if (!(ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &rs2, no_shadow))) break;
+    beta = S.rdiv(rs2, rs);
+    rs = rs2;
+    if (S.done != kRunning) break;
+    // p = beta p + r; q = beta q + s; (q,q) -> alpha
+    acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < R; k++) {
+      const int li = threadIdx.x + k * T, i = r0 + li;
+      if (i < a.n) {
+        p[k] = add_rn(mul_rn(beta, p[k]), r_s[li]);
+        q[k] = add_rn(mul_rn(beta, q[k]), sv[k]);
+        acc = add_rn(acc, mul_rn(q[k], q[k]));
+      }
+    }
+    double qq = 0.0;
+    if (!(ok = cluster_sum(acc, warp_s, &xg, m++, C, rank, &qq, no_shadow))) break;
+    alpha = S.rdiv(rs, qq);
+  }
+  if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    const int li = threadIdx.x + k * T, i = r0 + li;
+    if (i < a.n) a.x[i] = x_s[li];
+  }
+  S.end();
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
 // ---------------------------------------------------------------- host side
 struct ResShape {
   int C = 0;      // CTAs (0: the system is too large)
@@ -692,6 +839,27 @@ inline cudaError_t res_cg_launch(const ResShape &sh, cudaStream_t s, const ResCg
                                  bool *fits) {
   // x, r and two p slices
   return res_launch(k_cg_resident<R, I16>, sh, (4 * sizeof(double)) << sh.shift, s, a, probe_only, fits);
+}
+
+template <int R, bool I16>
+inline cudaError_t res_cr_launch(const ResShape &sh, cudaStream_t s, const ResCgArgs &a, bool probe_only,
+                                 bool *fits) {
+  // x and r slices
+  return res_launch(k_cr_resident<R, I16>, sh, (2 * sizeof(double)) << sh.shift, s, a, probe_only, fits);
+}
+
+// As res_cg, for CR.
+inline cudaError_t res_cr(const ResShape &sh, bool i16, cudaStream_t s, const ResCgArgs &a, bool probe_only,
+                          bool *fits) {
+  switch (sh.R * 2 + (i16 ? 1 : 0)) {
+    case 2: return res_cr_launch<1, false>(sh, s, a, probe_only, fits);
+    case 3: return res_cr_launch<1, true>(sh, s, a, probe_only, fits);
+    case 4: return res_cr_launch<2, false>(sh, s, a, probe_only, fits);
+    case 5: return res_cr_launch<2, true>(sh, s, a, probe_only, fits);
+    case 8: return res_cr_launch<4, false>(sh, s, a, probe_only, fits);
+    case 9: return res_cr_launch<4, true>(sh, s, a, probe_only, fits);
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <int R, bool IA16, bool IT16>

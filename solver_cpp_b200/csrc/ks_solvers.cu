@@ -831,8 +831,31 @@ struct Xpby2ToOp {
   __device__ void finish(const double (&sm)[1]) const { st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], sm[0]); }
 };
 
+// CR on small systems as one thread-block-cluster launch (as run_cg_resident).
+inline bool run_cr_resident(const Env<double> &E, const double *b, double *x, ks_status *s) {
+  if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A->val) return false;
+  const ResShape sh = resident_shape(E.n);
+  if (!sh.C) return false;
+  const CsrDev &A = *E.A;
+  const ResCgArgs a{A.ptr, A.col, A.col16, A.val, b, x, E.st, E.ctx->d_err, (int)E.n, sh.shift};
+  bool fits = false;
+  if (res_cr(sh, A.col16 != nullptr, E.ctx->stream, a, true, &fits) != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  E.ctx->launches++;
+  const cudaError_t e = res_cr(sh, A.col16 != nullptr, E.ctx->stream, a, false, nullptr);
+  *s = e == cudaSuccess ? KS_OK : cuda_fail(E.ctx, e, "cluster-resident CR launch");
+  return true;
+}
+
 template <class VT>
 ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
+  if constexpr (std::is_same<VT, double>::value) {
+    ks_status s = KS_OK;
+    if (run_cr_resident(E, b, x, &s)) return s;
+  }
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take(), *s = W.take();
   const bool defer = defer_x(E, KS_CR);

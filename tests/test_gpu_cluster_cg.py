@@ -1,6 +1,6 @@
-"""GPU: CG and BiCG on small systems as one thread-block-cluster launch.
+"""GPU: CG, CR and BiCG on small systems as one thread-block-cluster launch.
 
-Up to 32768 rows (one GPU, FP64) CG and BiCG run as a single launch of one
+Up to 32768 rows (one GPU, FP64) CG, CR and BiCG run as a single launch of one
 cluster of up to 16 CTAs (ks_params.cluster_solve 0, the default); cluster_solve 1
 selects the kernel-per-step engine used for larger systems. Both paths do the
 same element-wise arithmetic and differ only in the order in which the dot
@@ -149,6 +149,48 @@ def test_bicg_cluster_maxloop_and_history_flushes(ks, ctx, oracle, L):
     M = ctx.matrix(A, transpose=True)
     r = ks.solve(ctx, M, "BICG", b, L=L, E=1e-30)
     o, env, lr = oracle_envelope(oracle, A, b, "BICG", L=L, E=1e-30)
+    assert r.status == o["status"] == 2
+    assert r.loop == o["loop"]
+    assert np.array_equal(r.hist_iter, o["hist_iter"])
+    if L > 0:
+        check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
+
+
+# ------------------------------------------------------------------ CR
+CR_CASES = sorted(c for c, m in index().items() if m["outer"] == "CR")
+
+
+@pytest.mark.parametrize("cluster_solve", [0, 1])
+@pytest.mark.parametrize("cid", CR_CASES)
+def test_cr_golden_history_on_both_paths(ks, ctx, cid, cluster_solve):
+    meta, g = load(cid)
+    A, b, _ = config_problem(meta["problem"], meta["grid"])
+    M = ctx.matrix(A)
+    r = ks.solve(ctx, M, "CR", b, cluster_solve=cluster_solve, **meta["params"])
+    assert r.converged == meta["converged"]
+    check_history(r.hist_iter, r.hist_err, g["hist_iter"], g["hist_err"], g["envelope"], r.loop, meta["loop"],
+                  meta["loop_range"])
+    assert round(r.true_res_log10, 1) == pytest.approx(meta["true_res_log10"], abs=0.21)
+
+
+@pytest.mark.parametrize("prob,g", SHAPES)
+def test_cr_cluster_and_engine_within_envelope(ks, ctx, oracle, prob, g):
+    A, b, _ = config_problem(prob, g)
+    M = ctx.matrix(A)
+    o, env, lr = oracle_envelope(oracle, A, b, "CR", E=1e-12, L=5000)
+    for cs in (0, 1):
+        r = ks.solve(ctx, M, "CR", b, E=1e-12, L=5000, cluster_solve=cs)
+        assert r.status == o["status"] == 0, (cs, r.status)
+        check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
+        assert r.true_rel_res < 2e-12, (cs, r.true_rel_res)
+
+
+@pytest.mark.parametrize("L", [0, 1, 7, 255, 256, 257])
+def test_cr_cluster_maxloop_and_history_flushes(ks, ctx, oracle, L):
+    A, b, _ = config_problem("varcoef2d", 40)
+    M = ctx.matrix(A)
+    r = ks.solve(ctx, M, "CR", b, L=L, E=1e-30)
+    o, env, lr = oracle_envelope(oracle, A, b, "CR", L=L, E=1e-30)
     assert r.status == o["status"] == 2
     assert r.loop == o["loop"]
     assert np.array_equal(r.hist_iter, o["hist_iter"])
