@@ -22,8 +22,11 @@ steps.
 `--impl reference` times the reference's own CPU path (oracle/_ref/Solver,
 built from the reference sources) on the host cores for the same workload.
 
-Multi-GPU (torchrun, N > 1): the path does not shard in this build; every rank
-solves its own replica (weak scaling) and the step time is the max over ranks.
+Multi-GPU (torchrun, N > 1): the rows of the one system are split over the
+ranks (contiguous blocks on grid planes; before every SpMV each rank receives
+its halo from its neighbours and every reduction is summed over the ranks,
+over NCCL): strong scaling, the step time the max over ranks. `--replicas`
+instead solves one independent replica per rank (weak scaling).
 """
 from __future__ import annotations
 
@@ -206,13 +209,13 @@ def run_ours(args, world, rank, local):
     ctx = ks.Context(local)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
-    split = args.split and world > 1
+    split = world > 1 and not args.replicas
     comm = None
     if split:  # row-split solve of the one system over the ranks (strong scaling), NCCL transport
         import torch.distributed as dist
 
         if W.get("adjoint"):
-            raise SystemExit("--split does not cover the adjoint workloads")
+            raise SystemExit("the row split does not cover the adjoint workloads (use --replicas)")
         uid = [ks.Comm.unique_id() if rank == 0 else None]
         dist.broadcast_object_list(uid, src=0)
         comm = ks.Comm.nccl(ctx, world, rank, uid[0])
@@ -382,7 +385,7 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and adj is None:
-        cpu = cpu_baseline_port(A, b, W, res)
+        cpu = cpu_baseline_reference(A, b, W, res)
 
     out = {
         "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); SpMV HBM GB/s",
@@ -416,44 +419,65 @@ def run_ours(args, world, rank, local):
     del launches0
 
 
-def cpu_baseline_port(A, b, W, res):
-    """The oracle (single-threaded C restatement of the reference) on a
-    bounded sample: a few iterations of the same method, scaled to the GPU
-    run's iteration count."""
+def _ref_workdir(A, b, threads):
+    """The workload's matrix in the reference's CRS text format, written by
+    the pure-Python writer (no part of the product library is loaded)."""
+    from solver_cpp_b200.matrices import write_crs
+
+    wd = tempfile.mkdtemp(prefix="refbench_")
+    write_crs(os.path.join(wd, "Matrix", "CRS", "bench"), A, b, workers=max(1, threads))
+    return wd
+
+
+def _repo_objects_loaded():
+    """Shared objects of this repository mapped into this process."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {ln.split()[-1] for ln in f if ln.rstrip().endswith(".so") or ".so." in ln}
+    except OSError:
+        return []
+    return sorted(p for p in paths if p.startswith(ROOT))
+
+
+def cpu_baseline_reference(A, b, W, res):
+    """The reference's own CPU path (oracle/_ref/Solver) on every host thread,
+    on a bounded sample of the workload: `cap` iterations of the same method
+    (-L cap), scaled to the GPU run's iteration count. The complete solve is
+    the reference arm's measurement (`--impl reference`)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
-    p = dict(W["params"])
-    p.pop("inner_precision", None)
-    sample_iters = 2 if W["inner"] != "NONE" else 20
-    p["L"] = sample_iters
-    P = pyoracle.Problem(A, with_transpose=W["transpose"])
-    t0 = time.perf_counter()
-    o = pyoracle.solve(P, b, W["outer"], W["inner"], hist_cap=64, **p)
-    dt = time.perf_counter() - t0
+    if not pyoracle.reference_available() or not W["ref_args"]:
+        return None
+    threads = os.cpu_count() or 1
+    wd = _ref_workdir(A, b, threads)
     vp = W["inner"] != "NONE"
+    cap = 40 if vp else 400
+    try:
+        r = pyoracle.run_reference(None, None, W["ref_args"] + ["-L", str(cap)], threads=threads, workdir=wd,
+                                   name="bench", keep_x=False)
+    finally:
+        import shutil
+
+        shutil.rmtree(wd, ignore_errors=True)
+    if r["time"] is None:
+        return None
     # a VP run of L iterations does L + 1 inner solves (vpcg.cpp:685,743)
-    per_iter = dt / (sample_iters + 1 if vp else sample_iters)
-    est = per_iter * max(1, res.loop)
-    return {"value": round(est, 3), "unit": "s", "cores": 1, "kind": "port",
-            "sample": f"{sample_iters} iterations of {W['outer']}" + (f"/{W['inner']}" if W['inner'] != 'NONE' else '')
-                      + f" in FP64 on the full system ({dt:.2f} s), scaled to the GPU run's {res.loop} iterations"}
-
-
-#: Iterations the reference's own full solve takes on each workload (outer
-#: iterations for VPCG), measured once by running oracle/_ref/Solver to
-#: convergence with 8 OpenMP threads: c4_mixed `-S vpcg -s cg -l 20 -e 1e-30
-#: -E 1e-10` 593 outer iterations (285.8 s); plain CG on the same system 5157
-#: (144.8 s); c2_cg `-S cg -E 1e-10` 530; c1_cg 202 (the 64^2 golden run).
-REF_FULL_ITERATIONS = {"c4_mixed": 593, "c2_cg": 530, "c1_cg": 202}
+    units = (cap + 1) if vp else cap
+    full = (res.loop + 1) if vp else res.loop
+    est = r["time"] / units * max(1, full)
+    return {"value": round(est, 3), "unit": "s", "cores": threads, "kind": "reference",
+            "sample": f"{cap} iterations of the reference binary ({' '.join(W['ref_args'])} -L {cap} -t {threads}): "
+                      f"{r['time']:.3f} s, scaled to the GPU run's {res.loop} iterations"}
 
 
 def run_reference(args, world, rank):
-    """The reference's own CPU path (oracle/_ref/Solver, all host threads) on
-    the same workload: each step runs a bounded number of iterations of the
-    same method and is scaled to the iteration count of the reference's full
-    solve (REF_FULL_ITERATIONS). The timed quantity is the reference's own
-    `time =` line, which covers its solve() only, as in the reference."""
+    """The reference's own CPU path (oracle/_ref/Solver, built unmodified from
+    its sources, every host thread) on the same workload. `value` is the
+    printed `time =` (its solve() span, cg.cpp:150,241) of ONE complete solve
+    to the workload's stopping test. The --warmup/--steps runs are bounded
+    samples (`cap` iterations each, -L cap) that fill ms_per_step. Nothing of
+    the product library is loaded in this process."""
     if world > 1 and rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -464,54 +488,50 @@ def run_reference(args, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/Solver was not built (reference "
                           "sources absent when the package was built)"}))
         return
+    if not W["ref_args"]:
+        print(json.dumps({"impl": "reference", "unavailable": f"the reference has no run of {args.workload} "
+                          "(its k-skip CG recurrence does not converge)"}))
+        return
     from solver_cpp_b200.matrices import config_problem
 
     A, b, _ = config_problem(W["problem"], W["grid"])
     threads = os.cpu_count() or 1
-    wd = tempfile.mkdtemp(prefix="refbench_")
-    mdir = os.path.join(wd, "Matrix", "CRS", "bench")
-    os.makedirs(mdir, exist_ok=True)
+    wd = _ref_workdir(A, b, threads)
     try:
-        import solver_cpp_b200 as ks
-
-        ks.crs_write(mdir, A, b)
-    except Exception:
-        from solver_cpp_b200.matrices import write_crs
-
-        write_crs(mdir, A, b)
-    # A step runs `cap` iterations of the reference's method (-L cap). A VP
-    # method does one inner solve before its loop and one per iteration
-    # (vpcg.cpp:685,743), so cap iterations hold cap + 1 inner solves and a
-    # full solve of `full` iterations holds full + 1.
-    vp = W["inner"] != "NONE"
-    cap = 3 if vp else 40
-    units = cap + 1 if vp else cap
-    times, loops = [], []
-    for i in range(args.warmup + args.steps):
-        r = pyoracle.run_reference(A, b, W["ref_args"] + ["-L", str(cap)], threads=threads, workdir=wd,
-                                   name="bench", keep_x=False)
-        if r["time"] is None:
+        full = pyoracle.run_reference(None, None, W["ref_args"], threads=threads, workdir=wd, name="bench",
+                                      keep_x=False, timeout=3000)
+        if full["time"] is None:
             print(json.dumps({"impl": "reference", "unavailable": "the reference binary did not report a time: "
-                              + (r["stderr"] or "")[-200:].replace("\n", " ")}))
+                              + (full["stderr"] or "")[-200:].replace("\n", " ")}))
             return
-        if i >= args.warmup:
-            times.append(r["time"])
-            loops.append(r["loop"])
-    per_unit = statistics.median(t / units for t in times)
-    full = args.ref_iterations or REF_FULL_ITERATIONS.get(args.workload) or cap
-    value = per_unit * (full + 1 if vp else full)
-    per_iter = per_unit
+        vp = W["inner"] != "NONE"
+        cap = 3 if vp else 40
+        times = []
+        for i in range(args.warmup + args.steps):
+            r = pyoracle.run_reference(None, None, W["ref_args"] + ["-L", str(cap)], threads=threads, workdir=wd,
+                                       name="bench", keep_x=False)
+            if i >= args.warmup and r["time"] is not None:
+                times.append(r["time"])
+    finally:
+        import shutil
+
+        shutil.rmtree(wd, ignore_errors=True)
+    value = full["time"]
+    sample = (f"one complete solve ({' '.join(W['ref_args'])} -t {threads}): {full['loop']} iterations, "
+              f"printed time = {value:.3f} s; each of the {args.steps} steps: {cap} iterations (-L {cap})")
     out = {"impl": "reference", "metric": "time-to-solution at FP64 rel-res 1e-10 (mixed vs plain FP64 GPU); "
            "SpMV HBM GB/s", "value": round(value, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": round(statistics.median(times) * 1e3, 2), "higher_is_better": False,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "warmup": args.warmup, "ms_per_step": round(statistics.median(times) * 1e3, 2) if times else None,
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded generator of the configuration; no dataset)",
            "config": {"workload": args.workload, "problem": W["problem"], "grid": W["grid"], "n": A.n,
                       "nnz": A.nnz, "reference_flags": W["ref_args"]},
+           "result": {"loop": full["loop"], "converged": full["converged"],
+                      "true_res_log10": full["true_res_log10"]},
            "cpu_baseline": {"value": round(value, 4), "unit": "s", "cores": threads, "kind": "reference",
-                            "sample": f"{cap} iterations per step of the reference binary (-t {threads}), "
-                                      f"{per_iter:.4f} s/iteration scaled to {full} iterations"},
-           "e2e": {"value": round(value, 4), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                            "sample": sample},
+           "e2e": {"value": round(value, 4), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "repo_objects_loaded": _repo_objects_loaded()}
     print(json.dumps(out))
 
 
@@ -615,14 +635,13 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c4_mixed")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-iterations", type=int, default=0)
     ap.add_argument("--spmv-only", choices=["fp64", "fp32", "bf16"], default=None,
                     help="time only the SpMV kernel on the workload's matrix (profiling)")
     ap.add_argument("--index32", action="store_true", help="with --spmv-only: int32 column indices")
     ap.add_argument("--csr", action="store_true", help="with --spmv-only: CSR only (no diagonal copy)")
-    ap.add_argument("--split", action="store_true",
-                    help="with --gpus N > 1: split the one system's rows over the ranks (strong scaling) "
-                         "instead of one replica per rank")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with --gpus N > 1: one independent replica per rank (weak scaling) instead of the "
+                         "default row split of the one system over the ranks (strong scaling)")
     ap.add_argument("--ortho-only", type=int, nargs="+", default=None, metavar="K",
                     help="time only the GMRES block dot / block AXPY over K basis vectors (profiling)")
     args = ap.parse_args()

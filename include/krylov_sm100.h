@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define KS_ABI_VERSION 3
+#define KS_ABI_VERSION 4
 
 typedef enum {
   KS_OK = 0,              /* converged / success (reference solve() == 0)      */
@@ -77,6 +77,15 @@ const char *ks_status_string(ks_status s);
 int64_t ks_ctx_launches(const ks_ctx *ctx);
 const char *ks_last_error(const ks_ctx *ctx);
 int ks_abi_version(void);
+/* Limit of every bounded device wait of this context's kernels (the SpMV's
+ * shared-memory staging barriers), in nanoseconds; ns <= 0 restores the
+ * default of 2 s. A wait that runs out ends its kernel early with the
+ * context's timeout flag set, and the call returns KS_TIMEOUT; the kernel
+ * still drains its own copies in flight (bounded by the default limit), so
+ * the context stays usable. Lowering it is a way to exercise that path. No
+ * counterpart in the reference, whose waits are unbounded (cudaDeviceSynchronize
+ * in checkCudaErrors). */
+ks_status ks_ctx_set_wait_limit(ks_ctx *ctx, int64_t ns);
 
 /* ----------------------------------------------------------------- matrix */
 
@@ -119,6 +128,11 @@ ks_status ks_mat_index_bytes(const ks_mat *mat, int *a_bytes, int *t_bytes);
 /* Diagonals of the diagonal copy of A and of A^T (0: the SpMV reads CSR). No
  * counterpart in the reference. */
 ks_status ks_mat_diagonals(const ks_mat *mat, int *a_diagonals, int *t_diagonals);
+/* 1 where the diagonal copy of A (of A^T) keeps only its main and upper
+ * diagonals because the matrix equals its transpose bit for bit: the SpMV
+ * then reads each lower diagonal as its upper mirror, shifted (4 instead of 7
+ * value streams for a 7-point stencil). No counterpart in the reference. */
+ks_status ks_mat_dia_symmetric(const ks_mat *mat, int *a_sym, int *t_sym);
 /* Copy the device-built transpose back (CSR of A^T: tptr[n+1], trow[nnz],
  * tval[nnz]), i.e. the CSC arrays the reference's CSR2CSC returns. */
 ks_status ks_mat_transpose_download(const ks_mat *mat, int32_t *tptr,
@@ -238,6 +252,25 @@ typedef struct {
                               thread-block cluster where the device can hold
                               it; 1 never (one kernel per step, as for larger
                               systems)                                      */
+  int32_t inner_fast;      /* VP methods whose inner CG runs in FP32 / with
+                              BF16 values on a one-GPU matrix with a diagonal
+                              copy: 0 auto, two kernels per inner iteration
+                              (the SpMV forms the direction and applies the
+                              previous x update); 1 the three-kernel loop.
+                              Both give the same values per element.       */
+  int32_t true_residual;   /* VP methods: when the recurrence residual
+                              passes -E, recompute |b - A x| / |b| in FP64
+                              and stop only if it passes too, else go on
+                              (the residual history carries on). 0 auto: on
+                              for an FP32 / BF16 inner solve, off for FP64
+                              (the reference stops on the recurrence
+                              residual, vpcg.cpp:704-713); 1 on; 2 off.     */
+  int32_t profile;         /* 1: device time per kernel class in the report
+                              (ks_report.t_*); adds two events per launch  */
+  int32_t reserved0;
+  const double *x_ref;     /* NULL, or a device FP64 solution of the same
+                              system (e.g. from the plain FP64 method):
+                              ks_report.x_rel_diff = |x - x_ref| / |x_ref|  */
 } ks_params;
 
 typedef struct {
@@ -250,6 +283,14 @@ typedef struct {
   int64_t spmv_count;      /* SpMVs issued (A and A^T, outer and inner)      */
   int64_t inner_iterations;/* inner-solver iterations (VP methods)          */
   double solve_seconds;    /* device time of the solve loop (CUDA events)    */
+  double x_rel_diff;       /* |x - x_ref| / |x_ref| (params.x_ref), else -1  */
+  int64_t true_residual_checks; /* FP64 true-residual checks of a VP method  */
+  /* Device seconds per kernel class with params.profile = 1 (else 0), the
+   * classes of the reference's times report (times.cpp:60-76): SpMVs with
+   * their fused epilogues; reductions (dots, norms, Gram and block dots);
+   * other kernels (vector updates, basis combinations, scalar steps);
+   * memsets; host<->device copies of the solve (ks_solve_host). */
+  double t_mv, t_dot, t_other, t_memset, t_h2d, t_d2h;
 } ks_report;
 
 void ks_params_default(ks_params *p);

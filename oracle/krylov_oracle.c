@@ -39,11 +39,24 @@ void oracle_spmv_t(const or_mat *A, const double *x, double *y) {
  * or_params.sum_chunks). The oracle is single-threaded test code. */
 static int g_sum_chunks = 1;
 
+/* Pairwise (recursive halving) sum of x[i]*y[i], runs of 8 summed in
+ * order: the accuracy class of a parallel tree reduction. */
+static double pair_dot(long n, const double *x, const double *y) {
+  if (n <= 8) {
+    double t = 0.0;
+    for (long i = 0; i < n; i++) t += x[i] * y[i];
+    return t;
+  }
+  const long h = n / 2;
+  return pair_dot(h, x, y) + pair_dot(n - h, x + h, y + h);
+}
+
 /* blas::dot (blas.cpp:149-162). With g_sum_chunks = T > 1 the index range is
  * split as OpenMP schedule(static) splits it over T threads (the first n % T
  * threads take one extra element), each part summed from 0.0 in order and
- * the parts added in thread order. */
+ * the parts added in thread order. g_sum_chunks = -1: pairwise summation. */
 double oracle_dot(long n, const double *x, const double *y) {
+  if (g_sum_chunks == -1) return pair_dot(n, x, y);
   if (g_sum_chunks <= 1) {
     double t = 0.0;
     for (long i = 0; i < n; i++) t += x[i] * y[i];
@@ -961,7 +974,7 @@ int oracle_solve(const or_mat *A, const or_params *p, const double *b,
                  double *x, long *hist_iter, double *hist_err, long hist_cap,
                  or_report *rep) {
   ctx_t c = {A, p, 0, p->inner != OR_NONE};
-  g_sum_chunks = p->sum_chunks > 1 ? p->sum_chunks : 1;
+  g_sum_chunks = p->sum_chunks > 1 || p->sum_chunks == -1 ? p->sum_chunks : 1;
   hist_t h = {hist_iter, hist_err, hist_iter && hist_err ? hist_cap : 0, 0};
   res_t res = {99, 0};
   long n = A->n;

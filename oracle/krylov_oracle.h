@@ -55,7 +55,8 @@ typedef struct {
   int sum_chunks;         /* >1: dot products and norms summed as that many
                              contiguous partial sums added in order, the way
                              an OpenMP static reduction with that many
-                             threads does; 0/1: one sequential sum (-t 1) */
+                             threads does; 0/1: one sequential sum (-t 1);
+                             -1: pairwise (recursive halving) sums */
 } or_params;
 
 typedef struct {

@@ -211,10 +211,15 @@ def reference_available():
     return os.path.exists(REF_BIN)
 
 
-def run_reference(A, b, args, threads=1, workdir=None, name="prob", timeout=3600, keep_x=True):
+def run_reference(A, b, args, threads=1, workdir=None, name="prob", timeout=3600, keep_x=True,
+                  run_dir=None):
     """Run the reference CPU binary on (A, b) with extra CLI ``args`` (a list,
     e.g. ``["-S", "cg", "-E", "1e-10"]``). Returns a dict with the history,
-    x, the printed loop/time/true residual and the verdict."""
+    x, the printed loop/time/true residual and the verdict.
+
+    ``A`` may be None when ``workdir`` already holds the CRS files of
+    ``name``. ``run_dir`` (default ``<workdir>/run``) receives ``./output``;
+    give concurrent runs of one matrix their own."""
     from solver_cpp_b200.matrices import write_crs
 
     own = workdir is None
@@ -222,7 +227,7 @@ def run_reference(A, b, args, threads=1, workdir=None, name="prob", timeout=3600
     mdir = os.path.join(wd, "Matrix", "CRS", name)
     if not os.path.exists(os.path.join(mdir, "ColVal.txt")):
         write_crs(mdir, A, b)
-    run_dir = os.path.join(wd, "run")
+    run_dir = run_dir or os.path.join(wd, "run")
     os.makedirs(os.path.join(run_dir, "output"), exist_ok=True)
     cmd = [REF_BIN, "-p", wd, "-m", name, "-t", str(threads)] + list(args)
     proc = subprocess.run(cmd, cwd=run_dir, capture_output=True, text=True, timeout=timeout)

@@ -84,6 +84,10 @@ class Context:
     def set_stream(self, stream_ptr):
         _check(lib().ks_ctx_set_stream(self.handle, C.c_void_p(stream_ptr)), self.handle, "set_stream")
 
+    def set_wait_limit(self, ns: int):
+        """Limit of the kernels' bounded device waits in ns (<= 0: the 2 s default)."""
+        _check(lib().ks_ctx_set_wait_limit(self.handle, int(ns)), self.handle, "set_wait_limit")
+
     def matrix(self, A: CSR, transpose=False, fp32=False, bf16=False, index32=False, diag=True) -> "Matrix":
         return Matrix(self, A, transpose=transpose, fp32=fp32, bf16=bf16, index32=index32, diag=diag)
 
@@ -132,8 +136,11 @@ class Matrix:
         _check(lib().ks_mat_index_bytes(self.handle, C.byref(a), C.byref(t)), self.ctx.handle, "index_bytes")
         da, dt = C.c_int(), C.c_int()
         _check(lib().ks_mat_diagonals(self.handle, C.byref(da), C.byref(dt)), self.ctx.handle, "diagonals")
+        sa, st = C.c_int32(), C.c_int32()
+        _check(lib().ks_mat_dia_symmetric(self.handle, C.byref(sa), C.byref(st)), self.ctx.handle, "dia_symmetric")
         return {"n": n.value, "nnz": nnz.value, "row_blocks": rb.value, "index_bytes": a.value,
-                "t_index_bytes": t.value, "diagonals": da.value, "t_diagonals": dt.value}
+                "t_index_bytes": t.value, "diagonals": da.value, "t_diagonals": dt.value,
+                "dia_symmetric": sa.value, "t_dia_symmetric": st.value}
 
     def transpose_arrays(self):
         tptr = np.zeros(self.n + 1, dtype=np.int32)

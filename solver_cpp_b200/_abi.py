@@ -44,7 +44,7 @@ MAT_INDEX32 = 8
 MAT_NO_DIAG = 16
 
 
-ABI_VERSION = 3  # KS_ABI_VERSION of the header these structures mirror
+ABI_VERSION = 4  # KS_ABI_VERSION of the header these structures mirror
 
 
 class Params(C.Structure):
@@ -55,7 +55,8 @@ class Params(C.Structure):
         ("inner_kskip", C.c_int32), ("inner_fix", C.c_int32),
         ("inner_precision", C.c_int32), ("reference_defects", C.c_int32),
         ("transpose", C.c_int32), ("poll_interval", C.c_int32), ("x_update", C.c_int32),
-        ("cluster_solve", C.c_int32),
+        ("cluster_solve", C.c_int32), ("inner_fast", C.c_int32), ("true_residual", C.c_int32),
+        ("profile", C.c_int32), ("reserved0", C.c_int32), ("x_ref", C.c_void_p),
     ]
 
 
@@ -64,6 +65,9 @@ class Report(C.Structure):
         ("status", C.c_int32), ("loop", C.c_int64), ("hist_len", C.c_int64),
         ("final_rel_res", C.c_double), ("true_res_log10", C.c_double), ("true_rel_res", C.c_double),
         ("spmv_count", C.c_int64), ("inner_iterations", C.c_int64), ("solve_seconds", C.c_double),
+        ("x_rel_diff", C.c_double), ("true_residual_checks", C.c_int64),
+        ("t_mv", C.c_double), ("t_dot", C.c_double), ("t_other", C.c_double), ("t_memset", C.c_double),
+        ("t_h2d", C.c_double), ("t_d2h", C.c_double),
     ]
 
 
@@ -84,12 +88,14 @@ SIGNATURES = [
     ("ks_ctx_launches", C.c_int64, [_VP]),
     ("ks_last_error", C.c_char_p, [_VP]),
     ("ks_abi_version", C.c_int, []),
+    ("ks_ctx_set_wait_limit", C.c_int, [_VP, C.c_int64]),
     ("ks_csr_upload", C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP, C.c_uint, C.POINTER(_VP)]),
     ("ks_csr_upload_device", C.c_int, [_VP, _I64, _I64, _VP, _VP, _VP, C.c_uint, C.POINTER(_VP)]),
     ("ks_mat_destroy", C.c_int, [_VP]),
     ("ks_mat_info", C.c_int, [_VP, _PI64, _PI64, _PI64]),
     ("ks_mat_index_bytes", C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("ks_mat_diagonals", C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("ks_mat_dia_symmetric", C.c_int, [_VP, _PI32, _PI32]),
     ("ks_mat_transpose_download", C.c_int, [_VP, _VP, _VP, _VP]),
     ("ks_vec_create", C.c_int, [_VP, _I64, C.c_int, C.POINTER(_VP)]),
     ("ks_vec_wrap", C.c_int, [_VP, _I64, C.c_int, _VP, C.POINTER(_VP)]),

@@ -55,6 +55,36 @@ const char *kUsage =
     "  --precision fp64|fp32|bf16  (inner solve of VP methods)  --reference-defects  --device N\n"
     "methods: cg bicg cr gcr gmres kskipcg kskipcr kskipbicg vpcg vpbicg vpcr vpgcr vpgmres\n";
 
+// The times report (times::showTimeOnCPU / showTimeOnGPU, times.cpp:44-76),
+// line for line, the format data2csv.sh parses. No host thread does Krylov
+// arithmetic here, so the CPU block is zero; the GPU block holds the device
+// time of each kernel class (ks_report.t_*): SpMVs with their fused
+// epilogues, reductions (dots, norms, Gram and block dots, with the vector
+// updates fused into them), memsets, and the copies of b in and x out.
+void print_times(const ks_report &rep) {
+  const double total = rep.solve_seconds > 0 ? rep.solve_seconds : 1e-30;
+  auto line = [&](const char *label, double t) {
+    std::cout << label << std::setprecision(6) << t << ", " << std::setprecision(2) << t / total * 100 << "%"
+              << std::endl;
+  };
+  std::cout << "Execution time on CPU" << std::endl;
+  line("\tDot process time = ", 0.0);
+  line("\tMV process time  = ", 0.0);
+  line("\t  cons time    = ", 0.0);
+  line("\t  dis time    = ", 0.0);
+  const double all = rep.t_mv + rep.t_dot;
+  std::cout << "Execution time on GPU" << std::endl;
+  line("\tDot process time  = ", rep.t_dot);
+  line("\tMV process time   = ", rep.t_mv);
+  line("\t  H2D time       = ", rep.t_h2d);
+  line("\t  D2H time       = ", rep.t_d2h);
+  line("\t  Memset time    = ", rep.t_memset);
+  line("\tother time       = ", total - all);
+  line("\t  Copy time    = ", 0.0);
+  line("\t  cons time    = ", 0.0);
+  line("\t  dis time    = ", 0.0);
+}
+
 // solver_collection.cpp:240-267
 ks_solver to_solver(const std::string &s) {
   static const std::map<std::string, ks_solver> m = {
@@ -232,10 +262,39 @@ int main(int argc, char **argv) {
 
   const bool vp = outer == KS_VPCG || outer == KS_VPCR || outer == KS_VPGCR || outer == KS_VPGMRES ||
                   outer == KS_VPBICG;
+  // collection::showCMD (solver_collection.cpp:603-652), the lines
+  // data2csv.sh reads ("CUDA :", "MultiGPU :") among them; this program
+  // always runs on the GPU, on one device
   std::cout << "=========================================================" << std::endl;
+  std::cout << "InputSource : " << (o.crs_name != "NONE" ? "CRS" : "MM") << std::endl;
+  std::cout << "FullPath : "
+            << (o.crs_name != "NONE" ? o.crs_path + "/" + o.l1 + "/" + o.crs_dir + "/" + o.crs_name
+                                     : o.mm_path + "/" + o.l1 + "/" + o.mm_dir + "/" + o.mm_name)
+            << std::endl;
+  std::cout << "N : " << n << std::endl;
+  std::cout << "NNZ : " << nnz << std::endl;
+  std::cout << "-------------" << std::endl;
+  std::cout << "OpenMP thread : " << o.threads << std::endl;
+  std::cout << "GPU Num : " << o.device << std::endl;
+  std::cout << "-------------" << std::endl;
+  std::cout << "VP : " << (vp ? "On" : "Off") << std::endl;
+  std::cout << "CUDA : On" << std::endl;
+  std::cout << "Pinned : " << (o.pinned ? "On" : "Off") << std::endl;
+  std::cout << "MultiGPU : Off" << std::endl;
+  std::cout << "-------------" << std::endl;
   std::cout << "OuterSolver : " << solver_name(outer) << std::endl;
+  std::cout << "OuterMaxLoop : " << o.outer_maxloop << std::endl;
+  std::cout << "OuterEps : " << o.outer_eps << std::endl;
+  std::cout << "OuterRestart : " << o.outer_restart << std::endl;
+  std::cout << "OuterKskip : " << o.outer_kskip << std::endl;
+  std::cout << "OuterFix : " << o.outer_fix << std::endl;
+  std::cout << "-------------" << std::endl;
   std::cout << "InnerSolver : " << solver_name(inner) << std::endl;
-  std::cout << "N : " << n << "  NNZ : " << nnz << std::endl;
+  std::cout << "InnerMaxLoop : " << o.inner_maxloop << std::endl;
+  std::cout << "InnerEps : " << o.inner_eps << std::endl;
+  std::cout << "InnerRestart : " << o.inner_restart << std::endl;
+  std::cout << "InnerKskip : " << o.inner_kskip << std::endl;
+  std::cout << "InnerFix : " << o.inner_fix << std::endl;
   std::cout << "=========================================================" << std::endl;
   if (outer == KS_KSKIPCR || outer == KS_VPBICG) {  // outerMethods.cpp:46-48,57-59
     std::cout << "Not implemented" << std::endl;
@@ -268,6 +327,7 @@ int main(int argc, char **argv) {
   p.inner_fix = o.inner_fix;
   p.inner_precision = prec;
   p.reference_defects = o.reference_defects ? 1 : 0;
+  p.profile = 1;  // the times report below
   const int64_t cap = o.outer_maxloop + 2;
   std::vector<int64_t> hit((size_t)cap);
   std::vector<double> herr((size_t)cap);
@@ -299,9 +359,8 @@ int main(int argc, char **argv) {
   std::cout << "|b-ax|2/|b|2 = " << std::fixed << std::setprecision(1) << rep.true_res_log10 << std::endl;
   std::cout << "loop = " << rep.loop << std::endl;
   std::cout << "time = " << std::setprecision(6) << rep.solve_seconds << std::endl;
-  std::cout << "Execution time on GPU" << std::endl;
-  std::cout << "\tsolve (device, CUDA events) = " << std::setprecision(6) << rep.solve_seconds << std::endl;
-  std::cout << "\ttrue |b-Ax|/|b| = " << std::scientific << std::setprecision(3) << rep.true_rel_res << std::endl;
+  print_times(rep);
+  std::cout << "true |b-Ax|/|b| = " << std::scientific << std::setprecision(3) << rep.true_rel_res << std::endl;
   {
     std::ofstream fx("./output/" + nm + "_xvec.txt");
     if (!fx.is_open()) die("File open error");

@@ -82,7 +82,7 @@ struct CsrDev {
   // Diagonal copy of a stencil-like matrix, read by the SpMV instead of the
   // CSR arrays: every row holds its columns at offsets (col - row) from a set
   // of dia_nd <= kMaxDiag offsets, dia_off ascending. Values are stored
-  // diagonal-major, dia_val[d * n + i] (0 where row i has no entry on
+  // diagonal-major, dia_val[d * dia_ds + i] (0 where row i has no entry on
   // diagonal d), and bit d of dia_mask[i] is set where it has one. Kept only
   // when every row lists its columns in increasing order (so a row summed
   // diagonal by diagonal is summed in its CSR order) and the diagonals are at
@@ -94,6 +94,17 @@ struct CsrDev {
   float *dia_val32 = nullptr;
   __nv_bfloat16 *dia_val16 = nullptr;
   unsigned char *dia_mask = nullptr;
+  // Symmetric half storage (dia_sym = 1): when A equals its transpose bit for
+  // bit (pattern and values; offsets symmetric about a main diagonal), only
+  // the main diagonal and the upper diagonals are kept, dia_nd / 2 + 1 of
+  // them, each of dia_ds = dia_pad + n elements: dia_pad leading zeros, then
+  // row 0 .. n-1. Row i's entry on lower diagonal d (offset -o) is
+  // A[i][i-o] = A[i-o][i], the upper mirror's element at row i - o, which
+  // for i < o lands in the zero pad. dia_sym = 0: all dia_nd diagonals, each
+  // of n elements (dia_ds = n, dia_pad = 0).
+  int dia_sym = 0;
+  int dia_pad = 0;
+  long long dia_ds = 0;
 };
 
 template <class MT>
@@ -287,6 +298,7 @@ struct ks_ctx {
   unsigned *counters = nullptr; // last-CTA-done counters
   int ncounters = 0;
   int *d_err = nullptr;         // set by a kernel whose bounded wait ran out
+  unsigned long long wait_ns = 2000000000ull;  // limit of those waits (ks_ctx_set_wait_limit)
   double *d_result = nullptr;   // device staging for scalar results
   size_t d_result_len = 0;
   double *h_pinned = nullptr;   // pinned host staging (scalars)
@@ -308,10 +320,19 @@ struct ks_ctx {
   const int *poll_done = nullptr;
   int *h_snap = nullptr;        // mapped host ring (nflags entries)
   int *d_snap = nullptr;        // its device view
+  // Per-class device time of a solve (ks_params.profile): every launch_k
+  // records an event before and after its kernel and the class the launcher
+  // set in next_class (ks::KernelClass; reset to kOther after each launch).
+  int prof_on = 0;
+  int next_class = 0;
+  std::vector<cudaEvent_t> prof_events;  // pool, reused across solves
+  std::vector<unsigned char> prof_class;  // class of recorded launch i
 };
 
 namespace ks {
 constexpr int kStageLen = 4096;  // >= 2 x 1024 block-dot results, >= kMaxDots
+// Kernel classes of the times report (times.cpp:60-76).
+enum KernelClass : int { kOther = 0, kMv = 1, kDot = 2, kMemset = 3, kNumClasses = 4 };
 }
 
 namespace ks {

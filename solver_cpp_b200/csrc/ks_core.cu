@@ -307,6 +307,34 @@ __global__ void k_dia_fill(const int *__restrict__ ptr, const int *__restrict__ 
   }
 }
 
+// Pass 3: is the copy symmetric? For every lower diagonal d (offset -o) and
+// its mirror u = nd - 1 - d (offset +o), row i's entry on d must equal row
+// i - o's entry on u in presence and value, bit for bit (the zeros of absent
+// entries compare equal); a row i < o has no entry on d. flag = 1 otherwise.
+__global__ void k_dia_symcheck(const double *__restrict__ dval, const unsigned char *__restrict__ mask, int n,
+                               DiagOffsets o, int *flag) {
+  const int h = o.nd / 2;
+  int bad = 0;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    const unsigned m = mask[r];
+    for (int d = 0; d < h; d++) {
+      const int u = o.nd - 1 - d;
+      const long long q = r + o.off[d];
+      const unsigned has = (m >> d) & 1u;
+      if (q < 0) {
+        bad |= (int)has;
+        continue;
+      }
+      const unsigned hu = (mask[q] >> u) & 1u;
+      const long long a = __double_as_longlong(dval[(long long)d * n + r]);
+      const long long b = __double_as_longlong(dval[(long long)u * n + q]);
+      if (has != hu || a != b) bad = 1;
+    }
+  }
+  if (bad) atomicOr(flag, 1);
+}
+
 static void free_dia(CsrDev &A) {
   cudaFree(A.dia_val);
   cudaFree(A.dia_val32);
@@ -317,10 +345,15 @@ static void free_dia(CsrDev &A) {
   A.dia_val16 = nullptr;
   A.dia_mask = nullptr;
   A.dia_nd = 0;
+  A.dia_sym = 0;
+  A.dia_pad = 0;
+  A.dia_ds = 0;
 }
 
 // Builds the diagonal copy when the matrix qualifies (CsrDev::dia_*); leaves
-// dia_nd = 0 otherwise. Value copies follow the CSR ones (FP32, BF16).
+// dia_nd = 0 otherwise. Value copies follow the CSR ones (FP32, BF16). A
+// matrix equal to its transpose (on one GPU: the copy must hold every row a
+// lower diagonal reaches) keeps the symmetric half only.
 static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long long cmin, long long cmax) {
   if (A.n < 1 || A.nnz < 1) return KS_OK;
   const int g = ctx->num_sms * 8;
@@ -336,14 +369,19 @@ static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long lo
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_buf, d_buf, sizeof(h_buf), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  cudaFree(d_buf);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "diagonal scan");
-  if (h_buf[kMaxDiag]) return KS_OK;  // unordered rows or too many diagonals: CSR only
+  if (e != cudaSuccess) {
+    cudaFree(d_buf);
+    return cuda_fail(ctx, e, "diagonal scan");
+  }
   DiagOffsets o{};
   for (int k = 0; k < kMaxDiag; k++)
     if (h_buf[k] != kDiagEmpty) o.off[o.nd++] = h_buf[k];
   std::sort(o.off, o.off + o.nd);
-  if (o.nd < 1 || 4 * A.nnz < 3LL * o.nd * A.n) return KS_OK;  // diagonals less than 3/4 full
+  // unordered rows, too many diagonals, or diagonals less than 3/4 full: CSR only
+  if (h_buf[kMaxDiag] || o.nd < 1 || 4 * A.nnz < 3LL * o.nd * A.n) {
+    cudaFree(d_buf);
+    return KS_OK;
+  }
   const long long len = (long long)o.nd * A.n;
   // The copy is an optimisation: if the device cannot hold it, CSR serves.
   auto got = [&](cudaError_t a) {
@@ -352,19 +390,68 @@ static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long lo
     free_dia(A);
     return false;
   };
-  if (!got(cudaMalloc(&A.dia_val, sizeof(double) * (size_t)len)) || !got(cudaMalloc(&A.dia_mask, (size_t)A.n)))
+  if (!got(cudaMalloc(&A.dia_val, sizeof(double) * (size_t)len)) || !got(cudaMalloc(&A.dia_mask, (size_t)A.n))) {
+    cudaFree(d_buf);
     return KS_OK;
-  if ((flags & KS_MAT_FP32) && !got(cudaMalloc(&A.dia_val32, sizeof(float) * (size_t)len))) return KS_OK;
-  if ((flags & KS_MAT_BF16) && !got(cudaMalloc(&A.dia_val16, sizeof(__nv_bfloat16) * (size_t)len))) return KS_OK;
+  }
   KS_CUDA(ctx, cudaMemsetAsync(A.dia_val, 0, sizeof(double) * (size_t)len, ctx->stream));
   k_dia_fill<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.val, A.n, o, A.dia_val, A.dia_mask);
-  if (A.dia_val32) k_to_f32<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val32, len);
-  if (A.dia_val16) k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val16, len);
+  KS_CUDA(ctx, cudaGetLastError());
+  // symmetric half storage
+  const int h = o.nd / 2;
+  bool sym = (o.nd & 1) && o.off[h] == 0 && cmin == 0 && cmax == A.n && h > 0;
+  for (int k = 0; sym && k < h; k++) sym = o.off[k] == -o.off[o.nd - 1 - k];
+  if (sym) {
+    int flag = 0;
+    e = cudaMemsetAsync(d_buf, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess) {
+      k_dia_symcheck<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_mask, A.n, o, d_buf);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, d_buf, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      cudaFree(d_buf);
+      return cuda_fail(ctx, e, "diagonal symmetry check");
+    }
+    sym = flag == 0;
+  }
+  cudaFree(d_buf);
+  long long ds = A.n, stored = len;
+  int pad = 0;
+  if (sym) {
+    pad = -o.off[0];
+    ds = (long long)pad + A.n;
+    stored = (long long)(h + 1) * ds;
+    double *sv = nullptr;
+    if (cudaMalloc(&sv, sizeof(double) * (size_t)stored) == cudaSuccess) {
+      KS_CUDA(ctx, cudaMemsetAsync(sv, 0, sizeof(double) * (size_t)stored, ctx->stream));
+      for (int j = 0; j <= h; j++)
+        KS_CUDA(ctx, cudaMemcpyAsync(sv + (long long)j * ds + pad, A.dia_val + (long long)(h + j) * A.n,
+                                     sizeof(double) * (size_t)A.n, cudaMemcpyDeviceToDevice, ctx->stream));
+      KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      cudaFree(A.dia_val);
+      A.dia_val = sv;
+    } else {  // no room for the half copy next to the full one: keep the full one
+      (void)cudaGetLastError();
+      sym = false;
+      ds = A.n;
+      stored = len;
+      pad = 0;
+    }
+  }
+  if ((flags & KS_MAT_FP32) && !got(cudaMalloc(&A.dia_val32, sizeof(float) * (size_t)stored))) return KS_OK;
+  if ((flags & KS_MAT_BF16) && !got(cudaMalloc(&A.dia_val16, sizeof(__nv_bfloat16) * (size_t)stored))) return KS_OK;
+  if (A.dia_val32) k_to_f32<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val32, stored);
+  if (A.dia_val16) k_to_bf16<<<g, 256, 0, ctx->stream>>>(A.dia_val, A.dia_val16, stored);
   KS_CUDA(ctx, cudaGetLastError());
   A.dia_nd = o.nd;
   for (int k = 0; k < kMaxDiag; k++) A.dia_off[k] = k < o.nd ? o.off[k] : 0;
   A.dia_cmin = (int)cmin;
   A.dia_cmax = (int)cmax;
+  A.dia_sym = sym ? 1 : 0;
+  A.dia_pad = pad;
+  A.dia_ds = ds;
   return KS_OK;
 }
 
@@ -618,10 +705,25 @@ ks_status ks_ctx_destroy(ks_ctx *ctx) {
       if (ctx->flag_events[i]) cudaEventDestroy(ctx->flag_events[i]);
     delete[] ctx->flag_events;
   }
+  for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
+  return KS_OK;
+}
+
+ks_status ks_ctx_set_wait_limit(ks_ctx *ctx, int64_t ns) {
+  if (!ctx) return KS_BAD_INPUT;
+  const int64_t cap = 10000000000LL;  // 10 s
+  ctx->wait_ns = ns <= 0 ? kWaitLimitNs : (unsigned long long)std::min<int64_t>(ns, cap);
+  return KS_OK;
+}
+
+ks_status ks_mat_dia_symmetric(const ks_mat *m, int *a_sym, int *t_sym) {
+  if (!m) return KS_BAD_INPUT;
+  if (a_sym) *a_sym = m->A.dia_sym;
+  if (t_sym) *t_sym = m->has_T ? m->T.dia_sym : 0;
   return KS_OK;
 }
 

@@ -182,7 +182,27 @@ inline void launch_k(ks_ctx *ctx, void (*kern)(KArgs...), dim3 grid, dim3 block,
   cfg.attrs = at;
   cfg.numAttrs = 1;
   ctx->launches++;
+  const int cls = ctx->next_class;
+  ctx->next_class = kOther;
+  if (!ctx->prof_on) {
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+    return;
+  }
+  const size_t i = ctx->prof_class.size();
+  while (ctx->prof_events.size() < 2 * i + 2) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {  // no more events: stop recording
+      (void)cudaGetLastError();
+      ctx->prof_on = 0;
+      cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+      return;
+    }
+    ctx->prof_events.push_back(e);
+  }
+  cudaEventRecord(ctx->prof_events[2 * i], ctx->stream);
   cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+  cudaEventRecord(ctx->prof_events[2 * i + 1], ctx->stream);
+  ctx->prof_class.push_back((unsigned char)cls);
 }
 
 template <class MT>
@@ -299,10 +319,26 @@ inline const __nv_bfloat16 *dia_values_of<__nv_bfloat16>(const CsrDev &A) {
 template <class MT>
 inline DiaT<MT> dview(const CsrDev &A) {
   DiaT<MT> d;
-  d.val = dia_values_of<MT>(A);
-  d.mask = A.dia_mask;
+  const MT *v = dia_values_of<MT>(A);
+  const int nd = A.dia_nd, h = nd / 2;
+  for (int k = 0; k < kMaxDiag; k++) {
+    d.vb[k] = v;
+    d.vs[k] = 0;
+    if (k >= nd) continue;
+    if (!A.dia_sym) {
+      d.vb[k] = v + (long long)k * A.dia_ds;
+    } else if (k >= h) {  // main and upper diagonals: stored rows
+      d.vb[k] = v + (long long)(k - h) * A.dia_ds + A.dia_pad;
+    } else {  // lower diagonal k: its mirror nd-1-k, shifted back by the offset
+      d.vb[k] = v + (long long)(nd - 1 - k - h) * A.dia_ds + A.dia_pad;
+      d.vs[k] = A.dia_off[k];
+    }
+  }
+  // FP64 sums add only the entries the row has (bit-exact also for
+  // non-finite x); FP32/BF16 add the stored zeros (see ks_spmv_dia.cuh).
+  d.mask = std::is_same<MT, double>::value ? A.dia_mask : nullptr;
   d.n = A.n;
-  d.nd = A.dia_nd;
+  d.nd = nd;
   d.cmin = A.dia_cmin;
   d.cmax = A.dia_cmax;
   for (int k = 0; k < kMaxDiag; k++) d.off[k] = A.dia_off[k];
@@ -332,6 +368,7 @@ inline void launch_spmv_dn(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX 
   const long long need = ((long long)A.n + kThreads - 1) / kThreads;
   const long long wave = (long long)ctx->num_sms * spmv_dia_ctas_per_sm<NV, NDG, MT, GX, Epi>(ctx->device);
   const int grid = (int)std::max<long long>(1, std::min(need, wave));
+  ctx->next_class = kMv;
   launch_k(ctx, spmv_dia_kernel<NV, NDG, MT, GX, Epi>, dim3(grid), dim3(kThreads), 0, dview<MT>(A), g0, g1, epi,
            stop, red_of(ctx, slot));
 }
@@ -357,8 +394,9 @@ inline void launch_spmv_k(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &
                           int slot) {
   const int per_sm = spmv_tma_ctas_per_sm<NV, MT, IT, GX, Epi>(ctx->device);
   const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
+  ctx->next_class = kMv;
   launch_k(ctx, spmv_tma_kernel<NV, MT, IT, GX, Epi>, dim3(grid), dim3(kThreads), spmv_tma_smem<MT, IT>(),
-           tview<MT, IT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err);
+           tview<MT, IT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err, ctx->wait_ns);
 }
 
 template <int NV, class MT, class IT, class GX, class Epi>
@@ -393,6 +431,19 @@ inline void launch_spmv2(ks_ctx *ctx, const CsrDev &A, const XT *x0, const XT *x
   launch_spmv_g<2, MT, GPtr<XT>, Epi>(ctx, A, GPtr<XT>{x0}, GPtr<XT>{x1}, epi, stop, slot);
 }
 
+// Class of a vector pass in the times report: a pass with reductions is a
+// dot (most also update vectors: the reductions are fused into them), one
+// marked kMemset (ZeroOp) a memset, any other pass "other".
+template <class Op, class = void>
+struct is_memset_op : std::false_type {};
+template <class Op>
+struct is_memset_op<Op, std::void_t<decltype(Op::kMemset)>> : std::integral_constant<bool, Op::kMemset> {};
+
+template <class O>
+constexpr int vec_class() {
+  return is_memset_op<O>::value ? kMemset : (O::ND > 0 ? kDot : kOther);
+}
+
 template <class Op>
 inline void launch_vec(ks_ctx *ctx, long long n, const Op &op_in, Stop stop, int slot = 0) {
   long long need = (n + kThreads - 1) / kThreads;
@@ -400,6 +451,7 @@ inline void launch_vec(ks_ctx *ctx, long long n, const Op &op_in, Stop stop, int
   if (need < grid) grid = (int)(need > 0 ? need : 1);
   with_rank_sums(ctx, op_in, stop, [&](const auto &op) {
     using O = std::decay_t<decltype(op)>;
+    ctx->next_class = vec_class<O>();
     launch_k(ctx, vec_kernel<O>, dim3(grid), dim3(kThreads), 0, op, n, stop, red_of(ctx, slot));
   });
 }

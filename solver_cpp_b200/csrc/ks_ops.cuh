@@ -200,12 +200,14 @@ inline ks_status launch_block_dot(ks_ctx *ctx, const VT *V, long long ld, int k,
   dim3 grid(groups, gx);
   if (ctx->red_comm) {  // split solve: results summed over the ranks, then put
     if (NW * k > kStageLen) return set_error(ctx, KS_BAD_INPUT, "block dot: too many results for a split solve");
+    ctx->next_class = kDot;
     launch_k(ctx, block_dot_kernel<NW, VT, StagePuts<Epi>>, grid, dim3(kThreads), 0, V, ld, k, W0, W1, n,
              StagePuts<Epi>{ctx->d_stage, k}, stop, ctx->partials, ctx->counters + 16);
     note_dist(ctx, ctx->red_comm->allreduce(ctx->d_stage, NW * k));
     launch_scalar(ctx, PutSummed<Epi>{epi, ctx->d_stage, NW, k}, stop);
     return KS_OK;
   }
+  ctx->next_class = kDot;
   launch_k(ctx, block_dot_kernel<NW, VT, Epi>, grid, dim3(kThreads), 0, V, ld, k, W0, W1, n, epi, stop,
            ctx->partials, ctx->counters + 16);
   return KS_OK;

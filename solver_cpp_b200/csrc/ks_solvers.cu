@@ -56,6 +56,7 @@ struct Env {
   // row-split solve: the transport and the halo plans of A and AT
   ks_comm *comm = nullptr;
   const HaloPlan *planA = nullptr, *planT = nullptr;
+  bool true_check = false;  // VP outer methods: FP64 true-residual check before converging
   Stop stop() const { return Stop{&st->k.done, outer_done}; }
   // Fill the halo of an SpMV input from the peers (it is written, though
   // the method treats the vector as read-only: the halo is not its data).
@@ -166,6 +167,7 @@ template <class VT>
 struct ZeroOp {
   VT *x;
   static constexpr int ND = 0;
+  static constexpr bool kMemset = true;
   __device__ void elem(long long i, double (&)[1]) const { x[i] = (VT)0; }
   __device__ void finish(const double (&)[1]) const {}
 };
@@ -554,6 +556,71 @@ ks_status init_state(const Env<VT> &E, const VT *b) {
   launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
   launch_vec(E.ctx, E.n, NormBOp<VT>{b, E.st}, Stop{nullptr, E.outer_done});
   return KS_OK;
+}
+
+// ------------------------------------------------------------------ true residual
+// A VP method that has stopped on its recurrence residual (vpcg.cpp:704-713
+// tests r, which drifts from b - A x in finite precision, the more so with an
+// FP32 inner solve) checks |b - A x| / |b| in FP64 before its convergence
+// stands (ks_params.true_residual). The check's SpMV writes the true residual
+// into r (residual replacement). If it passes the eps, the method stays
+// converged; otherwise it is marked running again and restarts from its
+// current x and r, its iteration count and history carrying on.
+template <class VT>
+struct TrueChkEpi {
+  using acc_t = VT;
+  const VT *b;
+  VT *r;
+  DevState *st;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    const VT rt = sub_rn(b[i], v);
+    r[i] = rt;
+    acc[0] = add_rn(acc[0], mul_rn(widen(rt), widen(rt)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    if (st->k.done != kConverged) return;
+    const double tr = sqrt(s[0]) / st->k.s[S_BNORM];
+    st->k.s[S_TRUECNT] += 1.0;
+    st->k.s[S_TRUERES] = tr;
+    if (!(tr <= st->k.s[S_EPS])) {
+      st->k.aux[A_FINAL] = 0;  // GMRES: the next stop assembles x again
+      set_done(st, kRunning);
+    }
+  }
+};
+
+struct SetDoneOp {
+  DevState *st;
+  int code;
+  __device__ void run() const {
+    if (st->k.done == kRunning) set_done(st, code);
+  }
+};
+
+// After the method's loop: the check, when it applies. Returns true when the
+// method has to go on (the host waits for the answer; this happens only when
+// the recurrence test has fired).
+template <class VT>
+inline bool true_check_continue(const Env<VT> &E, const VT *b, const VT *x, VT *r) {
+  if constexpr (!std::is_same<VT, double>::value) {
+    return false;  // VP methods run their outer loop in FP64
+  } else {
+  if (!E.true_check) return false;
+  E.halo(*E.A, x);
+  launch_spmv<double, double>(E.ctx, *E.A, x, TrueChkEpi<double>{b, r, E.st}, Stop{nullptr, nullptr});
+  int done = 0;
+  if (cudaMemcpyAsync(&done, &E.st->k.done, sizeof(int), cudaMemcpyDeviceToHost, E.ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(E.ctx->stream) != cudaSuccess)
+    return false;
+  return done == kRunning;
+  }
+}
+
+// No iteration left after a failed check: the method ends as out of loops.
+template <class VT>
+inline void true_check_exhausted(const Env<VT> &E) {
+  launch_scalar(E.ctx, SetDoneOp{E.st, kMaxLoop}, Stop{nullptr, nullptr});
 }
 
 // ------------------------------------------------------------------ iteration issue
@@ -1179,7 +1246,16 @@ ks_status run_gcr_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws
         break;
       }
     }
-    if (stop_host || (E.outer && P_.step()) || issued_steps >= E.sp.maxloop) break;
+    if (stop_host || (E.outer && P_.step()) || issued_steps >= E.sp.maxloop) {
+      // VPGCR: x is current after every step; a failed true-residual check
+      // restarts the cycles from it
+      if (!inner || !true_check_continue(E, b, (const VT *)x, r)) break;
+      if (issued_steps >= E.sp.maxloop) {
+        true_check_exhausted(E);
+        break;
+      }
+      stop_host = false;
+    }
   }
   return KS_OK;
 }
@@ -1380,6 +1456,7 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
   bool stop_host = false;
   const VT *B = inner ? Z : V;
   bool x_zero = true;  // the first cycle starts from x = 0
+ restart:
   while (!stop_host) {
     const StartEpi<VT> se{b, r, nullptr, nullptr, nullptr, E.st, START_NORM};
     if (x_zero)
@@ -1425,6 +1502,17 @@ ks_status run_gmres_core(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *d
   launch_basis(E.ctx, n, m - 1, GmUpdateOp<VT>{B, ld, 0, g.y, x, E.st, 1, E.faithful ? 1 : 0},
                Stop{nullptr, E.outer_done});
   launch_scalar(E.ctx, GmMarkFinal{E.st}, Stop{nullptr, E.outer_done});
+  // VPGMRES: x is assembled; a failed true-residual check starts a new cycle
+  // from it (the cycle start recomputes r = b - A x)
+  if (inner && true_check_continue(E, b, (const VT *)x, r)) {
+    if (issued >= E.sp.maxloop) {
+      true_check_exhausted(E);
+      return KS_OK;
+    }
+    stop_host = false;
+    P = Poller{E.ctx, E.hflag, E.lookahead};
+    goto restart;
+  }
   return KS_OK;
 }
 
@@ -1730,6 +1818,211 @@ template <class IT>
 ks_status run_method(int method, const Env<IT> &E, const IT *b, IT *x, IT *ws, double *dws,
                      InnerRunner<IT> *inner);
 
+// ------------------------------------------------------------------ fast inner CG
+// The FP32 (or BF16-valued) inner CG of a VP method on a one-GPU matrix with
+// a diagonal copy runs two kernels per iteration instead of three:
+//   K1(L): q = A p_L, with p_L = beta_L p_{L-1} + r formed in the SpMV's
+//          reads (GDir) and the row's own p_L stored; the x update of
+//          iteration L-1, x += alpha_{L-1} p_{L-1}, applied for the row
+//          (L = 1: x = 0); (p,q) -> alpha_L.
+//   K2(L): r -= alpha_L q; (r,r) -> beta_{L+1}; stopping test.
+// Nothing in the loop reads x (cg.cpp:211 is its only update), so applying
+// each update one kernel later changes no value: every element sees the same
+// FP32 operations in the same order as in the three-kernel loop (XpbyToOp,
+// XrUpdOp). The update still pending when the loop stops (alpha_L p_L, when
+// K2(L) stopped it) is applied by the kernel that hands z back to the outer
+// method. The loop's vectors are r, q, two direction slots and x: five FP32
+// vectors that the streamed matrix leaves in L2. The start (r = (float) b,
+// (r,r), the state reset) and the end (z = (double) x) fuse into the outer
+// method's own kernels where the outer method is VPCG.
+
+// K1 epilogue (see above). `first`: iteration 1, where pold = r and beta = 0.
+template <class VT>
+struct CgInMvEpi {
+  using acc_t = VT;
+  const VT *pold;
+  const VT *r;
+  VT *p;
+  VT *q;
+  VT *x;
+  DevState *st;
+  int first;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT v, double (&acc)[1]) const {
+    const VT b = (VT)rd(&st->k.s[S_BETA]);
+    const VT po = pold[i];
+    const VT pi = add_rn(mul_rn(b, po), r[i]);
+    p[i] = pi;
+    q[i] = v;
+    x[i] = first ? (VT)0 : add_rn(mul_rn((VT)rd(&st->k.s[S_ALPHA]), po), x[i]);
+    acc[0] = add_rn(acc[0], mul_rn(widen(pi), widen(v)));
+  }
+  // Runs after every CTA has finished its rows, so no row reads the new
+  // alpha_L in place of alpha_{L-1}.
+  __device__ void finish(const double (&s)[1]) const {
+    st->k.aux[A_PENDING] = 0;
+    st->k.aux[A_XZERO] = 0;
+    st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], s[0]);
+  }
+};
+
+// K2: r -= alpha q; (r,r) -> beta, check (XrUpdOp mode 0 without x);
+// alpha_L p_L is now pending, p_L in slot (L - 1) % 2.
+template <class VT>
+struct CgInRUpdOp {
+  VT *r;
+  const VT *q;
+  DevState *st;
+  long long L;
+  static constexpr int ND = 1;
+  struct Regs {
+    VT q, r;
+  };
+  __device__ Regs load(long long i) const { return {q[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
+    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
+    const VT ri = add_rn(mul_rn((VT)(-a), g.q), g.r);
+    r[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    st->k.aux[A_PENDING] = 1;
+    st->k.aux[A_KIDX] = L;
+    st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
+    st->k.s[S_RR] = s[0];
+    check_top(st, st->k.loop + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
+  }
+};
+
+// The inner state's reset (InitOp without history) and the top of iteration 1
+// (StartZeroOp with START_CG, x = 0): |b| and (r,r) are the same sum.
+__device__ __forceinline__ void inner_cg_start(DevState *st, double eps, long long maxloop, double rr) {
+  st->k.done = kRunning;
+  st->k.loop = 0;
+  st->k.hlen = 0;
+  st->k.s[S_EPS] = eps;
+  st->k.aux[A_MAXLOOP] = maxloop;
+  st->k.aux[A_RECORD] = 0;
+  st->k.aux[A_CONVK] = 0;
+  st->k.aux[A_FINAL] = 0;
+  st->k.aux[A_PENDING] = 0;
+  st->k.aux[A_XZERO] = 1;
+  st->k.s[S_BETA] = 0.0;
+  st->k.s[S_BNORM] = sqrt(rr);
+  st->k.s[S_RR] = rr;
+  check_top(st, 1, sqrt(rr) / st->k.s[S_BNORM]);
+}
+
+// Inner start from an outer vector b: r = (VT) b (ConvertOp), (r,r).
+template <class VT>
+struct CgInStartOp {
+  const double *b;
+  VT *r;
+  DevState *st;
+  double eps;
+  long long maxloop;
+  static constexpr int ND = 1;
+  struct Regs {
+    double b;
+  };
+  __device__ Regs load(long long i) const { return {b[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
+    const VT ri = (VT)g.b;
+    r[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[1]) const { inner_cg_start(st, eps, maxloop, s[0]); }
+};
+
+// Inner end: z = (double) x_final, x_final = x + alpha_K p_K when an update is
+// pending (ConvertOp of the three-kernel loop's x). mode 1 / 2 also fuse
+// VPCG's RzOp (init / beta) over the outer r and z on the outer state.
+template <class VT>
+struct CgInFinalOp {
+  const VT *x;
+  const VT *P0;
+  const VT *P1;
+  const DevState *ist;
+  double *z;
+  const double *r;
+  DevState *ost;
+  int mode;
+  static constexpr int ND = 1;
+  struct Regs {
+    VT x, p;
+    double r;
+  };
+  __device__ Regs load(long long i) const {
+    const long long K = __ldg(&ist->k.aux[A_KIDX]);
+    const VT *p = (K - 1) & 1 ? P1 : P0;
+    return {x[i], __ldg(&ist->k.aux[A_PENDING]) ? p[i] : (VT)0, mode ? r[i] : 0.0};
+  }
+  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
+    VT xf = __ldg(&ist->k.aux[A_XZERO]) ? (VT)0 : g.x;
+    if (__ldg(&ist->k.aux[A_PENDING])) xf = add_rn(mul_rn((VT)__ldg(&ist->k.s[S_ALPHA]), g.p), xf);
+    const double zi = (double)xf;
+    z[i] = zi;
+    acc[0] = add_rn(acc[0], mul_rn(g.r, zi));
+  }
+  __device__ void finish(const double (&s)[1]) const {
+    if (mode == 2) ost->k.s[S_BETA] = rdiv(ost, s[0], ost->k.s[S_RR]);
+    if (mode) ost->k.s[S_RR] = s[0];
+  }
+};
+
+// VPCG's outer x/r update (XrUpdOp mode 1) fused with the start of the next
+// fast inner solve from the new r: (r,r) in FP64 for the outer stopping
+// test, r rounded to the inner precision and its (r,r) for the inner start.
+template <class IT>
+struct VpXrStartOp {
+  double *x;
+  double *r;
+  const double *p;
+  const double *q;
+  DevState *st;
+  IT *ri;
+  DevState *ist;
+  double ieps;
+  long long imaxloop;
+  static constexpr int ND = 2;
+  struct Regs {
+    double x, p, q, r;
+  };
+  __device__ Regs load(long long i) const { return {x[i], p[i], q[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[2]) const {
+    const double a = rd(&st->k.s[S_ALPHA]);
+    x[i] = add_rn(mul_rn(a, g.p), g.x);
+    const double rn = add_rn(mul_rn(-a, g.q), g.r);
+    r[i] = rn;
+    acc[0] = add_rn(acc[0], mul_rn(rn, rn));
+    const IT r32 = (IT)rn;
+    ri[i] = r32;
+    acc[1] = add_rn(acc[1], mul_rn(widen(r32), widen(r32)));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    check_top(st, st->k.loop + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
+    inner_cg_start(ist, ieps, imaxloop, s[1]);
+  }
+};
+
+// The fast inner loop's buffers, carved from the inner workspace.
+template <class VT>
+struct InnerCgBufs {
+  VT *r, *q, *P0, *P1, *x;
+  VT *slot(long long L) const { return ((L - 1) & 1) ? P1 : P0; }
+};
+
+// Iterations 1..maxloop of the fast inner CG (start already issued).
+template <class VT>
+inline void run_cg_inner_loop(const Env<VT> &E, const InnerCgBufs<VT> &B) {
+  for (long long L = 1; L <= E.sp.maxloop; L++) {
+    const VT *pold = L == 1 ? B.r : B.slot(L + 1);
+    mv_g(E, *E.A, GDir<VT>{pold, B.r, &E.st->k.s[S_BETA], (VT)0},
+         CgInMvEpi<VT>{pold, B.r, B.slot(L), B.q, B.x, E.st, L == 1 ? 1 : 0});
+    vec(E, CgInRUpdOp<VT>{B.r, B.q, E.st, L});
+  }
+}
+
 template <class VT>
 struct InnerRunner {
   // Outer-precision view (VT) and the inner environment.
@@ -1745,8 +2038,29 @@ struct InnerRunner {
   float *b32 = nullptr, *z32 = nullptr;
   long long calls = 0;
   ks_status status = KS_OK;
+  // fast inner CG (see above): chosen at set-up
+  bool fast_cg = false;
+  InnerCgBufs<float> fb{};
+  void setup_fast();
   void solve(const VT *b, VT *z);
 };
+
+// The fast inner CG applies where the inner method is CG in FP32 or with BF16
+// values, on one GPU, and the SpMV reads a diagonal copy of those values.
+template <class VT>
+void InnerRunner<VT>::setup_fast() {
+  fast_cg = false;
+  if (method != KS_CG || iprec == KS_FP64 || E32.comm || !E32.A || !E32.A->dia_nd) return;
+  if (iprec == KS_FP32 ? !E32.A->dia_val32 : !E32.A->dia_val16) return;
+  if (vec_count(KS_CG, E32.sp, E32.n, sizeof(float), ctx->l2_bytes) < 4) return;
+  Ws<float> W{ws32, E32.ld, E32.off};
+  fb.r = W.take();
+  fb.q = W.take();
+  fb.P0 = W.take();
+  fb.P1 = W.take();
+  fb.x = z32;
+  fast_cg = true;
+}
 
 template <class VT>
 void InnerRunner<VT>::solve(const VT *b, VT *z) {
@@ -1755,6 +2069,11 @@ void InnerRunner<VT>::solve(const VT *b, VT *z) {
   if constexpr (std::is_same<VT, double>::value) {
     if (iprec == KS_FP64) {
       status = run_method<double>(method, E64, b, z, ws64, dws, nullptr);
+    } else if (fast_cg) {
+      const Stop os{nullptr, E32.outer_done};
+      launch_vec(ctx, n, CgInStartOp<float>{b, fb.r, E32.st, E32.sp.eps, E32.sp.maxloop}, os);
+      run_cg_inner_loop(E32, fb);
+      launch_vec(ctx, n, CgInFinalOp<float>{fb.x, fb.P0, fb.P1, E32.st, z, nullptr, nullptr, 0}, os);
     } else {
       launch_vec(ctx, n, ConvertOp<double, float>{b, b32}, Stop{nullptr, E32.outer_done});
       status = run_method<float>(method, E32, b32, z32, ws32, dws, nullptr);
@@ -1793,17 +2112,65 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
-  inner->solve(r, z);
-  vec(E, CopyOp<VT>{z, p});
-  vec(E, RzOp<VT>{r, z, E.st, 1});
-  Poller P{E.ctx, E.hflag, E.lookahead};
-  for (long long L = 1; L <= E.sp.maxloop; L++) {
+  // vpcg.cpp:659-750. With the fast inner CG its start is fused into the
+  // outer x/r update and its end into (r, z).
+  bool fast = false;
+  if constexpr (std::is_same<VT, double>::value) fast = inner->fast_cg;
+  // z = M r, rr = (r, z), p = z: the method's start, and its restart after a
+  // failed true-residual check (r then holds b - A x)
+  auto start = [&]() {
+    if constexpr (std::is_same<VT, double>::value) {
+      if (fast) {
+        InnerRunner<double> &I = *inner;
+        const Env<float> &F = I.E32;
+        const Stop os{nullptr, F.outer_done};
+        I.calls++;
+        launch_vec(E.ctx, E.n, CgInStartOp<float>{r, I.fb.r, F.st, F.sp.eps, F.sp.maxloop}, os);
+        run_cg_inner_loop(F, I.fb);
+        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, I.fb.P0, I.fb.P1, F.st, z, r, E.st, 1}, os);
+        vec(E, CopyOp<VT>{z, p});
+        return;
+      }
+    }
+    inner->solve(r, z);
+    vec(E, CopyOp<VT>{z, p});
+    vec(E, RzOp<VT>{r, z, E.st, 1});
+  };
+  auto iteration = [&]() {
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, mvv, E.st});
+    if constexpr (std::is_same<VT, double>::value) {
+      if (fast) {
+        InnerRunner<double> &I = *inner;
+        const Env<float> &F = I.E32;
+        I.calls++;
+        vec(E, VpXrStartOp<float>{x, r, p, mvv, E.st, I.fb.r, F.st, F.sp.eps, F.sp.maxloop});
+        run_cg_inner_loop(F, I.fb);
+        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, I.fb.P0, I.fb.P1, F.st, z, r, E.st, 2},
+                   Stop{nullptr, F.outer_done});
+        vec(E, XpbyOp<VT>{p, z, &E.st->k.s[S_BETA]});
+        return;
+      }
+    }
     vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
     inner->solve(r, z);
     vec(E, RzOp<VT>{r, z, E.st, 0});
     vec(E, XpbyOp<VT>{p, z, &E.st->k.s[S_BETA]});
-    if (P.step()) break;
+  };
+  start();
+  long long issued = 0;
+  for (;;) {
+    Poller P{E.ctx, E.hflag, E.lookahead};
+    while (issued < E.sp.maxloop) {
+      iteration();
+      issued++;
+      if (P.step()) break;
+    }
+    if (!true_check_continue(E, b, x, r)) break;
+    if (issued >= E.sp.maxloop) {
+      true_check_exhausted(E);
+      break;
+    }
+    start();
   }
   return KS_OK;
 }
@@ -1841,16 +2208,30 @@ ks_status run_vpcr(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
-  inner->solve(r, z);
-  vec(E, CopyOp<VT>{z, p});
-  mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, Ap, E.st, 1});
-  Poller P{E.ctx, E.hflag, E.lookahead};
-  for (long long L = 1; L <= E.sp.maxloop; L++) {
-    vec(E, XrUpdOp<VT>{x, r, p, Ap, E.st, 1});
+  // vpcr.cpp:670-775; start() also restarts after a failed true-residual check
+  auto start = [&]() {
     inner->solve(r, z);
-    mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, nullptr, E.st, 0});
-    vec(E, Xpby2Op<VT>{p, z, Ap, Av, E.st, 1});
-    if (P.step()) break;
+    vec(E, CopyOp<VT>{z, p});
+    mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, Ap, E.st, 1});
+  };
+  start();
+  long long issued = 0;
+  for (;;) {
+    Poller P{E.ctx, E.hflag, E.lookahead};
+    while (issued < E.sp.maxloop) {
+      vec(E, XrUpdOp<VT>{x, r, p, Ap, E.st, 1});
+      inner->solve(r, z);
+      mv(E, *E.A, (const VT *)z, VpcrMvEpi<VT>{z, Av, nullptr, E.st, 0});
+      vec(E, Xpby2Op<VT>{p, z, Ap, Av, E.st, 1});
+      issued++;
+      if (P.step()) break;
+    }
+    if (!true_check_continue(E, b, x, r)) break;
+    if (issued >= E.sp.maxloop) {
+      true_check_exhausted(E);
+      break;
+    }
+    start();
   }
   return KS_OK;
 }
@@ -1901,11 +2282,33 @@ struct Alloc {  // RAII for pool buffers
   }
 };
 
+// out[0] = |x - y|^2, out[1] = |y|^2 (the report's x_rel_diff).
+struct DiffNormOp {
+  const double *x;
+  const double *y;
+  double *out;
+  static constexpr int ND = 2;
+  struct Regs {
+    double x, y;
+  };
+  __device__ Regs load(long long i) const { return {x[i], y[i]}; }
+  __device__ void store(long long, const Regs &g, double (&acc)[2]) const {
+    const double d = sub_rn(g.x, g.y);
+    acc[0] = add_rn(acc[0], mul_rn(d, d));
+    acc[1] = add_rn(acc[1], mul_rn(g.y, g.y));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    out[0] = s[0];
+    out[1] = s[1];
+  }
+};
+
 __global__ void k_copy_state(const DevState *st, long long *out) {
   out[0] = st->k.done;
   out[1] = st->k.loop;
   out[2] = st->k.hlen;
   out[3] = st->k.aux[A_CONVK];
+  out[4] = (long long)st->k.s[S_TRUECNT];
 }
 
 }  // namespace ks
@@ -1940,6 +2343,10 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   if (prm->x_update < 0 || prm->x_update > 2) return set_error(ctx, KS_BAD_INPUT, "x_update must be 0, 1 or 2");
   if (prm->cluster_solve < 0 || prm->cluster_solve > 1)
     return set_error(ctx, KS_BAD_INPUT, "cluster_solve must be 0 or 1");
+  if (prm->inner_fast < 0 || prm->inner_fast > 1) return set_error(ctx, KS_BAD_INPUT, "inner_fast must be 0 or 1");
+  if (prm->true_residual < 0 || prm->true_residual > 2)
+    return set_error(ctx, KS_BAD_INPUT, "true_residual must be 0, 1 or 2");
+  if (prm->profile < 0 || prm->profile > 1) return set_error(ctx, KS_BAD_INPUT, "profile must be 0 or 1");
   if ((outer == KS_GCR || outer == KS_GMRES || outer == KS_VPGCR || outer == KS_VPGMRES) &&
       (outer_sp.restart < 1 || outer_sp.restart > 1024))
     return set_error(ctx, KS_BAD_INPUT, "restart must be in [1, 1024]");
@@ -2018,6 +2425,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     E.planT = trans ? &dist->planA : &dist->planT;
   }
   E.hflag = (volatile int *)ctx->h_flags;
+  E.true_check = vp && (prm->true_residual == 1 || (prm->true_residual == 0 && ip != KS_FP64));
   E.lookahead = prm->poll_interval > 0 ? prm->poll_interval : (vp ? 2 : 8);
   E.lookahead = std::min(E.lookahead, ctx->nflags - 1);  // event ring size
   if (!ctx->h_flags || !st) return KS_CUDA_ERROR;
@@ -2063,9 +2471,19 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
       KS_TRY(al.get((size_t)ld, &IR.z32));
       IR.b32 += off;
       IR.z32 += off;
+      if (prm->inner_fast == 0) IR.setup_fast();
     }
   }
 
+  // per-class device times (ks_params.profile)
+  struct ProfScope {
+    ks_ctx *c;
+    ProfScope(ks_ctx *c_, bool on) : c(c_) {
+      c->prof_on = on ? 1 : 0;
+      c->prof_class.clear();
+    }
+    ~ProfScope() { c->prof_on = 0; }
+  } prof(ctx, prm->profile == 1);
   KS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
   ks_status s = run_method<double>(outer, E, b, xs, ws, dws, vp ? &IR : nullptr);
   if (s == KS_OK && vp) s = IR.status;
@@ -2085,9 +2503,9 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   }
   KS_CUDA(ctx, cudaGetLastError());
   long long *d_out = nullptr;
-  KS_TRY(al.get(4, &d_out));
+  KS_TRY(al.get(5, &d_out));
   k_copy_state<<<1, 1, 0, ctx->stream>>>(st, d_out);
-  long long hs[4];
+  long long hs[5];
   KS_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, d_out, sizeof(hs), cudaMemcpyDeviceToHost, ctx->stream));
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(hs, ctx->h_pinned, sizeof(hs));
@@ -2139,6 +2557,29 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     rep->spmv_count = 0;
     rep->true_res_log10 = 0.0;
     rep->true_rel_res = 0.0;
+    rep->x_rel_diff = -1.0;
+    rep->true_residual_checks = hs[4];
+    rep->t_mv = rep->t_dot = rep->t_other = rep->t_memset = rep->t_h2d = rep->t_d2h = 0.0;
+    if (prm->profile == 1) {  // the stream is synchronised: every event has completed
+      double t[kNumClasses] = {0, 0, 0, 0};
+      for (size_t i = 0; i < ctx->prof_class.size(); i++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->prof_events[2 * i], ctx->prof_events[2 * i + 1]) == cudaSuccess)
+          t[ctx->prof_class[i]] += ms * 1e-3;
+        else
+          (void)cudaGetLastError();
+      }
+      rep->t_mv = t[kMv];
+      rep->t_dot = t[kDot];
+      rep->t_other = t[kOther];
+      rep->t_memset = t[kMemset];
+    }
+    if (prm->x_ref && !dist) {  // |x - x_ref| / |x_ref| over the solution
+      launch_vec(ctx, n, DiffNormOp{x, prm->x_ref, ctx->d_result}, Stop{nullptr, nullptr});
+      double s2[2];
+      KS_CUDA(ctx, cudaMemcpy(s2, ctx->d_result, sizeof(s2), cudaMemcpyDeviceToHost));
+      rep->x_rel_diff = s2[1] > 0.0 ? std::sqrt(s2[0]) / std::sqrt(s2[1]) : (s2[0] > 0.0 ? INFINITY : 0.0);
+    }
     if (dist) {  // summed over the ranks after the solve
       double s2[2];
       KS_CUDA(ctx, cudaMemcpy(s2, ctx->d_result, sizeof(s2), cudaMemcpyDeviceToHost));
@@ -2221,11 +2662,28 @@ ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solv
   vb.type = vx.type = KS_FP64;
   vb.d = buf;
   vx.d = (char *)buf + ((sizeof(double) * (size_t)n + 255) / 256) * 256;
+  // with params->profile the copies are timed too (the times report's H2D / D2H)
+  const bool prof = params && params->profile == 1 && report;
+  float up_ms = 0.f, down_ms = 0.f;
+  if (prof) cudaEventRecord(ctx->ev_start, ctx->stream);
   ks_status r = ks_vec_upload(&vb, b);
+  if (prof) {
+    cudaEventRecord(ctx->ev_stop, ctx->stream);
+    cudaEventSynchronize(ctx->ev_stop);
+    cudaEventElapsedTime(&up_ms, ctx->ev_start, ctx->ev_stop);
+  }
   if (r == KS_OK) {
     r = ks_solve(ctx, mat, outer, inner, params, &vb, &vx, hist_iter, hist_err, hist_cap, report);
     if (r == KS_OK || r == KS_NOT_CONVERGED || r == KS_BREAKDOWN || r == KS_NAN_DETECTED) {
+      if (prof) cudaEventRecord(ctx->ev_start, ctx->stream);
       const ks_status d = ks_vec_download(&vx, x);
+      if (prof) {
+        cudaEventRecord(ctx->ev_stop, ctx->stream);
+        cudaEventSynchronize(ctx->ev_stop);
+        cudaEventElapsedTime(&down_ms, ctx->ev_start, ctx->ev_stop);
+        report->t_h2d = up_ms * 1e-3;
+        report->t_d2h = down_ms * 1e-3;
+      }
       if (d != KS_OK) r = d;
     }
   }

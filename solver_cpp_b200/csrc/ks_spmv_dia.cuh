@@ -3,16 +3,23 @@
 // Matrices of structured grids (5- and 7-point stencils, upwind
 // convection-diffusion) hold every row's columns at a handful of fixed
 // offsets from the row. Stored diagonal-major, the SpMV needs no column
-// indices or row offsets at all: per nonzero only its value (plus one mask
-// byte per row), against value + int16 offset + a share of the row offsets in
-// CSR. Thread i computes row i: for each diagonal d whose bit is set in the
-// row's mask it adds val[d][i] * x[i + off[d]], diagonals in ascending offset
-// order, which is the row's CSR column order, from 0.0 with separately
-// rounded products and sums: the same sums as blas::MtxVec_mult
-// (blas.cpp:56-62), bit for bit. A warp reads 32 consecutive values of each
-// diagonal and 32 consecutive entries of x per diagonal (coalesced; x is
-// shared by the diagonals through L1/L2). Matrix data is read with the
-// streaming hint, so the Krylov vectors keep their place in L2.
+// indices or row offsets at all: per nonzero only its value (plus, for FP64,
+// one mask byte per row), against value + int16 offset + a share of the row
+// offsets in CSR. A symmetric matrix keeps only its main and upper diagonals:
+// a lower term A[i][i-o] is read as its mirror A[i-o][i], the same stream
+// shifted back by o rows, which the CTAs working o rows behind have just
+// pulled into L2 (4 instead of 7 value streams for a 7-point stencil).
+// Thread i computes row i: for each diagonal d it adds val[d][i] *
+// x[i + off[d]], diagonals in ascending offset order, which is the row's CSR
+// column order, from 0.0 with separately rounded products and sums: the same
+// sums as blas::MtxVec_mult (blas.cpp:56-62), bit for bit. FP64 adds only the
+// terms the row's mask names. FP32 and BF16 add every diagonal: an absent
+// entry is a stored zero, and 0 * x (x finite) added to a sum that started at
+// +0.0 leaves it unchanged bit for bit, so the mask byte is not read. A warp
+// reads 32 consecutive values of each diagonal and 32 consecutive entries of
+// x per diagonal (coalesced; x is shared by the diagonals through L1/L2).
+// Matrix data is read with the streaming hint, so the Krylov vectors keep
+// their place in L2.
 #pragma once
 
 #include "ks_spmv_tma.cuh"
@@ -21,8 +28,12 @@ namespace ks {
 
 template <class MT>
 struct DiaT {
-  const MT *__restrict__ val;              // nd * n, diagonal-major
-  const unsigned char *__restrict__ mask;  // n
+  // Diagonal d's element of row i is vb[d][i + vs[d]]: the full layout has
+  // vs = 0; the symmetric half reads a lower diagonal from its upper mirror,
+  // shifted by the (negative) offset into its zero pad.
+  const MT *vb[kMaxDiag];
+  int vs[kMaxDiag];
+  const unsigned char *__restrict__ mask;  // n; null: every diagonal's term is added
   int n;
   int nd;
   int cmin, cmax;  // columns that exist in x (a split rank's window: beyond its rows)
@@ -59,13 +70,13 @@ __global__ void __launch_bounds__(kThreads) spmv_dia_kernel(DiaT<MT> D, GX gx0, 
   if (stop()) return;
   const GX g0 = gx0.prep(), g1 = gx1.prep();
   for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < D.n; i += stride) {
-    const unsigned m = __ldcs(D.mask + i);
+    const unsigned m = D.mask ? (unsigned)__ldcs(D.mask + i) : 0xffu;
     MT a[K];
     AT x0[K], x1[NV == 2 ? K : 1];
 #pragma unroll
     for (int d = 0; d < K; d++) {
       if (NDG > 0 || d < nd) {
-        a[d] = ld_stream(D.val + (size_t)d * (size_t)D.n + i);
+        a[d] = ld_stream(D.vb[d] + (i + D.vs[d]));
         const int c = min(max(i + D.off[d], D.cmin), D.cmax - 1);
         x0[d] = g0.template get<AT>(c);
         if constexpr (NV == 2) x1[d] = g1.template get<AT>(c);

@@ -89,12 +89,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: false if the phase did not complete within kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Bounded wait: false if the phase did not complete within `limit` ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          unsigned long long limit = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (global_ns() - t0 > kWaitLimitNs) return false;
+    if (global_ns() - t0 > limit) return false;
   }
   return true;
 }
@@ -168,7 +169,8 @@ struct GPtr {
 // GX. Epi::row(r, y) for NV = 1, Epi::row(r, y0, y1) for NV = 2 (with acc).
 template <int NV, class MT, class IT, class GX, class Epi>
 __global__ void __launch_bounds__(kThreads)
-    spmv_tma_kernel(CsrT<MT, IT> A, GX gx0, GX gx1, Epi epi, Stop stop, Red red, int *err) {
+    spmv_tma_kernel(CsrT<MT, IT> A, GX gx0, GX gx1, Epi epi, Stop stop, Red red, int *err,
+                    unsigned long long wait_ns) {
   using AT = typename Epi::acc_t;
   using SB = StageBuf<MT, IT>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     const int s = consumed % kStages;
     const uint32_t parity = (uint32_t)((consumed / kStages) & 1);
-    const bool ok = mbar_wait(&bars[s], parity);
+    const bool ok = mbar_wait(&bars[s], parity, wait_ns);
     // One decision for the whole CTA: a thread whose wait ran out must not
     // leave the others behind at a barrier.
     if (__syncthreads_or(!ok)) {
@@ -307,7 +309,8 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   if (failed) {
-    // copies still in flight: one more bounded wait on each, then finish
+    // copies still in flight: one more bounded wait on each (the default
+    // limit, whatever limit ended the loop), then finish
     for (int c = consumed; c < staged; c++) mbar_wait(&bars[c % kStages], (uint32_t)((c / kStages) & 1));
   }
   __syncthreads();

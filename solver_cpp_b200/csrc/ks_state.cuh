@@ -17,6 +17,8 @@ enum Slot : int {
   S_BETA = 4,
   S_T = 5,      // GMRES: current norm
   S_GAMMA = 6,  // k-skip
+  S_TRUECNT = 8,  // VP methods: FP64 true-residual checks made
+  S_TRUERES = 9,  // the last one's |b - A x| / |b|
 };
 enum Aux : int { A_MAXLOOP = 0, A_RECORD = 1, A_SPMV = 2, A_CONVK = 3, A_FINAL = 4, A_KIDX = 5, A_PENDING = 6, A_XZERO = 7 };
 

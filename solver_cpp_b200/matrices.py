@@ -285,32 +285,57 @@ def config_problem(name: str, size: int | None = None):
     return A, np.ascontiguousarray(b, dtype=np.float64), {"name": name, "grid": nx}
 
 
-def _write_lines(path, header, columns, fmts):
-    """Write a header and whitespace-separated columns in bounded chunks."""
+_LINES_PER_CHUNK = 1 << 20
+
+
+def _format_chunk(fmt, cols):
+    """Text of the rows of one chunk (module level: runs in worker processes)."""
+    block = np.column_stack(cols) if len(cols) > 1 else cols[0][:, None]
+    return "".join(fmt % tuple(row) for row in block.tolist())
+
+
+def _write_lines(path, header, columns, fmts, pool=None):
+    """Write a header and whitespace-separated columns in bounded chunks;
+    with a process pool the chunks are formatted in parallel and written in
+    order."""
+    fmt = " ".join(fmts) + "\n"
+    n = columns[0].shape[0]
+    spans = [(s, min(n, s + _LINES_PER_CHUNK)) for s in range(0, n, _LINES_PER_CHUNK)]
     with open(path, "w") as f:
         f.write(header)
-        n = columns[0].shape[0]
-        step = 1 << 20
-        fmt = " ".join(fmts) + "\n"
-        for s in range(0, n, step):
-            e = min(n, s + step)
-            block = np.column_stack([c[s:e] for c in columns]) if len(columns) > 1 else columns[0][s:e, None]
-            f.write("".join(fmt % tuple(row) for row in block.tolist()))
+        if pool is None:
+            for s, e in spans:
+                f.write(_format_chunk(fmt, [c[s:e] for c in columns]))
+        else:
+            futs = [pool.submit(_format_chunk, fmt, [c[s:e] for c in columns]) for s, e in spans]
+            for fu in futs:
+                f.write(fu.result())
 
 
-def write_crs(directory: str, A: CSR, b: np.ndarray, x: np.ndarray | None = None) -> None:
+def write_crs(directory: str, A: CSR, b: np.ndarray, x: np.ndarray | None = None, workers: int = 1) -> None:
     """Write ``ColVal.txt``, ``Ptr.txt`` and ``bx.txt`` in the reference format.
 
     Values are written with 17 significant digits so ``fscanf("%le")`` reads
-    back the identical doubles.
+    back the identical doubles. ``workers`` > 1 formats the text in that many
+    processes (started with ``spawn``).
     """
     os.makedirs(directory, exist_ok=True)
     n, nnz = A.n, A.nnz
     header = f"{n} {n} {nnz}\n"
     x = np.zeros(n) if x is None else x
-    _write_lines(os.path.join(directory, "ColVal.txt"), header, [A.col, A.val], ["%d", "%.17e"])
-    _write_lines(os.path.join(directory, "Ptr.txt"), header, [A.ptr], ["%d"])
-    _write_lines(os.path.join(directory, "bx.txt"), header, [b, x], ["%.17e", "%.17e"])
+    pool = None
+    if workers > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+
+        pool = ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"))
+    try:
+        _write_lines(os.path.join(directory, "ColVal.txt"), header, [A.col, A.val], ["%d", "%.17e"], pool)
+        _write_lines(os.path.join(directory, "Ptr.txt"), header, [A.ptr], ["%d"], pool)
+        _write_lines(os.path.join(directory, "bx.txt"), header, [b, x], ["%.17e", "%.17e"], pool)
+    finally:
+        if pool is not None:
+            pool.shutdown()
 
 
 def read_crs(directory: str):

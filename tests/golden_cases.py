@@ -18,6 +18,21 @@ def load(case_id):
     return meta, {k: d[k] for k in d.files}
 
 
+def index_large():
+    """Full-size fixtures (make_golden.py --large); empty when absent."""
+    path = os.path.join(GOLDEN, "index_large.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        return json.load(f)
+
+
+def load_large(case_id):
+    meta = index_large()[case_id]
+    d = np.load(os.path.join(GOLDEN, f"{case_id}.npz"))
+    return meta, {k: d[k] for k in d.files}
+
+
 def rel_close(a, b, rtol):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)

@@ -34,7 +34,8 @@ def test_abi_version_and_status_strings(ks):
     from solver_cpp_b200 import _abi
 
     lib = ks.lib()
-    assert lib.ks_abi_version() == _abi.ABI_VERSION == 3  # 2: ks_params.x_update; 3: cluster_solve
+    # 2: ks_params.x_update; 3: cluster_solve; 4: inner_fast, true_residual, profile, x_ref
+    assert lib.ks_abi_version() == _abi.ABI_VERSION == 4
     assert b"not converged" in lib.ks_status_string(2)
     assert b"not implemented" in lib.ks_status_string(99)
 
@@ -115,4 +116,10 @@ def test_bench_reference_arm_json(ks, tmp_path):
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "cpu_baseline", "e2e",
               "config"):
         assert k in d, k
+    # the value is one complete solve of the workload: the reference's 202
+    # CG iterations on the 64^2 system, its printed time
+    assert d["result"]["loop"] == 202 and d["result"]["converged"]
+    assert d["value"] == d["cpu_baseline"]["value"] > 0
+    # the reference arm maps no shared object of the product library
+    assert not [p for p in d["repo_objects_loaded"] if "libkrylov" in p], d["repo_objects_loaded"]
     assert d["value"] > 0 and d["cpu_baseline"]["kind"] == "reference" and d["config"]["workload"] == "c1_cg"

@@ -139,3 +139,46 @@ def test_cli_matrix_market_solve(cli, tmp_path):
     assert "converge" in r.stdout and "not converge" not in r.stdout
     x = np.loadtxt(os.path.join(rd, "output", "CG_xvec.txt"), ndmin=2)[:, 1]
     assert x.shape[0] == A.n and np.max(np.abs(x - 1.0)) < 1e-9  # b = A * 1
+
+
+def _data2csv_fields(log):
+    """The fields data2csv.sh's Seek() extracts from a run log, restated:
+    each is `grep PATTERN | head/tail -1 | cut -d ',' -f1 | sed 's/[^0-9.]//g'`
+    (and `cut -c 2-` for H2D / D2H)."""
+    lines = log.splitlines()
+
+    def grep(p):
+        return [ln for ln in lines if p in ln]
+
+    def num(ln, comma=True):
+        s = ln.split(",")[0] if comma else ln
+        return re.sub(r"[^0-9.]", "", s)
+
+    f = {"CUDA": grep("CUDA :")[0].split(":")[1].strip(), "MultiGPU": grep("MultiGPU :")[0].split(":")[1].strip()}
+    f["Total"] = num(grep("time")[0], comma=False)
+    f["Converge"] = grep("converge")
+    f["Loop"] = re.sub(r"[^0-9]", "", grep("loop")[0]) if len(grep("loop")) == 1 else None
+    f["CPU-Dot"], f["CPU-MV"] = num(grep("Dot")[0]), num(grep("MV")[0])
+    f["GPU-Dot"], f["GPU-MV"] = num(grep("Dot")[-1]), num(grep("MV")[-1])
+    f["GPU-H2D"], f["GPU-D2H"] = num(grep("H2D time")[0])[1:], num(grep("D2H time")[0])[1:]
+    f["GPU-Memset"] = num(grep("Memset")[0])
+    f["Other"] = num(grep("other")[0])
+    return f
+
+
+@pytest.mark.gpu
+def test_cli_times_report_parses_like_data2csv(cli, tmp_path):
+    """The log carries the reference's header and times report (times.cpp:44-76)
+    line for line: every field data2csv.sh reads is there and numeric, the
+    GPU Dot + MV + other add up to the solve time."""
+    A, b, rd = _problem_dir(tmp_path, "p3", "poisson3d", 24)
+    r = run(["-S", "cg", "-E", "1e-10", "-m", "p3", "-p", str(tmp_path)], rd)
+    assert r.returncode == 0, r.stderr
+    f = _data2csv_fields(r.stdout)
+    assert f["CUDA"] == "On" and f["MultiGPU"] == "Off"
+    assert f["Converge"] == ["converge"] and int(f["Loop"]) > 10
+    total = float(f["Total"])
+    vals = {k: float(f[k]) for k in ("CPU-Dot", "CPU-MV", "GPU-Dot", "GPU-MV", "GPU-H2D", "GPU-D2H", "GPU-Memset",
+                                       "Other")}
+    assert total > 0 and vals["GPU-MV"] > 0 and vals["GPU-Dot"] > 0 and vals["GPU-H2D"] > 0
+    assert vals["GPU-MV"] + vals["GPU-Dot"] + vals["Other"] == pytest.approx(total, rel=1e-3, abs=2e-6)

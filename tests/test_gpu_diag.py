@@ -123,3 +123,58 @@ def test_solves_identical_on_both_layouts(ks, ctx, prob, outer, inner, kw):
     d, c = res
     assert d.status == c.status and d.loop == c.loop
     assert np.array_equal(d.hist_err, c.hist_err) and np.array_equal(d.x, c.x)
+
+
+SYMMETRIC = [("poisson2d", 40, True), ("poisson3d", 12, True), ("varcoef3d", 12, True), ("varcoef2d", 40, True),
+             ("convdiff3d", 12, False), ("convdiff2d", 40, False)]
+
+
+@pytest.mark.parametrize("prob,g,sym", SYMMETRIC)
+def test_symmetric_matrices_keep_half_the_diagonals(ks, ctx, oracle, prob, g, sym):
+    """A matrix equal to its transpose bit for bit keeps only its main and
+    upper diagonals; its SpMV (lower terms read from the upper mirror) is
+    still the reference's bit for bit, and so is A^T's."""
+    A, _, _ = config_problem(prob, g)
+    M = ctx.matrix(A, transpose=True, fp32=True, bf16=True)
+    assert M.info()["dia_symmetric"] == (1 if sym else 0)
+    assert M.info()["t_dia_symmetric"] == (1 if sym else 0)
+    P = oracle.Problem(A)
+    x = np.random.default_rng(12).standard_normal(A.n)
+    X, Y = ctx.vector(x), ctx.vector(n=A.n)
+    for trans in (False, True):
+        ks.spmv(M, X, Y, trans=trans)
+        assert np.array_equal(Y.numpy(), oracle.spmv(P, x, transpose=trans))
+
+
+def test_almost_symmetric_matrix_keeps_every_diagonal(ks, ctx, oracle):
+    """One value off by one ulp: not symmetric, all 7 diagonals kept, SpMV exact."""
+    A, _, _ = config_problem("varcoef3d", 12)
+    val = A.val.copy()
+    j = int(A.ptr[500])  # the first (lowest) entry of row 500
+    val[j] = np.nextafter(val[j], np.inf)
+    B = CSR(A.ptr, A.col, val)
+    M = ctx.matrix(B, fp32=True)
+    assert M.info()["diagonals"] == 7 and M.info()["dia_symmetric"] == 0
+    x = np.random.default_rng(13).standard_normal(B.n)
+    X, Y = ctx.vector(x), ctx.vector(n=B.n)
+    ks.spmv(M, X, Y)
+    assert np.array_equal(Y.numpy(), oracle.spmv(oracle.Problem(B), x))
+
+
+@pytest.mark.parametrize("outer,inner,prec,kw", [
+    ("VPCG", "CG", "fp32", {}), ("VPCG", "CG", "bf16", {}), ("VPGMRES", "CG", "fp32", {"R": 20, "l": 10}),
+    ("VPGCR", "CG", "fp32", {"R": 20, "l": 10}), ("VPCR", "CG", "fp32", {"L": 40}),
+])
+def test_two_kernel_inner_cg_equals_three_kernel_loop(ks, ctx, outer, inner, prec, kw):
+    """The two-kernel inner CG (the SpMV forms the direction and applies the
+    previous x update) gives every element the three-kernel loop's values:
+    identical histories and solutions (16^3: both loops sum their dots in the
+    same order)."""
+    A, b, _ = config_problem("varcoef3d", 16)
+    M = ctx.matrix(A, transpose=True, fp32=True, bf16=True)
+    p = dict(E=1e-10, L=3000, l=20, e=1e-30, inner_precision=prec)
+    p.update(kw)
+    fast = ks.solve(ctx, M, outer, b, inner=inner, inner_fast=0, **p)
+    slow = ks.solve(ctx, M, outer, b, inner=inner, inner_fast=1, **p)
+    assert fast.status == slow.status and fast.loop == slow.loop
+    assert np.array_equal(fast.hist_err, slow.hist_err) and np.array_equal(fast.x, slow.x)

@@ -22,11 +22,54 @@ def test_mixed_vp_reaches_fp64_residual(ks, ctx, outer, inner, prec):
     A, b, _ = config_problem("varcoef3d", 20)
     M = ctx.matrix(A, transpose=True, fp32=True, bf16=True)
     ref = ks.solve(ctx, M, "CG", b, E=1e-12)
-    r = ks.solve(ctx, M, outer, b, inner=inner, E=1e-10, l=20, e=1e-30, r=21, R=30, inner_precision=prec)
+    # the FP64 true-residual check is on by default for FP32 / BF16 inner
+    # solves; the FP64 inner solve asks for it
+    r = ks.solve(ctx, M, outer, b, inner=inner, E=1e-10, l=20, e=1e-30, r=21, R=30, inner_precision=prec,
+                 true_residual=1 if prec == "fp64" else 0)
     assert r.converged, (r.status, r.loop)
-    assert r.true_rel_res < 2e-10
+    assert r.true_rel_res < 1e-10
+    assert r.report["true_residual_checks"] >= 1
     err = np.linalg.norm(r.x - ref.x) / np.linalg.norm(ref.x)
     assert err < 1e-6
+
+
+def test_failed_true_residual_check_restarts(ks, ctx):
+    """VPGMRES stops on its Givens residual, which runs ahead of b - A x: with
+    the check off it can stop above the eps; with it on it carries on until
+    the FP64 true residual passes, and the history continues past the first
+    stop."""
+    A, b, _ = config_problem("varcoef3d", 20)
+    M = ctx.matrix(A, transpose=True, fp32=True, bf16=True)
+    kw = dict(E=1e-10, l=20, e=1e-30, R=30, inner_precision="fp32")
+    off = ks.solve(ctx, M, "VPGMRES", b, inner="CG", true_residual=2, **kw)
+    on = ks.solve(ctx, M, "VPGMRES", b, inner="CG", true_residual=1, **kw)
+    assert off.report["true_residual_checks"] == 0
+    assert on.converged and on.true_rel_res < 1e-10
+    assert on.report["true_residual_checks"] >= 1
+    if off.true_rel_res >= 1e-10:  # the check had to restart
+        assert on.report["true_residual_checks"] >= 2 and on.loop > off.loop
+    n = min(len(off.hist_err), len(on.hist_err))
+    assert np.array_equal(off.hist_err[:n], on.hist_err[:n])  # same run up to the first stop
+
+
+def test_x_rel_diff_in_report(ks, ctx):
+    """params.x_ref: the report carries |x - x_ref| / |x_ref| against an FP64
+    solution, as every mixed-precision result should."""
+    A, b, _ = config_problem("varcoef3d", 16)
+    M = ctx.matrix(A, fp32=True)
+    B = ctx.vector(b)
+    ref = ks.solve(ctx, M, "CG", B, E=1e-12)
+    xr = ctx.vector(n=A.n)
+    ks.solve(ctx, M, "CG", B, x=xr, E=1e-12)
+    X = ctx.vector(n=A.n)
+    r = ks.solve(ctx, M, "VPCG", B, inner="CG", x=X, E=1e-10, l=20, e=1e-30, inner_precision="fp32",
+                 x_ref=xr.device_ptr())
+    xm, x64 = X.numpy(), xr.numpy()
+    want = np.linalg.norm(xm - x64) / np.linalg.norm(x64)
+    assert r.report["x_rel_diff"] == pytest.approx(want, rel=1e-6)
+    assert 0 < r.report["x_rel_diff"] < 1e-6
+    assert ks.solve(ctx, M, "CG", B, x=X, E=1e-10).report["x_rel_diff"] == -1.0
+    del ref
 
 
 def _dense_grad(A, b, xstar):
