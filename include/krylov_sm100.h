@@ -68,6 +68,10 @@ ks_status ks_ctx_destroy(ks_ctx *ctx);
 /* Use an existing cudaStream_t (passed as void*); NULL restores the
  * context's own stream. */
 ks_status ks_ctx_set_stream(ks_ctx *ctx, void *stream);
+/* Waits for the context's queued work; KS_TIMEOUT if a bounded device wait of
+ * a queued kernel ran out since the last call that reported one (asynchronous
+ * calls such as ks_spmv report it here, at the next call returning host
+ * scalars, or at the next ks_solve). */
 ks_status ks_ctx_synchronize(ks_ctx *ctx);
 /* Number of CUDA devices (cuda::GetDeviceNum, cudaFunction.cu:1905). */
 int ks_device_count(void);
@@ -254,10 +258,12 @@ typedef struct {
                               systems)                                      */
   int32_t inner_fast;      /* VP methods whose inner CG runs in FP32 / with
                               BF16 values on a one-GPU matrix with a diagonal
-                              copy: 0 auto, two kernels per inner iteration
-                              (the SpMV forms the direction and applies the
-                              previous x update); 1 the three-kernel loop.
-                              Both give the same values per element.       */
+                              copy: 0 auto, the whole inner solve as one
+                              cooperative kernel with its vectors on chip
+                              where the system fits (up to ~28,900 rows per
+                              SM); 1 one kernel per step. Both apply the same
+                              operations to every element; the order in which
+                              the dot products add their terms differs.    */
   int32_t true_residual;   /* VP methods: when the recurrence residual
                               passes -E, recompute |b - A x| / |b| in FP64
                               and stop only if it passes too, else go on
@@ -291,6 +297,12 @@ typedef struct {
    * other kernels (vector updates, basis combinations, scalar steps);
    * memsets; host<->device copies of the solve (ks_solve_host). */
   double t_mv, t_dot, t_other, t_memset, t_h2d, t_d2h;
+  /* With params.profile = 1: kernels launched per class (SpMVs, reductions,
+   * other, memsets), and the share of the SpMV class that read FP32 / BF16
+   * values (a VP method's inner solves): its time and launches. */
+  int64_t n_mv, n_dot, n_other, n_memset;
+  double t_mv_low;
+  int64_t n_mv_low;
 } ks_report;
 
 void ks_params_default(ks_params *p);

@@ -56,7 +56,7 @@ static double pair_dot(long n, const double *x, const double *y) {
  * threads take one extra element), each part summed from 0.0 in order and
  * the parts added in thread order. g_sum_chunks = -1: pairwise summation. */
 double oracle_dot(long n, const double *x, const double *y) {
-  if (g_sum_chunks == -1) return pair_dot(n, x, y);
+  if (g_sum_chunks == -1 || g_sum_chunks == -2) return pair_dot(n, x, y);
   if (g_sum_chunks <= 1) {
     double t = 0.0;
     for (long i = 0; i < n; i++) t += x[i] * y[i];
@@ -79,6 +79,7 @@ double oracle_dot(long n, const double *x, const double *y) {
  * Gcr_sp_1's parallel loop (blas.cpp:529-535) run as nested, one-thread
  * regions. */
 static double seq_dot(long n, const double *x, const double *y) {
+  if (g_sum_chunks == -2) return pair_dot(n, x, y);
   double t = 0.0;
   for (long i = 0; i < n; i++) t += x[i] * y[i];
   return t;
@@ -153,6 +154,14 @@ void oracle_matpow(const or_mat *A, const double *r, const double *p, int k,
 void oracle_gram_cg(long n, int k, const double *Ar, const double *Ap,
                     const double *r, const double *p, double *delta,
                     double *eta, double *zeta) {
+  if (g_sum_chunks == -2) {  /* every Gram value summed pairwise */
+    for (int i = 0; i < 2 * k + 2; i++) {
+      if (i < 2 * k) delta[i] = pair_dot(n, r, Ar + (long)i * n);
+      if (i < 2 * k + 1) eta[i] = pair_dot(n, r, Ap + (long)i * n);
+      zeta[i] = pair_dot(n, p, Ap + (long)i * n);
+    }
+    return;
+  }
   for (int i = 0; i < 2 * k + 2; i++) {
     double t1 = 0.0, t2 = 0.0, t3 = 0.0;
     for (long j = 0; j < n; j++) {
@@ -170,6 +179,17 @@ void oracle_gram_cg(long n, int k, const double *Ar, const double *Ap,
 void oracle_gram_bicg(long n, int k, const double *Ar, const double *Ap,
                       const double *rs, const double *ps, double *theta,
                       double *eta, double *rho, double *phi) {
+  if (g_sum_chunks == -2) {  /* every Gram value summed pairwise */
+    for (int i = 0; i < 2 * k + 2; i++) {
+      if (i < 2 * k) theta[i] = pair_dot(n, rs, Ar + (long)i * n);
+      if (i < 2 * k + 1) {
+        eta[i] = pair_dot(n, rs, Ap + (long)i * n);
+        rho[i] = pair_dot(n, ps, Ar + (long)i * n);
+      }
+      phi[i] = pair_dot(n, ps, Ap + (long)i * n);
+    }
+    return;
+  }
   for (int i = 0; i < 2 * k + 2; i++) {
     double t1 = 0.0, t2 = 0.0, t3 = 0.0, t4 = 0.0;
     for (long j = 0; j < n; j++) {
@@ -974,7 +994,7 @@ int oracle_solve(const or_mat *A, const or_params *p, const double *b,
                  double *x, long *hist_iter, double *hist_err, long hist_cap,
                  or_report *rep) {
   ctx_t c = {A, p, 0, p->inner != OR_NONE};
-  g_sum_chunks = p->sum_chunks > 1 || p->sum_chunks == -1 ? p->sum_chunks : 1;
+  g_sum_chunks = p->sum_chunks > 1 || p->sum_chunks == -1 || p->sum_chunks == -2 ? p->sum_chunks : 1;
   hist_t h = {hist_iter, hist_err, hist_iter && hist_err ? hist_cap : 0, 0};
   res_t res = {99, 0};
   long n = A->n;

@@ -56,7 +56,10 @@ typedef struct {
                              contiguous partial sums added in order, the way
                              an OpenMP static reduction with that many
                              threads does; 0/1: one sequential sum (-t 1);
-                             -1: pairwise (recursive halving) sums */
+                             -1: pairwise (recursive halving) sums;
+                             -2: pairwise, and so are the dots the
+                             reference always sums sequentially (the
+                             k-skip Gram values, GCR's beta dots) */
 } or_params;
 
 typedef struct {

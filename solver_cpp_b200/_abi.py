@@ -68,6 +68,8 @@ class Report(C.Structure):
         ("x_rel_diff", C.c_double), ("true_residual_checks", C.c_int64),
         ("t_mv", C.c_double), ("t_dot", C.c_double), ("t_other", C.c_double), ("t_memset", C.c_double),
         ("t_h2d", C.c_double), ("t_d2h", C.c_double),
+        ("n_mv", C.c_int64), ("n_dot", C.c_int64), ("n_other", C.c_int64), ("n_memset", C.c_int64),
+        ("t_mv_low", C.c_double), ("n_mv_low", C.c_int64),
     ]
 
 

@@ -323,6 +323,7 @@ struct ks_ctx {
   // Per-class device time of a solve (ks_params.profile): every launch_k
   // records an event before and after its kernel and the class the launcher
   // set in next_class (ks::KernelClass; reset to kOther after each launch).
+  void *ir_sync = nullptr;      // barrier state of the on-chip inner CG (ks_inner_resident.cuh)
   int prof_on = 0;
   int next_class = 0;
   std::vector<cudaEvent_t> prof_events;  // pool, reused across solves
@@ -332,7 +333,8 @@ struct ks_ctx {
 namespace ks {
 constexpr int kStageLen = 4096;  // >= 2 x 1024 block-dot results, >= kMaxDots
 // Kernel classes of the times report (times.cpp:60-76).
-enum KernelClass : int { kOther = 0, kMv = 1, kDot = 2, kMemset = 3, kNumClasses = 4 };
+// kMvLow: an SpMV reading FP32 / BF16 values (reported within kMv too).
+enum KernelClass : int { kOther = 0, kMv = 1, kDot = 2, kMemset = 3, kMvLow = 4, kNumClasses = 5 };
 }
 
 namespace ks {

@@ -674,6 +674,7 @@ ks_status ks_ctx_create(int device, ks_ctx **out) {
     return fail(KS_OUT_OF_MEMORY);
   std::memset(ctx->h_snap, 0, sizeof(int) * ctx->nflags);
   if (cudaMalloc(&ctx->d_stage, sizeof(double) * kStageLen) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
+  if (cudaMalloc(&ctx->ir_sync, 64) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
   ctx->flag_events = new cudaEvent_t[ctx->nflags];
   for (int i = 0; i < ctx->nflags; i++) {
     if (cudaEventCreateWithFlags(&ctx->flag_events[i], cudaEventDisableTiming) != cudaSuccess)
@@ -706,6 +707,7 @@ ks_status ks_ctx_destroy(ks_ctx *ctx) {
     delete[] ctx->flag_events;
   }
   for (cudaEvent_t e : ctx->prof_events) cudaEventDestroy(e);
+  cudaFree(ctx->ir_sync);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -736,7 +738,7 @@ ks_status ks_ctx_set_stream(ks_ctx *ctx, void *stream) {
 ks_status ks_ctx_synchronize(ks_ctx *ctx) {
   if (!ctx) return KS_BAD_INPUT;
   KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return KS_OK;
+  return check_device_error(ctx);  // a bounded wait of a queued kernel that ran out
 }
 
 // ============================================================= C ABI: matrices

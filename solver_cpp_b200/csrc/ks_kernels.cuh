@@ -166,6 +166,34 @@ inline Red red_of(ks_ctx *ctx, int slot = 0) {
   return Red{ctx->partials, ctx->counters + slot};
 }
 
+// With ks_params.profile: events around one launch, recorded with its class
+// (every launch of a profiled solve goes through this, launch_k or not).
+struct ProfLaunch {
+  ks_ctx *ctx;
+  long long i = -1;
+  int cls;
+  ProfLaunch(ks_ctx *c, int k) : ctx(c), cls(k) {
+    if (!ctx->prof_on) return;
+    const size_t n = ctx->prof_class.size();
+    while (ctx->prof_events.size() < 2 * n + 2) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreate(&e) != cudaSuccess) {  // no more events: stop recording
+        (void)cudaGetLastError();
+        ctx->prof_on = 0;
+        return;
+      }
+      ctx->prof_events.push_back(e);
+    }
+    i = (long long)n;
+    cudaEventRecord(ctx->prof_events[2 * n], ctx->stream);
+  }
+  ~ProfLaunch() {
+    if (i < 0) return;
+    cudaEventRecord(ctx->prof_events[2 * i + 1], ctx->stream);
+    ctx->prof_class.push_back((unsigned char)cls);
+  }
+};
+
 // Launch on the context's stream with programmatic stream serialization:
 // the kernel may be scheduled while the previous one finishes, and reads the
 // previous kernels' results only after its griddepcontrol.wait (pdl_wait).
@@ -184,25 +212,8 @@ inline void launch_k(ks_ctx *ctx, void (*kern)(KArgs...), dim3 grid, dim3 block,
   ctx->launches++;
   const int cls = ctx->next_class;
   ctx->next_class = kOther;
-  if (!ctx->prof_on) {
-    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-    return;
-  }
-  const size_t i = ctx->prof_class.size();
-  while (ctx->prof_events.size() < 2 * i + 2) {
-    cudaEvent_t e = nullptr;
-    if (cudaEventCreate(&e) != cudaSuccess) {  // no more events: stop recording
-      (void)cudaGetLastError();
-      ctx->prof_on = 0;
-      cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-      return;
-    }
-    ctx->prof_events.push_back(e);
-  }
-  cudaEventRecord(ctx->prof_events[2 * i], ctx->stream);
+  ProfLaunch pl(ctx, cls);
   cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-  cudaEventRecord(ctx->prof_events[2 * i + 1], ctx->stream);
-  ctx->prof_class.push_back((unsigned char)cls);
 }
 
 template <class MT>
@@ -368,7 +379,7 @@ inline void launch_spmv_dn(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX 
   const long long need = ((long long)A.n + kThreads - 1) / kThreads;
   const long long wave = (long long)ctx->num_sms * spmv_dia_ctas_per_sm<NV, NDG, MT, GX, Epi>(ctx->device);
   const int grid = (int)std::max<long long>(1, std::min(need, wave));
-  ctx->next_class = kMv;
+  ctx->next_class = std::is_same<MT, double>::value ? kMv : kMvLow;
   launch_k(ctx, spmv_dia_kernel<NV, NDG, MT, GX, Epi>, dim3(grid), dim3(kThreads), 0, dview<MT>(A), g0, g1, epi,
            stop, red_of(ctx, slot));
 }
@@ -394,7 +405,7 @@ inline void launch_spmv_k(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX &
                           int slot) {
   const int per_sm = spmv_tma_ctas_per_sm<NV, MT, IT, GX, Epi>(ctx->device);
   const int grid = std::max(1, std::min(ctx->num_sms * per_sm, A.nrb));
-  ctx->next_class = kMv;
+  ctx->next_class = std::is_same<MT, double>::value ? kMv : kMvLow;
   launch_k(ctx, spmv_tma_kernel<NV, MT, IT, GX, Epi>, dim3(grid), dim3(kThreads), spmv_tma_smem<MT, IT>(),
            tview<MT, IT>(A), g0, g1, epi, stop, red_of(ctx, slot), ctx->d_err, ctx->wait_ns);
 }

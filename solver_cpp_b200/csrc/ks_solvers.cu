@@ -17,6 +17,7 @@
 #include "ks_ops.cuh"
 #include "ks_state.cuh"
 #include "ks_resident.cuh"
+#include "ks_inner_resident.cuh"
 
 namespace ks {
 
@@ -790,6 +791,7 @@ inline bool run_cg_resident(const Env<double> &E, const double *b, double *x, ks
   }
   launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
   E.ctx->launches++;
+  ProfLaunch pl(E.ctx, kOther);  // a whole solve in one cluster launch
   const cudaError_t e = res_cg(sh, A.col16 != nullptr, E.ctx->stream, a, false, nullptr);
   *s = e == cudaSuccess ? KS_OK : cuda_fail(E.ctx, e, "cluster-resident CG launch");
   return true;
@@ -912,6 +914,7 @@ inline bool run_cr_resident(const Env<double> &E, const double *b, double *x, ks
   }
   launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
   E.ctx->launches++;
+  ProfLaunch pl(E.ctx, kOther);  // a whole solve in one cluster launch
   const cudaError_t e = res_cr(sh, A.col16 != nullptr, E.ctx->stream, a, false, nullptr);
   *s = e == cudaSuccess ? KS_OK : cuda_fail(E.ctx, e, "cluster-resident CR launch");
   return true;
@@ -1034,6 +1037,7 @@ inline bool run_bicg_resident(const Env<double> &E, const double *b, double *x, 
   }
   launch_scalar(E.ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
   E.ctx->launches++;
+  ProfLaunch pl(E.ctx, kOther);  // a whole solve in one cluster launch
   const cudaError_t e = res_bicg(sh, ia16, it16, E.ctx->stream, a, false, nullptr);
   *s = e == cudaSuccess ? KS_OK : cuda_fail(E.ctx, e, "cluster-resident BiCG launch");
   return true;
@@ -1818,81 +1822,13 @@ template <class IT>
 ks_status run_method(int method, const Env<IT> &E, const IT *b, IT *x, IT *ws, double *dws,
                      InnerRunner<IT> *inner);
 
-// ------------------------------------------------------------------ fast inner CG
+// ------------------------------------------------------------------ on-chip inner CG
 // The FP32 (or BF16-valued) inner CG of a VP method on a one-GPU matrix with
-// a diagonal copy runs two kernels per iteration instead of three:
-//   K1(L): q = A p_L, with p_L = beta_L p_{L-1} + r formed in the SpMV's
-//          reads (GDir) and the row's own p_L stored; the x update of
-//          iteration L-1, x += alpha_{L-1} p_{L-1}, applied for the row
-//          (L = 1: x = 0); (p,q) -> alpha_L.
-//   K2(L): r -= alpha_L q; (r,r) -> beta_{L+1}; stopping test.
-// Nothing in the loop reads x (cg.cpp:211 is its only update), so applying
-// each update one kernel later changes no value: every element sees the same
-// FP32 operations in the same order as in the three-kernel loop (XpbyToOp,
-// XrUpdOp). The update still pending when the loop stops (alpha_L p_L, when
-// K2(L) stopped it) is applied by the kernel that hands z back to the outer
-// method. The loop's vectors are r, q, two direction slots and x: five FP32
-// vectors that the streamed matrix leaves in L2. The start (r = (float) b,
-// (r,r), the state reset) and the end (z = (double) x) fuse into the outer
-// method's own kernels where the outer method is VPCG.
-
-// K1 epilogue (see above). `first`: iteration 1, where pold = r and beta = 0.
-template <class VT>
-struct CgInMvEpi {
-  using acc_t = VT;
-  const VT *pold;
-  const VT *r;
-  VT *p;
-  VT *q;
-  VT *x;
-  DevState *st;
-  int first;
-  static constexpr int ND = 1;
-  __device__ void row(int i, VT v, double (&acc)[1]) const {
-    const VT b = (VT)rd(&st->k.s[S_BETA]);
-    const VT po = pold[i];
-    const VT pi = add_rn(mul_rn(b, po), r[i]);
-    p[i] = pi;
-    q[i] = v;
-    x[i] = first ? (VT)0 : add_rn(mul_rn((VT)rd(&st->k.s[S_ALPHA]), po), x[i]);
-    acc[0] = add_rn(acc[0], mul_rn(widen(pi), widen(v)));
-  }
-  // Runs after every CTA has finished its rows, so no row reads the new
-  // alpha_L in place of alpha_{L-1}.
-  __device__ void finish(const double (&s)[1]) const {
-    st->k.aux[A_PENDING] = 0;
-    st->k.aux[A_XZERO] = 0;
-    st->k.s[S_ALPHA] = rdiv(st, st->k.s[S_RR], s[0]);
-  }
-};
-
-// K2: r -= alpha q; (r,r) -> beta, check (XrUpdOp mode 0 without x);
-// alpha_L p_L is now pending, p_L in slot (L - 1) % 2.
-template <class VT>
-struct CgInRUpdOp {
-  VT *r;
-  const VT *q;
-  DevState *st;
-  long long L;
-  static constexpr int ND = 1;
-  struct Regs {
-    VT q, r;
-  };
-  __device__ Regs load(long long i) const { return {q[i], r[i]}; }
-  __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
-    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
-    const VT ri = add_rn(mul_rn((VT)(-a), g.q), g.r);
-    r[i] = ri;
-    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
-  }
-  __device__ void finish(const double (&s)[1]) const {
-    st->k.aux[A_PENDING] = 1;
-    st->k.aux[A_KIDX] = L;
-    st->k.s[S_BETA] = rdiv(st, s[0], st->k.s[S_RR]);
-    st->k.s[S_RR] = s[0];
-    check_top(st, st->k.loop + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
-  }
-};
+// a diagonal copy runs as one cooperative kernel per inner solve, its vectors
+// on chip (k_inner_cg_resident, ks_inner_resident.cuh). Around it: the start
+// (r = (float) b, (r,r), the state reset) and the end (z = (double) x) are
+// vector passes, fused into the outer method's own kernels where the outer
+// method is VPCG (its x/r update and its (r, z)).
 
 // The inner state's reset (InitOp without history) and the top of iteration 1
 // (StartZeroOp with START_CG, x = 0): |b| and (r,r) are the same sum.
@@ -1934,14 +1870,12 @@ struct CgInStartOp {
   __device__ void finish(const double (&s)[1]) const { inner_cg_start(st, eps, maxloop, s[0]); }
 };
 
-// Inner end: z = (double) x_final, x_final = x + alpha_K p_K when an update is
-// pending (ConvertOp of the three-kernel loop's x). mode 1 / 2 also fuse
-// VPCG's RzOp (init / beta) over the outer r and z on the outer state.
+// Inner end: z = (double) x (ConvertOp of the kernel-per-step loop's x; x
+// is 0 if the inner method stopped before its first update). mode 1 / 2 also
+// fuse VPCG's RzOp (init / beta) over the outer r and z on the outer state.
 template <class VT>
 struct CgInFinalOp {
   const VT *x;
-  const VT *P0;
-  const VT *P1;
   const DevState *ist;
   double *z;
   const double *r;
@@ -1949,18 +1883,12 @@ struct CgInFinalOp {
   int mode;
   static constexpr int ND = 1;
   struct Regs {
-    VT x, p;
+    VT x;
     double r;
   };
-  __device__ Regs load(long long i) const {
-    const long long K = __ldg(&ist->k.aux[A_KIDX]);
-    const VT *p = (K - 1) & 1 ? P1 : P0;
-    return {x[i], __ldg(&ist->k.aux[A_PENDING]) ? p[i] : (VT)0, mode ? r[i] : 0.0};
-  }
+  __device__ Regs load(long long i) const { return {x[i], mode ? r[i] : 0.0}; }
   __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
-    VT xf = __ldg(&ist->k.aux[A_XZERO]) ? (VT)0 : g.x;
-    if (__ldg(&ist->k.aux[A_PENDING])) xf = add_rn(mul_rn((VT)__ldg(&ist->k.s[S_ALPHA]), g.p), xf);
-    const double zi = (double)xf;
+    const double zi = __ldg(&ist->k.aux[A_XZERO]) ? 0.0 : (double)g.x;
     z[i] = zi;
     acc[0] = add_rn(acc[0], mul_rn(g.r, zi));
   }
@@ -2005,22 +1933,24 @@ struct VpXrStartOp {
   }
 };
 
-// The fast inner loop's buffers, carved from the inner workspace.
-template <class VT>
-struct InnerCgBufs {
-  VT *r, *q, *P0, *P1, *x;
-  VT *slot(long long L) const { return ((L - 1) & 1) ? P1 : P0; }
+// The on-chip inner CG's buffers: its right-hand side r (FP32), the
+// published directions P and the solution x, in the inner workspace.
+struct InnerResBufs {
+  float *r, *P, *x;
 };
 
-// Iterations 1..maxloop of the fast inner CG (start already issued).
-template <class VT>
-inline void run_cg_inner_loop(const Env<VT> &E, const InnerCgBufs<VT> &B) {
-  for (long long L = 1; L <= E.sp.maxloop; L++) {
-    const VT *pold = L == 1 ? B.r : B.slot(L + 1);
-    mv_g(E, *E.A, GDir<VT>{pold, B.r, &E.st->k.s[S_BETA], (VT)0},
-         CgInMvEpi<VT>{pold, B.r, B.slot(L), B.q, B.x, E.st, L == 1 ? 1 : 0});
-    vec(E, CgInRUpdOp<VT>{B.r, B.q, E.st, L});
+// One inner solve with the on-chip kernel (its start already issued).
+inline ks_status run_cg_inner_resident(const Env<float> &E, const InnerResBufs &B, const IrShape &sh) {
+  ks_ctx *ctx = E.ctx;
+  IrArgs a{B.r, B.x, B.P, E.st, E.outer_done, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
+           (int)E.n, sh.rpc, sh.K};
+  cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, sizeof(IrSync), ctx->stream);
+  if (e == cudaSuccess) {
+    bool fits = false;
+    e = E.mvals == KS_BF16 ? ir_launch<__nv_bfloat16>(ctx, *E.A, a, sh, false, &fits)
+                           : ir_launch<float>(ctx, *E.A, a, sh, false, &fits);
   }
+  return e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip inner CG launch");
 }
 
 template <class VT>
@@ -2038,28 +1968,37 @@ struct InnerRunner {
   float *b32 = nullptr, *z32 = nullptr;
   long long calls = 0;
   ks_status status = KS_OK;
-  // fast inner CG (see above): chosen at set-up
-  bool fast_cg = false;
-  InnerCgBufs<float> fb{};
-  void setup_fast();
+  // on-chip inner CG (see above): chosen at set-up
+  bool res_cg = false;
+  InnerResBufs fb{};
+  IrShape sh{};
+  void setup_resident();
   void solve(const VT *b, VT *z);
 };
 
-// The fast inner CG applies where the inner method is CG in FP32 or with BF16
-// values, on one GPU, and the SpMV reads a diagonal copy of those values.
+// The on-chip inner CG applies where the inner method is CG in FP32 or with
+// BF16 values, on one GPU, the SpMV reads a diagonal copy of those values,
+// and the system fits the kernel's shape (ir_shape) on this device.
 template <class VT>
-void InnerRunner<VT>::setup_fast() {
-  fast_cg = false;
+void InnerRunner<VT>::setup_resident() {
+  res_cg = false;
   if (method != KS_CG || iprec == KS_FP64 || E32.comm || !E32.A || !E32.A->dia_nd) return;
   if (iprec == KS_FP32 ? !E32.A->dia_val32 : !E32.A->dia_val16) return;
-  if (vec_count(KS_CG, E32.sp, E32.n, sizeof(float), ctx->l2_bytes) < 4) return;
+  if (vec_count(KS_CG, E32.sp, E32.n, sizeof(float), ctx->l2_bytes) < 2) return;
+  if (!ir_shape(ctx, E32.n, &sh)) return;
+  bool fits = false;
+  const IrArgs none{};
+  const cudaError_t e = iprec == KS_BF16 ? ir_launch<__nv_bfloat16>(ctx, *E32.A, none, sh, true, &fits)
+                                         : ir_launch<float>(ctx, *E32.A, none, sh, true, &fits);
+  if (e != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return;
+  }
   Ws<float> W{ws32, E32.ld, E32.off};
   fb.r = W.take();
-  fb.q = W.take();
-  fb.P0 = W.take();
-  fb.P1 = W.take();
+  fb.P = W.take();
   fb.x = z32;
-  fast_cg = true;
+  res_cg = true;
 }
 
 template <class VT>
@@ -2069,11 +2008,11 @@ void InnerRunner<VT>::solve(const VT *b, VT *z) {
   if constexpr (std::is_same<VT, double>::value) {
     if (iprec == KS_FP64) {
       status = run_method<double>(method, E64, b, z, ws64, dws, nullptr);
-    } else if (fast_cg) {
+    } else if (res_cg) {
       const Stop os{nullptr, E32.outer_done};
       launch_vec(ctx, n, CgInStartOp<float>{b, fb.r, E32.st, E32.sp.eps, E32.sp.maxloop}, os);
-      run_cg_inner_loop(E32, fb);
-      launch_vec(ctx, n, CgInFinalOp<float>{fb.x, fb.P0, fb.P1, E32.st, z, nullptr, nullptr, 0}, os);
+      status = run_cg_inner_resident(E32, fb, sh);
+      launch_vec(ctx, n, CgInFinalOp<float>{fb.x, E32.st, z, nullptr, nullptr, 0}, os);
     } else {
       launch_vec(ctx, n, ConvertOp<double, float>{b, b32}, Stop{nullptr, E32.outer_done});
       status = run_method<float>(method, E32, b32, z32, ws32, dws, nullptr);
@@ -2112,10 +2051,10 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
-  // vpcg.cpp:659-750. With the fast inner CG its start is fused into the
+  // vpcg.cpp:659-750. With the on-chip inner CG its start is fused into the
   // outer x/r update and its end into (r, z).
   bool fast = false;
-  if constexpr (std::is_same<VT, double>::value) fast = inner->fast_cg;
+  if constexpr (std::is_same<VT, double>::value) fast = inner->res_cg;
   // z = M r, rr = (r, z), p = z: the method's start, and its restart after a
   // failed true-residual check (r then holds b - A x)
   auto start = [&]() {
@@ -2126,8 +2065,8 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
         const Stop os{nullptr, F.outer_done};
         I.calls++;
         launch_vec(E.ctx, E.n, CgInStartOp<float>{r, I.fb.r, F.st, F.sp.eps, F.sp.maxloop}, os);
-        run_cg_inner_loop(F, I.fb);
-        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, I.fb.P0, I.fb.P1, F.st, z, r, E.st, 1}, os);
+        if (I.status == KS_OK) I.status = run_cg_inner_resident(F, I.fb, I.sh);
+        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, F.st, z, r, E.st, 1}, os);
         vec(E, CopyOp<VT>{z, p});
         return;
       }
@@ -2144,8 +2083,8 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
         const Env<float> &F = I.E32;
         I.calls++;
         vec(E, VpXrStartOp<float>{x, r, p, mvv, E.st, I.fb.r, F.st, F.sp.eps, F.sp.maxloop});
-        run_cg_inner_loop(F, I.fb);
-        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, I.fb.P0, I.fb.P1, F.st, z, r, E.st, 2},
+        if (I.status == KS_OK) I.status = run_cg_inner_resident(F, I.fb, I.sh);
+        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, F.st, z, r, E.st, 2},
                    Stop{nullptr, F.outer_done});
         vec(E, XpbyOp<VT>{p, z, &E.st->k.s[S_BETA]});
         return;
@@ -2471,7 +2410,7 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
       KS_TRY(al.get((size_t)ld, &IR.z32));
       IR.b32 += off;
       IR.z32 += off;
-      if (prm->inner_fast == 0) IR.setup_fast();
+      if (prm->inner_fast == 0) IR.setup_resident();
     }
   }
 
@@ -2559,20 +2498,30 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     rep->true_rel_res = 0.0;
     rep->x_rel_diff = -1.0;
     rep->true_residual_checks = hs[4];
-    rep->t_mv = rep->t_dot = rep->t_other = rep->t_memset = rep->t_h2d = rep->t_d2h = 0.0;
+    rep->t_mv = rep->t_dot = rep->t_other = rep->t_memset = rep->t_h2d = rep->t_d2h = rep->t_mv_low = 0.0;
+    rep->n_mv = rep->n_dot = rep->n_other = rep->n_memset = rep->n_mv_low = 0;
     if (prm->profile == 1) {  // the stream is synchronised: every event has completed
-      double t[kNumClasses] = {0, 0, 0, 0};
+      double t[kNumClasses] = {0, 0, 0, 0, 0};
+      long long c[kNumClasses] = {0, 0, 0, 0, 0};
       for (size_t i = 0; i < ctx->prof_class.size(); i++) {
         float ms = 0.f;
+        const int k = ctx->prof_class[i];
+        c[k]++;
         if (cudaEventElapsedTime(&ms, ctx->prof_events[2 * i], ctx->prof_events[2 * i + 1]) == cudaSuccess)
-          t[ctx->prof_class[i]] += ms * 1e-3;
+          t[k] += ms * 1e-3;
         else
           (void)cudaGetLastError();
       }
-      rep->t_mv = t[kMv];
+      rep->t_mv = t[kMv] + t[kMvLow];
       rep->t_dot = t[kDot];
       rep->t_other = t[kOther];
       rep->t_memset = t[kMemset];
+      rep->n_mv = c[kMv] + c[kMvLow];
+      rep->n_dot = c[kDot];
+      rep->n_other = c[kOther];
+      rep->n_memset = c[kMemset];
+      rep->t_mv_low = t[kMvLow];
+      rep->n_mv_low = c[kMvLow];
     }
     if (prm->x_ref && !dist) {  // |x - x_ref| / |x_ref| over the solution
       launch_vec(ctx, n, DiffNormOp{x, prm->x_ref, ctx->d_result}, Stop{nullptr, nullptr});

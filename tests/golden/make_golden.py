@@ -262,8 +262,11 @@ def main_large(workroot, cores, only=None):
 # Summation orders of the oracle study (--orders): the reference's sequential
 # order (1: pins the oracle at full size against the -t 1 golden), contiguous
 # partial sums as OpenMP would add them with more threads than the host has,
-# and pairwise summation (-1), the accuracy class of a parallel tree.
-ORDER_CHUNKS = (1, 16, 256, 4096, -1)
+# pairwise summation (-1), the accuracy class of a parallel tree, and
+# pairwise summation of every dot (-2), also of those the reference always
+# adds sequentially whatever its thread count (the k-skip Gram values,
+# blas.cpp:401-475), as the GPU's tree reductions do.
+ORDER_CHUNKS = (1, 16, 256, 4096, -1, -2)
 
 
 def _oracle_order_run(args):
@@ -276,7 +279,7 @@ def _oracle_order_run(args):
     return cid, chunks, int(r["loop"]), int(r["status"]), r["hist_err"]
 
 
-def main_orders(cores, only=None):
+def main_orders(cores, only=None, chunks=ORDER_CHUNKS):
     """Oracle loop counts under ORDER_CHUNKS for the full-size cases whose
     reference runs differ between thread counts; adds them to
     index_large.json as ``oracle_loops_by_order`` (and, for chunks = 1,
@@ -291,7 +294,7 @@ def main_orders(cores, only=None):
             continue
         if len(set(index[cid]["loops_by_threads"].values())) == 1:
             continue
-        jobs += [(cid, prob, grid, args, c) for c in ORDER_CHUNKS]
+        jobs += [(cid, prob, grid, args, c) for c in chunks]
     with mp.get_context("spawn").Pool(max(1, min(cores, len(jobs)))) as pool:
         for cid, chunks, loop, status, hist in pool.imap_unordered(_oracle_order_run, jobs):
             e = index[cid].setdefault("oracle_loops_by_order", {})
@@ -316,8 +319,9 @@ if __name__ == "__main__":
         ap.add_argument("--orders", action="store_true")
         ap.add_argument("--cores", type=int, default=max(1, (os.cpu_count() or 2) - 1))
         ap.add_argument("--only", nargs="*")
+        ap.add_argument("--chunks", type=int, nargs="*", default=list(ORDER_CHUNKS))
         a = ap.parse_args()
-        main_orders(a.cores, a.only)
+        main_orders(a.cores, a.only, tuple(a.chunks))
     elif "--large" in sys.argv:
         import argparse
 

@@ -123,3 +123,115 @@ def test_split_spmv_over_two_gloo_ranks():
         p.join(timeout=300)
     assert all(p.exitcode == 0 for p in procs)
     assert q.get(timeout=10) is True
+
+
+def _halo_exchange(dist, torch, plan, rank, world, v, xe, lo):
+    """The engine's exchange before an SpMV (Env::halo): each peer's planned
+    range of its own rows lands in this rank's window."""
+    reqs = []
+    for peer in range(world):
+        if peer == rank:
+            continue
+        a, b = plan["send"][peer]
+        if b > a:
+            reqs.append(dist.isend(torch.from_numpy(np.ascontiguousarray(v[a:b])), peer))
+    for peer in range(world):
+        if peer == rank:
+            continue
+        a, b = plan["recv"][peer]
+        if b > a:
+            buf = torch.empty(b - a, dtype=torch.float64)
+            dist.recv(buf, peer)
+            xe[a - lo:b - lo] = buf.numpy()
+    for r in reqs:
+        r.wait()
+
+
+def _gloo_cg_rank(rank, world, port, q):
+    """CG (cg.cpp:148-240) split by rows the way the library splits it: the
+    library's plan, a halo exchange before every SpMV, every reduction summed
+    over the ranks before its scalar step (with_rank_sums), the stopping test
+    on the summed value, so every rank takes the same decisions and the same
+    number of collectives."""
+    import torch
+    import torch.distributed as dist
+
+    import solver_cpp_b200 as ks
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g = 12
+        A, b, _ = config_problem("varcoef3d", g)
+        rs = ks.partition_rows(A.n, world, g * g)
+        r0, r1 = int(rs[rank]), int(rs[rank + 1])
+        lo, hi = ks.halo_window(A, r0, r1)
+        wins = [None] * world
+        dist.all_gather_object(wins, (lo, hi))
+        plan = ks.halo_plan(rs, [w[0] for w in wins], [w[1] for w in wins], rank)
+        Aloc = _local_rows(A, r0, r1, lo, hi)
+
+        def allsum(v):
+            t = torch.tensor([v], dtype=torch.float64)
+            dist.all_reduce(t)
+            return float(t.item())
+
+        full_p = np.zeros(A.n)  # only [r0, r1) and the received halo are ever read
+        bl = b[r0:r1]
+        x = np.zeros(r1 - r0)
+        r = bl.copy()
+        p = r.copy()
+        bnorm = np.sqrt(allsum(float(bl @ bl)))
+        rr = allsum(float(r @ r))
+        hist, status = [], 2
+        for L in range(1, 2001):
+            err = np.sqrt(rr) / bnorm
+            hist.append(err)
+            if err <= 1e-10:
+                status = 0
+                break
+            full_p[r0:r1] = p
+            xe = np.full(hi - lo, np.nan)
+            xe[r0 - lo:r1 - lo] = p
+            _halo_exchange(dist, torch, plan, rank, world, full_p, xe, lo)
+            qv = Aloc @ xe
+            alpha = rr / allsum(float(p @ qv))
+            x += alpha * p
+            r -= alpha * qv
+            rr2 = allsum(float(r @ r))
+            beta, rr = rr2 / rr, rr2
+            p = beta * p + r
+        xs = [None] * world
+        dist.all_gather_object(xs, (status, len(hist), hist, x))
+        if rank == 0:
+            q.put(xs)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_split_cg_over_two_gloo_ranks(oracle):
+    """Two CPU ranks run the split CG with the library's plan, exchanges and
+    rank-summed reductions: identical histories and verdicts on both ranks,
+    the same iteration count as one rank (+-1 %), the same solution."""
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gloo_cg_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    (s0, n0, h0, x0), (s1, n1, h1, x1) = res
+    assert s0 == s1 == 0 and n0 == n1 and h0 == h1  # the same decisions, bit for bit
+    A, b, _ = config_problem("varcoef3d", 12)
+    o = oracle.solve(A, b, "CG", E=1e-10)
+    assert o["status"] == 0 and abs(n0 - o["loop"]) <= max(1, 0.01 * o["loop"])
+    x = np.concatenate([x0, x1])
+    assert np.linalg.norm(x - o["x"]) <= 1e-8 * np.linalg.norm(o["x"])

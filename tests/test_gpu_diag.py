@@ -114,12 +114,14 @@ SOLVES = [
 
 @pytest.mark.parametrize("prob,outer,inner,kw", SOLVES)
 def test_solves_identical_on_both_layouts(ks, ctx, prob, outer, inner, kw):
+    """inner_fast=1: both layouts run the inner solves kernel by kernel (the
+    on-chip inner CG needs the diagonal copy; it is compared below)."""
     A, b, _ = config_problem(prob, 16)
     res = []
     for diag in (True, False):
         M = ctx.matrix(A, transpose=True, fp32=True, bf16=True, diag=diag)
         assert (M.info()["diagonals"] > 0) == diag
-        res.append(ks.solve(ctx, M, outer, b, inner=inner, E=1e-10, L=3000, **kw))
+        res.append(ks.solve(ctx, M, outer, b, inner=inner, E=1e-10, L=3000, inner_fast=1, **kw))
     d, c = res
     assert d.status == c.status and d.loop == c.loop
     assert np.array_equal(d.hist_err, c.hist_err) and np.array_equal(d.x, c.x)
@@ -161,20 +163,26 @@ def test_almost_symmetric_matrix_keeps_every_diagonal(ks, ctx, oracle):
     assert np.array_equal(Y.numpy(), oracle.spmv(oracle.Problem(B), x))
 
 
+@pytest.mark.parametrize("grid", [16, 28])
 @pytest.mark.parametrize("outer,inner,prec,kw", [
     ("VPCG", "CG", "fp32", {}), ("VPCG", "CG", "bf16", {}), ("VPGMRES", "CG", "fp32", {"R": 20, "l": 10}),
     ("VPGCR", "CG", "fp32", {"R": 20, "l": 10}), ("VPCR", "CG", "fp32", {"L": 40}),
 ])
-def test_two_kernel_inner_cg_equals_three_kernel_loop(ks, ctx, outer, inner, prec, kw):
-    """The two-kernel inner CG (the SpMV forms the direction and applies the
-    previous x update) gives every element the three-kernel loop's values:
-    identical histories and solutions (16^3: both loops sum their dots in the
-    same order)."""
-    A, b, _ = config_problem("varcoef3d", 16)
+def test_on_chip_inner_cg_matches_kernel_per_step(ks, ctx, grid, outer, inner, prec, kw):
+    """The inner CG as one cooperative kernel with its vectors on chip applies
+    the kernel-per-step loop's FP32 operations to every element; its inner dot
+    products add exact FP64 products of FP32 values in another order, so the
+    two agree to rounding of the sums: the same verdict and iteration count
+    (within 2 %), histories and solutions within 1e-6."""
+    A, b, _ = config_problem("varcoef3d", grid)
     M = ctx.matrix(A, transpose=True, fp32=True, bf16=True)
-    p = dict(E=1e-10, L=3000, l=20, e=1e-30, inner_precision=prec)
+    p = dict(E=1e-10, L=3000, l=20, e=1e-30, inner_precision=prec, true_residual=2)
     p.update(kw)
-    fast = ks.solve(ctx, M, outer, b, inner=inner, inner_fast=0, **p)
-    slow = ks.solve(ctx, M, outer, b, inner=inner, inner_fast=1, **p)
-    assert fast.status == slow.status and fast.loop == slow.loop
-    assert np.array_equal(fast.hist_err, slow.hist_err) and np.array_equal(fast.x, slow.x)
+    chip = ks.solve(ctx, M, outer, b, inner=inner, inner_fast=0, **p)
+    step = ks.solve(ctx, M, outer, b, inner=inner, inner_fast=1, **p)
+    assert chip.status == step.status
+    assert abs(chip.loop - step.loop) <= max(1, 0.02 * step.loop)
+    m = min(len(chip.hist_err), len(step.hist_err), 30)
+    assert np.allclose(chip.hist_err[:m], step.hist_err[:m], rtol=1e-6, atol=0)
+    if step.status == 0:
+        assert np.linalg.norm(chip.x - step.x) <= 1e-6 * np.linalg.norm(step.x)

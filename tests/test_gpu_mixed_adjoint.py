@@ -63,7 +63,7 @@ def test_x_rel_diff_in_report(ks, ctx):
     ks.solve(ctx, M, "CG", B, x=xr, E=1e-12)
     X = ctx.vector(n=A.n)
     r = ks.solve(ctx, M, "VPCG", B, inner="CG", x=X, E=1e-10, l=20, e=1e-30, inner_precision="fp32",
-                 x_ref=xr.device_ptr())
+                 x_ref=xr.device_ptr)
     xm, x64 = X.numpy(), xr.numpy()
     want = np.linalg.norm(xm - x64) / np.linalg.norm(x64)
     assert r.report["x_rel_diff"] == pytest.approx(want, rel=1e-6)
