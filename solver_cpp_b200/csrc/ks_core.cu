@@ -674,7 +674,8 @@ ks_status ks_ctx_create(int device, ks_ctx **out) {
     return fail(KS_OUT_OF_MEMORY);
   std::memset(ctx->h_snap, 0, sizeof(int) * ctx->nflags);
   if (cudaMalloc(&ctx->d_stage, sizeof(double) * kStageLen) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
-  if (cudaMalloc(&ctx->ir_sync, 64) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
+  // barrier state of the on-chip inner CG: 32 bytes + one flag per SM
+  if (cudaMalloc(&ctx->ir_sync, 64 + 8 * (size_t)ctx->num_sms) != cudaSuccess) return fail(KS_OUT_OF_MEMORY);
   ctx->flag_events = new cudaEvent_t[ctx->nflags];
   for (int i = 0; i < ctx->nflags; i++) {
     if (cudaEventCreateWithFlags(&ctx->flag_events[i], cudaEventDisableTiming) != cudaSuccess)

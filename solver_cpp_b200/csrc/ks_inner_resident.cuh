@@ -23,7 +23,8 @@
 //   A: q = A p (own p from shared memory, other CTAs' from P), (p, q) summed
 //      over the grid -> alpha = (r, r) / (p, q);
 //   B: x += alpha p, r -= alpha q, (r, r) summed -> beta, stopping test;
-//   C: p = beta p + r, published; a grid barrier.
+//   C: p = beta p + r, published; each CTA then waits only for the CTAs
+//      whose rows its own rows read (release/acquire flags per CTA).
 // Each element sees the FP32 operations of the kernel-per-step loop
 // (CgMvEpi, XrUpdOp, XpbyToOp) in the same order; only the order in which
 // the dot products add their terms differs (per thread over its rows, a
@@ -31,13 +32,13 @@
 // in every run). Every CTA computes alpha, beta and the stopping decision
 // from the same sums, so all leave the loop together.
 //
-// Grid reductions: each CTA adds its partial to a monotonic arrival counter;
-// the last to arrive sums the partials in index order and publishes the
-// result with a release store of the generation; the others wait for it with
-// acquire loads, bounded by the context's wait limit. A wait that runs out
-// sets the context's timeout flag and ends the kernel (the caller returns
-// KS_TIMEOUT); every CTA is resident (cooperative launch), so the waits end
-// as soon as the last CTA arrives.
+// Grid reductions: each CTA writes its partial sums and adds itself to a
+// monotonic arrival counter, waits with acquire loads until every CTA has
+// arrived, then adds all the partials itself in one fixed order (the same
+// bits in every CTA). Every wait is bounded by the context's wait limit; one
+// that runs out sets the context's timeout flag and ends the kernel (the
+// caller returns KS_TIMEOUT). Every CTA is resident (cooperative launch), so
+// the waits end as soon as the last CTA arrives.
 #pragma once
 
 #include "ks_kernels.cuh"
@@ -49,26 +50,36 @@ constexpr int kIrThreads = 1024;  // threads per CTA, one CTA per SM
 constexpr int kIrMaxK = 32;       // rows per thread (r and q in 64 TMEM columns)
 constexpr int kIrWarps = kIrThreads / 32;
 
-// Barrier state in device memory, zeroed before every launch.
+// Barrier state in device memory, zeroed before every launch: the grid
+// reductions' counter, generation and result, then one publication flag per
+// CTA (ir_sync_bytes).
 struct IrSync {
-  unsigned long long count;  // CTA arrivals, all generations
-  unsigned long long flag;   // the last completed generation
-  double result[2];
+  unsigned long long count;  // CTA arrivals at the reductions, all generations
+  unsigned long long reserved;
 };
+static_assert(sizeof(IrSync) % 8 == 0, "the publication flags follow IrSync");
+
+// Flag of CTA q right after IrSync: the last generation of p it has published.
+__device__ __forceinline__ unsigned long long *ir_pub(IrSync *s, int q) {
+  return reinterpret_cast<unsigned long long *>(s + 1) + q;
+}
+
+inline size_t ir_sync_bytes(int G) { return sizeof(IrSync) + sizeof(unsigned long long) * (size_t)G; }
 
 struct IrArgs {
-  const float *rin;  // the inner right-hand side, rounded to FP32 (n)
-  float *x;          // the inner solution z (n)
-  float *P;          // published directions (n)
-  DevState *st;      // the inner method's state
-  const int *outer_done;
-  double *partials;  // 2 per CTA
+  const void *rin;  // inner solve: r rounded to FP32; whole solve: b (FP64); n entries
+  void *x;          // the solution (the kernel's precision), n
+  void *P;          // published directions (the kernel's precision), n
+  DevState *st;     // the method's state
+  const int *outer_done;  // inner solve: the outer method's done; whole solve: null
+  double *partials;  // 4 per CTA (two generations of two sums)
   IrSync *sync;
   int *err;
   unsigned long long wait_ns;
   int n;
-  int rpc;  // rows per CTA, a multiple of 32
-  int K;    // rows per thread: ceil(rpc / kIrThreads) <= kIrMaxK
+  int rpc;    // rows per CTA, a multiple of 32
+  int K;      // rows per thread: ceil(rpc / kIrThreads) <= kIrMaxK (half for FP64)
+  int whole;  // 1: a whole CG solve (|b|, the stopping state and the history of the method)
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
@@ -108,62 +119,96 @@ __device__ __forceinline__ void ir_block_sum(double (&v)[2], double (*sh)[kIrWar
 
 // Grid-wide sums of (v0, v1), the same in every CTA; also a barrier (every
 // store the CTA's threads made before it is visible to every CTA after it).
-// Returns false when a wait ran out (the timeout flag is then set).
+// Each CTA writes its partials, counts itself in, waits (bounded) until all G
+// have, then sums all partials itself, every load issued before the first
+// add and the terms added in one fixed order, so every CTA obtains the same
+// bits. Returns false when a wait ran out (the timeout flag is then set).
+constexpr int kIrMaxGrid = 256;  // CTAs a reduction takes (one per SM)
+
 __device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long gen, double (&v)[2]) {
   __shared__ double sh[2][kIrWarps];
   __shared__ double s_res[2];
-  __shared__ int s_state;  // 1: last to arrive, 2: waited, 0: timed out
+  __shared__ int s_ok;
   ir_block_sum(v, sh);
   const unsigned G = gridDim.x;
+  // Two sets of partials, by the parity of the generation: a CTA writes
+  // generation g + 2's only after every CTA has arrived at g + 1, i.e. after
+  // every CTA has read generation g's.
+  double *part = a.partials + (size_t)(gen & 1) * 2 * G;
   if (threadIdx.x == 0) {
-    a.partials[2 * blockIdx.x] = v[0];
-    a.partials[2 * blockIdx.x + 1] = v[1];
+    part[2 * blockIdx.x] = v[0];
+    part[2 * blockIdx.x + 1] = v[1];
     __threadfence();
-    const unsigned long long old = atomicAdd(&a.sync->count, 1ull);
-    s_state = (old + 1 == gen * (unsigned long long)G) ? 1 : 2;
-  }
-  __syncthreads();
-  if (s_state == 1) {
-    if (threadIdx.x < 32) {
-      __threadfence();
-      double s0 = 0.0, s1 = 0.0;
-      for (unsigned b = threadIdx.x; b < G; b += 32) {
-        s0 += __ldcg(&a.partials[2 * b]);
-        s1 += __ldcg(&a.partials[2 * b + 1]);
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        s0 += __shfl_down_sync(0xffffffffu, s0, o);
-        s1 += __shfl_down_sync(0xffffffffu, s1, o);
-      }
-      if (threadIdx.x == 0) {
-        s_res[0] = s0;
-        s_res[1] = s1;
-        a.sync->result[0] = s0;
-        a.sync->result[1] = s1;
-        __threadfence();
-        st_release_u64(&a.sync->flag, gen);
-      }
-    }
-  } else if (threadIdx.x == 0) {
+    atomicAdd(&a.sync->count, 1ull);
+    s_ok = 1;
+    const unsigned long long want = gen * (unsigned long long)G;
     const unsigned long long t0 = global_ns();
-    while (ld_acquire_u64(&a.sync->flag) < gen) {
+    while (ld_acquire_u64(&a.sync->count) < want) {
       if (global_ns() - t0 > a.wait_ns) {
         atomicExch(a.err, 1);
-        s_state = 0;
+        s_ok = 0;
         break;
       }
     }
-    if (s_state) {
-      s_res[0] = __ldcg(&a.sync->result[0]);
-      s_res[1] = __ldcg(&a.sync->result[1]);
+  }
+  __syncthreads();
+  if (!s_ok) return false;
+  if (threadIdx.x < 32) {
+    constexpr int U = kIrMaxGrid / 32;
+    double p0[U], p1[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const unsigned b = threadIdx.x + 32u * u;
+      p0[u] = b < G ? __ldcg(&part[2 * b]) : 0.0;
+      p1[u] = b < G ? __ldcg(&part[2 * b + 1]) : 0.0;
+    }
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      s0 += p0[u];
+      s1 += p1[u];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_down_sync(0xffffffffu, s0, o);
+      s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    }
+    if (threadIdx.x == 0) {
+      s_res[0] = s0;
+      s_res[1] = s1;
     }
   }
   __syncthreads();
-  if (!s_state) return false;
   v[0] = s_res[0];
   v[1] = s_res[1];
   return true;
+}
+
+// After publishing its rows of p: release this CTA's flag, then wait until
+// the CTAs owning the columns its rows read ([bl, bh]) have published the same
+// generation. Replaces a grid barrier where only neighbours' values are read.
+// Returns false when a wait ran out (the timeout flag is then set).
+__device__ __forceinline__ bool ir_publish_sync(const IrArgs &a, unsigned long long gen, int bl, int bh) {
+  __shared__ int s_ok;
+  __syncthreads();  // every thread's stores of p are issued
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release_u64(ir_pub(a.sync, blockIdx.x), gen);
+    s_ok = 1;
+    const unsigned long long t0 = global_ns();
+    for (int q = bl; q <= bh && s_ok; q++) {
+      if (q == (int)blockIdx.x) continue;
+      while (ld_acquire_u64(ir_pub(a.sync, q)) < gen) {
+        if (global_ns() - t0 > a.wait_ns) {
+          atomicExch(a.err, 1);
+          s_ok = 0;
+          break;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  return s_ok != 0;
 }
 
 template <class MT>
@@ -188,115 +233,407 @@ __device__ __forceinline__ void tm_dealloc(uint32_t taddr, uint32_t ncols) {
 }
 __device__ __forceinline__ void tm_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tm_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// 2 consecutive columns of this warp's 32 lanes (one word per column per thread)
-__device__ __forceinline__ void tm_st2(uint32_t taddr, float a, float b) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(__float_as_uint(a)),
-               "r"(__float_as_uint(b))
+// N consecutive columns of this warp's 32 lanes (one word per column per thread)
+__device__ __forceinline__ void tm_st4(uint32_t taddr, const uint32_t (&w)[4]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(w[0]), "r"(w[1]),
+               "r"(w[2]), "r"(w[3])
                : "memory");
 }
-__device__ __forceinline__ void tm_ld2(uint32_t taddr, float &a, float &b) {
-  uint32_t u0, u1;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(u0), "=r"(u1) : "r"(taddr) : "memory");
-  // the registers are valid only after the wait; passing them through it
-  // keeps every use behind it
-  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(u0), "+r"(u1)::"memory");
-  a = __uint_as_float(u0);
-  b = __uint_as_float(u1);
+__device__ __forceinline__ void tm_ld4(uint32_t taddr, uint32_t (&w)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3])
+               : "r"(taddr)
+               : "memory");
+}
+// The registers of a load are valid only after the wait; passing them
+// through it keeps every use behind it.
+__device__ __forceinline__ void tm_wait_ld4(uint32_t (&w)[4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(w[0]), "+r"(w[1]), "+r"(w[2]), "+r"(w[3])::"memory");
+}
+__device__ __forceinline__ void tm_wait_ld8(uint32_t (&w)[4], uint32_t (&v)[4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(w[0]), "+r"(w[1]), "+r"(w[2]), "+r"(w[3]), "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3])::"memory");
 }
 __device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 constexpr uint32_t kIrTmemCols = 512;
+constexpr int kIrQ = 4;                     // consecutive rows a thread takes at a time
+constexpr int kIrTile = kIrThreads * kIrQ;  // rows of one pass of the CTA
 
-// y_row = sum_d A[row][row + off_d] * p[row + off_d] for one row, p from the
-// CTA's shared copy or, for other CTAs' rows, from P (every diagonal's value
-// loaded, zeros where the row has none: FP32 sums as in the SpMV kernel).
-template <class MT, int NDG>
-struct IrRow {
-  MT av[NDG > 0 ? NDG : kMaxDiag];
-  float pv[NDG > 0 ? NDG : kMaxDiag];
-  __device__ __forceinline__ void load(const DiaT<MT> &D, const IrArgs &a, const float *sp, int r0, int nr, int i,
-                                       int nd) {
-    constexpr int KD = NDG > 0 ? NDG : kMaxDiag;
+// A quad of a thread's rows in TMEM: 4 words per quad in FP32 (16 in the
+// thread's 32-word region, so 8 quads), 8 words in FP64 (4 quads).
+template <class VT>
+struct IrWords {
+  static constexpr int W = kIrQ * (int)sizeof(VT) / 4;  // words per quad
+  static constexpr int MaxQuads = 32 / W;
+  __device__ static void put(uint32_t taddr, const VT (&v)[kIrQ]) {
+    if constexpr (sizeof(VT) == 4) {
+      const uint32_t w[4] = {__float_as_uint(v[0]), __float_as_uint(v[1]), __float_as_uint(v[2]),
+                             __float_as_uint(v[3])};
+      tm_st4(taddr, w);
+    } else {
+      uint32_t w[4], x[4];
 #pragma unroll
-    for (int d = 0; d < KD; d++) {
-      if (NDG > 0 || d < nd) {
-        av[d] = ir_ld(D.vb[d] + (i + D.vs[d]));
-        const int c = min(max(i + D.off[d], D.cmin), D.cmax - 1);
-        const int lc = c - r0;
-        pv[d] = (lc >= 0 && lc < nr) ? sp[lc] : __ldcg(a.P + c);
+      for (int e = 0; e < 2; e++) {
+        const unsigned long long u0 = (unsigned long long)__double_as_longlong(v[e]);
+        const unsigned long long u1 = (unsigned long long)__double_as_longlong(v[2 + e]);
+        w[2 * e] = (uint32_t)u0;
+        w[2 * e + 1] = (uint32_t)(u0 >> 32);
+        x[2 * e] = (uint32_t)u1;
+        x[2 * e + 1] = (uint32_t)(u1 >> 32);
       }
+      tm_st4(taddr, w);
+      tm_st4(taddr + 4, x);
     }
   }
-  __device__ __forceinline__ float sum(int nd) const {
-    constexpr int KD = NDG > 0 ? NDG : kMaxDiag;
-    float q = 0.f;
+  // Two quads (r and q) loaded together, one wait.
+  __device__ static void get2(uint32_t ta, VT (&a)[kIrQ], uint32_t tb, VT (&b)[kIrQ]) {
+    if constexpr (sizeof(VT) == 4) {
+      uint32_t w[4], x[4];
+      tm_ld4(ta, w);
+      tm_ld4(tb, x);
+      tm_wait_ld8(w, x);
 #pragma unroll
-    for (int d = 0; d < KD; d++)
-      if (NDG > 0 || d < nd) q = add_rn(q, mul_rn(mval<float>(av[d]), pv[d]));
-    return q;
+      for (int e = 0; e < 4; e++) {
+        a[e] = __uint_as_float(w[e]);
+        b[e] = __uint_as_float(x[e]);
+      }
+    } else {
+      uint32_t w[4], x[4];
+      tm_ld4(ta, w);
+      tm_ld4(ta + 4, x);
+      tm_wait_ld8(w, x);
+      a[0] = __longlong_as_double((long long)(((unsigned long long)w[1] << 32) | w[0]));
+      a[1] = __longlong_as_double((long long)(((unsigned long long)w[3] << 32) | w[2]));
+      a[2] = __longlong_as_double((long long)(((unsigned long long)x[1] << 32) | x[0]));
+      a[3] = __longlong_as_double((long long)(((unsigned long long)x[3] << 32) | x[2]));
+      tm_ld4(tb, w);
+      tm_ld4(tb + 4, x);
+      tm_wait_ld8(w, x);
+      b[0] = __longlong_as_double((long long)(((unsigned long long)w[1] << 32) | w[0]));
+      b[1] = __longlong_as_double((long long)(((unsigned long long)w[3] << 32) | w[2]));
+      b[2] = __longlong_as_double((long long)(((unsigned long long)x[1] << 32) | x[0]));
+      b[3] = __longlong_as_double((long long)(((unsigned long long)x[3] << 32) | x[2]));
+    }
+  }
+  __device__ static void get(uint32_t ta, VT (&a)[kIrQ]) {
+    if constexpr (sizeof(VT) == 4) {
+      uint32_t w[4];
+      tm_ld4(ta, w);
+      tm_wait_ld4(w);
+#pragma unroll
+      for (int e = 0; e < 4; e++) a[e] = __uint_as_float(w[e]);
+    } else {
+      uint32_t w[4], x[4];
+      tm_ld4(ta, w);
+      tm_ld4(ta + 4, x);
+      tm_wait_ld8(w, x);
+      a[0] = __longlong_as_double((long long)(((unsigned long long)w[1] << 32) | w[0]));
+      a[1] = __longlong_as_double((long long)(((unsigned long long)w[3] << 32) | w[2]));
+      a[2] = __longlong_as_double((long long)(((unsigned long long)x[1] << 32) | x[0]));
+      a[3] = __longlong_as_double((long long)(((unsigned long long)x[3] << 32) | x[2]));
+    }
   }
 };
 
-// The inner solve (see the top of this file). Returns the stopping code, or
-// -1 when a wait ran out; *xw: x was written (one update at least).
-template <class MT, int NDG>
-__device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, float *sp, float *sx, uint32_t tm,
+// The largest K (rows per thread) the 64 TMEM words of a thread hold, r and q.
+template <class VT>
+constexpr int ir_max_k() {
+  return IrWords<VT>::MaxQuads * kIrQ;
+}
+
+// 4 consecutive elements, p[0..3] of one 16-byte-aligned (FP32) or 32-byte-
+// aligned (FP64) address; matrix values the same from an 8-byte (BF16) one.
+template <class T>
+__device__ __forceinline__ void ld4(const T *p, T (&v)[kIrQ], bool global_cg);
+template <>
+__device__ __forceinline__ void ld4<float>(const float *p, float (&v)[kIrQ], bool cg) {
+  const float4 u = cg ? __ldcg(reinterpret_cast<const float4 *>(p)) : __ldg(reinterpret_cast<const float4 *>(p));
+  v[0] = u.x;
+  v[1] = u.y;
+  v[2] = u.z;
+  v[3] = u.w;
+}
+template <>
+__device__ __forceinline__ void ld4<double>(const double *p, double (&v)[kIrQ], bool cg) {
+  const double2 *q = reinterpret_cast<const double2 *>(p);
+  const double2 a = cg ? __ldcg(q) : __ldg(q), b = cg ? __ldcg(q + 1) : __ldg(q + 1);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+template <>
+__device__ __forceinline__ void ld4<__nv_bfloat16>(const __nv_bfloat16 *p, __nv_bfloat16 (&v)[kIrQ], bool) {
+  const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+  v[0] = __ushort_as_bfloat16((unsigned short)(u.x & 0xffffu));
+  v[1] = __ushort_as_bfloat16((unsigned short)(u.x >> 16));
+  v[2] = __ushort_as_bfloat16((unsigned short)(u.y & 0xffffu));
+  v[3] = __ushort_as_bfloat16((unsigned short)(u.y >> 16));
+}
+template <class T>
+__device__ __forceinline__ void lds4(const T *p, T (&v)[kIrQ]) {  // shared memory, aligned as ld4
+  if constexpr (sizeof(T) == 4) {
+    const float4 u = *reinterpret_cast<const float4 *>(p);
+    v[0] = u.x;
+    v[1] = u.y;
+    v[2] = u.z;
+    v[3] = u.w;
+  } else {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+  }
+}
+template <class T>
+__device__ __forceinline__ void sts4(T *p, const T (&v)[kIrQ]) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+  }
+}
+template <class T>
+__device__ __forceinline__ void stcg4(T *p, const T (&v)[kIrQ]) {
+  if constexpr (sizeof(T) == 4) {
+    __stcg(reinterpret_cast<float4 *>(p), make_float4(v[0], v[1], v[2], v[3]));
+  } else {
+    __stcg(reinterpret_cast<double2 *>(p), make_double2(v[0], v[1]));
+    __stcg(reinterpret_cast<double2 *>(p) + 1, make_double2(v[2], v[3]));
+  }
+}
+
+// A quad of matrix values as loaded: packed where MT is narrower than 4
+// bytes (BF16: two per register, unpacked at use).
+template <class MT>
+struct IrVals {
+  MT v[kIrQ];
+  __device__ __forceinline__ float get(int e) const { return mval<float>(v[e]); }
+};
+template <>
+struct IrVals<__nv_bfloat16> {
+  uint2 u;
+  __device__ __forceinline__ float get(int e) const {
+    const unsigned w = e < 2 ? u.x : u.y;
+    return __uint_as_float((e & 1) ? (w & 0xffff0000u) : (w << 16));
+  }
+};
+
+// The values of diagonal d for rows i0 .. i0+3: one vector load where all 4
+// rows are present and the address is aligned, else one load per row.
+template <class MT>
+__device__ __forceinline__ void ir_vals(const MT *vp, bool full, int li0, int nr, IrVals<MT> &a) {
+  const bool aligned = (reinterpret_cast<uintptr_t>(vp) & (kIrQ * sizeof(MT) - 1)) == 0;
+  if constexpr (std::is_same<MT, __nv_bfloat16>::value) {
+    if (full && aligned) {
+      a.u = __ldg(reinterpret_cast<const uint2 *>(vp));
+    } else {
+      unsigned short h[kIrQ];
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) h[e] = li0 + e < nr ? __ldg(reinterpret_cast<const unsigned short *>(vp) + e) : 0;
+      a.u = make_uint2(h[0] | ((unsigned)h[1] << 16), h[2] | ((unsigned)h[3] << 16));
+    }
+  } else {
+    if (full && aligned) {
+      ld4<MT>(vp, a.v, false);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) a.v[e] = li0 + e < nr ? __ldg(vp + e) : (MT)0;
+    }
+  }
+}
+
+// p[c .. c+3] for an aligned column c: one vector load from the CTA's shared
+// copy or from P when the 4 columns are all on one side of the CTA's rows and
+// inside [cmin, cmax); else per column, clamped into the window (whose terms
+// have zero matrix values).
+template <class VT>
+__device__ __forceinline__ void ir_p4(const VT *sp, const VT *P, int r0, int nr, int cmin, int cmax, int c,
+                                      VT (&p)[kIrQ]) {
+  const int lc = c - r0;
+  if (lc >= 0 && lc + kIrQ <= nr) {
+    lds4<VT>(sp + lc, p);
+  } else if (c >= cmin && c + kIrQ <= cmax && (lc + kIrQ <= 0 || lc >= nr)) {
+    ld4<VT>(P + c, p, true);
+  } else {
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) {
+      const int cc = min(max(c + e, cmin), cmax - 1);
+      const int l = cc - r0;
+      p[e] = (l >= 0 && l < nr) ? sp[l] : __ldcg(P + cc);
+    }
+  }
+}
+
+// q = A p for the 4 consecutive rows i0 .. i0+3 (local li0 .. li0+3, i0 a
+// multiple of 4) of a thread, diagonals in ascending offset order (the
+// row's CSR order), in batches whose loads are all issued before the batch
+// is summed. p at an offset o: the aligned quad when 4 divides o, else the
+// two aligned quads around it and a funnel by o mod 4 (uniform across the
+// warp). Every diagonal's value is loaded (zeros where a row has none); FP64
+// adds only the terms the row's mask names, FP32 adds every one.
+template <class VT, class MT, int NDG>
+__device__ __forceinline__ void ir_quad_mv(const DiaT<MT> &D, const IrArgs &a, const VT *sp, int r0, int nr, int li0,
+                                           int nd, VT (&q)[kIrQ]) {
+  constexpr int KD = NDG > 0 ? NDG : kMaxDiag;
+  constexpr int B = sizeof(MT) == 2 ? KD : (sizeof(MT) == 4 ? 4 : 2);  // diagonals per batch
+  constexpr bool kMask = std::is_same<MT, double>::value;
+  const VT *P = (const VT *)a.P;
+  const int i0 = r0 + li0;
+  const bool full = li0 + kIrQ <= nr;
+  unsigned m = 0xffffffffu;  // the rows' mask bytes, row e in byte e
+  if constexpr (kMask) {
+    if (full) {
+      m = __ldg(reinterpret_cast<const unsigned *>(D.mask + i0));
+    } else {
+      m = 0;
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) m |= (unsigned)__ldg(D.mask + i0 + e) << (8 * e);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < kIrQ; e++) q[e] = (VT)0;
+#pragma unroll
+  for (int d0 = 0; d0 < KD; d0 += B) {
+    IrVals<MT> av[B];
+#pragma unroll
+    for (int u = 0; u < B; u++) {
+      const int d = d0 + u;
+      if (d < KD && (NDG > 0 || d < nd)) ir_vals<MT>(D.vb[d] + (i0 + D.vs[d]), full, li0, nr, av[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < B; u++) {
+      const int d = d0 + u;
+      if (d < KD && (NDG > 0 || d < nd)) {
+        const int c0 = i0 + D.off[d];
+        const int sh = c0 & (kIrQ - 1);
+        VT pv[kIrQ];
+        if (sh == 0) {
+          ir_p4<VT>(sp, P, r0, nr, D.cmin, D.cmax, c0, pv);
+        } else {
+          VT lo[kIrQ], hi[kIrQ];
+          ir_p4<VT>(sp, P, r0, nr, D.cmin, D.cmax, c0 - sh, lo);
+          ir_p4<VT>(sp, P, r0, nr, D.cmin, D.cmax, c0 - sh + kIrQ, hi);
+#pragma unroll
+          for (int e = 0; e < kIrQ; e++) {
+            const int k = e + sh;  // 1 .. 6
+            pv[e] = k == 1 ? lo[1] : k == 2 ? lo[2] : k == 3 ? lo[3] : k == 4 ? hi[0] : k == 5 ? hi[1] : hi[2];
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          VT val;
+          if constexpr (std::is_same<MT, __nv_bfloat16>::value)
+            val = av[u].get(e);
+          else
+            val = (VT)av[u].v[e];
+          const VT t = add_rn(q[e], mul_rn(val, pv[e]));
+          if constexpr (kMask)
+            q[e] = ((m >> (8 * e + d)) & 1u) ? t : q[e];
+          else
+            q[e] = t;
+        }
+      }
+    }
+  }
+}
+
+// The solve (see the top of this file). Returns the stopping code, or -1
+// when a wait ran out; *xw: x was written (one update at least).
+template <class VT, class MT, int NDG>
+__device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *sp, VT *sx, uint32_t tm,
                                        long long *Lout, double *alpha_out, double *beta_out, double *rr_out,
                                        bool *xw) {
+  using TW = IrWords<VT>;
   const int nd = NDG > 0 ? NDG : D.nd;
   const int t = threadIdx.x;
   const int r0 = blockIdx.x * a.rpc;
   const int nr = max(0, min(a.rpc, a.n - r0));
+  const bool lead = blockIdx.x == 0 && t == 0;  // keeps the method's state (whole solve)
   DevState *st = a.st;
+  VT *P = (VT *)a.P;
   const double eps = st->k.s[S_EPS];
-  const double bnorm = st->k.s[S_BNORM];
   const long long maxloop = st->k.aux[A_MAXLOOP];
-  double rr = st->k.s[S_RR];
-  const int K2 = (a.K + 1) / 2;  // row pairs per thread
-  const uint32_t tr = tm, tq = tm + 32;  // this thread's r_k at column tr + k, q_k at tq + k
+  const int quads = (a.rpc + kIrTile - 1) / kIrTile;  // quads per thread
+  const uint32_t tr = tm, tq = tm + 32;  // this thread's r at column tr + W j, q at tq + W j
+  // the CTAs owning the columns this CTA's rows read
+  int bl = blockIdx.x, bh = blockIdx.x;
+  if (nr > 0) {
+    const int lo = max(r0 + D.off[0], D.cmin), hi = min(r0 + nr - 1 + D.off[nd - 1], D.cmax - 1);
+    bl = min(bl, lo / a.rpc);
+    bh = max(bh, hi / a.rpc);
+  }
 
   // start: r = b (TMEM), p = r (shared memory and P), x = 0
-  for (int j = 0; j < K2; j++) {
-    float v[2];
+  double acc = 0.0;
+  for (int j = 0; j < quads; j++) {
+    const int li0 = j * kIrTile + kIrQ * t;
+    VT v[kIrQ];
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
-      const int li = t + (2 * j + u) * kIrThreads;
-      v[u] = 0.f;
+    for (int e = 0; e < kIrQ; e++) {
+      const int li = li0 + e;
+      v[e] = (VT)0;
       if (li < nr) {
-        v[u] = __ldcg(a.rin + r0 + li);
-        sp[li] = v[u];
-        sx[li] = 0.f;
-        __stcg(a.P + r0 + li, v[u]);
+        v[e] = __ldcg((const VT *)a.rin + r0 + li);
+        sp[li] = v[e];
+        sx[li] = (VT)0;
+        __stcg(P + r0 + li, v[e]);
+        acc = add_rn(acc, mul_rn(widen(v[e]), widen(v[e])));
       }
     }
-    tm_st2(tr + 2 * j, v[0], v[1]);
+    TW::put(tr + TW::W * j, v);
   }
   tm_wait_st();
-  unsigned long long gen = 0;
+  unsigned long long gen = 0, pgen = 1;  // reductions, publications of p
   double v[2] = {0.0, 0.0};
-  if (!ir_allreduce(a, ++gen, v)) return -1;  // every p published
-
+  double rr, bnorm;
   int code = kRunning;
+  if (a.whole) {
+    // |b| and the stopping test at the top of iteration 1 (NormBOp, StartZeroOp)
+    v[0] = acc;
+    if (!ir_allreduce(a, ++gen, v)) return -1;
+    rr = v[0];
+    bnorm = sqrt(rr);
+    const double err = sqrt(rr) / bnorm;
+    if (1 > maxloop)
+      code = kMaxLoop;
+    else if (err <= eps)
+      code = kConverged;
+    else if (err != err)
+      code = kNaN;
+    if (lead) {
+      st->k.s[S_BNORM] = bnorm;
+      st->k.s[S_RR] = rr;
+      check_top(st, 1, err);
+    }
+    if (code != kRunning) return code;
+  } else {
+    rr = st->k.s[S_RR];
+    bnorm = st->k.s[S_BNORM];
+  }
+  if (!ir_publish_sync(a, pgen, bl, bh)) return -1;
+
   double alpha = 0.0, beta = 0.0;
   long long L = 1;
   for (; L <= maxloop; L++) {
-    // A: q = A p (two rows' loads in flight per thread), (p, q)
-    double acc = 0.0;
-    for (int j = 0; j < K2; j++) {
-      const int l0 = t + 2 * j * kIrThreads, l1 = l0 + kIrThreads;
-      IrRow<MT, NDG> R0, R1;
-      if (l0 < nr) R0.load(D, a, sp, r0, nr, r0 + l0, nd);
-      if (l1 < nr) R1.load(D, a, sp, r0, nr, r0 + l1, nd);
-      float q0 = 0.f, q1 = 0.f;
-      if (l0 < nr) {
-        q0 = R0.sum(nd);
-        acc = add_rn(acc, mul_rn(widen(sp[l0]), widen(q0)));
+    // A: q = A p, (p, q)
+    acc = 0.0;
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      VT q[kIrQ];
+      if (li0 < nr) {
+        ir_quad_mv<VT, MT, NDG>(D, a, sp, r0, nr, li0, nd, q);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++)
+          if (li0 + e < nr) acc = add_rn(acc, mul_rn(widen(sp[li0 + e]), widen(q[e])));
+      } else {
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) q[e] = (VT)0;
       }
-      if (l1 < nr) {
-        q1 = R1.sum(nd);
-        acc = add_rn(acc, mul_rn(widen(sp[l1]), widen(q1)));
-      }
-      tm_st2(tq + 2 * j, q0, q1);
+      TW::put(tq + TW::W * j, q);
     }
     tm_wait_st();
     v[0] = acc;
@@ -306,30 +643,31 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, float
     if (v[0] == 0.0) {
       code = kBreakdown;
       alpha = 0.0;
-      break;
+    } else {
+      alpha = div_rn(rr, v[0]);
+      if (!isfinite(alpha)) code = kNaN;
     }
-    alpha = div_rn(rr, v[0]);
-    if (!isfinite(alpha)) {
-      code = kNaN;
+    if (code != kRunning) {
+      if (lead && a.whole) set_done(st, code);
       break;
     }
     // B: x += alpha p, r -= alpha q, (r, r)
-    const float af = (float)alpha;
+    const VT av = (VT)alpha;
     acc = 0.0;
-    for (int j = 0; j < K2; j++) {
-      float rv[2], qv[2];
-      tm_ld2(tr + 2 * j, rv[0], rv[1]);
-      tm_ld2(tq + 2 * j, qv[0], qv[1]);
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      VT rv[kIrQ], qv[kIrQ];
+      TW::get2(tr + TW::W * j, rv, tq + TW::W * j, qv);
 #pragma unroll
-      for (int u = 0; u < 2; u++) {
-        const int li = t + (2 * j + u) * kIrThreads;
+      for (int e = 0; e < kIrQ; e++) {
+        const int li = li0 + e;
         if (li < nr) {
-          sx[li] = add_rn(mul_rn(af, sp[li]), sx[li]);
-          rv[u] = add_rn(mul_rn(-af, qv[u]), rv[u]);
-          acc = add_rn(acc, mul_rn(widen(rv[u]), widen(rv[u])));
+          sx[li] = add_rn(mul_rn(av, sp[li]), sx[li]);
+          rv[e] = add_rn(mul_rn((VT)(-av), qv[e]), rv[e]);
+          acc = add_rn(acc, mul_rn(widen(rv[e]), widen(rv[e])));
         }
       }
-      tm_st2(tr + 2 * j, rv[0], rv[1]);
+      TW::put(tr + TW::W * j, rv);
     }
     tm_wait_st();
     *xw = true;
@@ -339,38 +677,54 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, float
     // beta = (r, r)_new / (r, r); then the stopping test at the top of
     // iteration L + 1 (check_top), whose verdict overrides beta's
     const double rr2 = v[0];
+    int bcode = kRunning;
     if (rr == 0.0) {
-      code = kBreakdown;
+      bcode = kBreakdown;
       beta = 0.0;
     } else {
       beta = div_rn(rr2, rr);
-      if (!isfinite(beta)) code = kNaN;
+      if (!isfinite(beta)) bcode = kNaN;
     }
     rr = rr2;
     const double err = sqrt(rr2) / bnorm;
+    code = bcode;
     if (L + 1 > maxloop)
       code = kMaxLoop;
     else if (err <= eps)
       code = kConverged;
     else if (err != err)
       code = kNaN;
+    if (lead && a.whole) {
+      if (bcode != kRunning) set_done(st, bcode);
+      check_top(st, L + 1, err);
+    }
     if (code != kRunning) break;
     // C: p = beta p + r, published
-    const float bf = (float)beta;
-    for (int j = 0; j < K2; j++) {
-      float rv[2];
-      tm_ld2(tr + 2 * j, rv[0], rv[1]);
+    const VT bv = (VT)beta;
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      VT rv[kIrQ];
+      TW::get(tr + TW::W * j, rv);
+      if (li0 + kIrQ <= nr) {
+        VT pv[kIrQ];
+        lds4<VT>(sp + li0, pv);
 #pragma unroll
-      for (int u = 0; u < 2; u++) {
-        const int li = t + (2 * j + u) * kIrThreads;
-        if (li < nr) {
-          const float pn = add_rn(mul_rn(bf, sp[li]), rv[u]);
-          sp[li] = pn;
-          __stcg(a.P + r0 + li, pn);
+        for (int e = 0; e < kIrQ; e++) pv[e] = add_rn(mul_rn(bv, pv[e]), rv[e]);
+        sts4<VT>(sp + li0, pv);
+        stcg4<VT>(P + r0 + li0, pv);
+      } else {
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          const int li = li0 + e;
+          if (li < nr) {
+            const VT pn = add_rn(mul_rn(bv, sp[li]), rv[e]);
+            sp[li] = pn;
+            __stcg(P + r0 + li, pn);
+          }
         }
       }
     }
-    if (!ir_allreduce(a, ++gen, v)) return -1;
+    if (!ir_publish_sync(a, ++pgen, bl, bh)) return -1;
   }
   *Lout = L;
   *alpha_out = alpha;
@@ -379,18 +733,18 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, float
   return code;
 }
 
-template <class MT, int NDG>
-__global__ void __launch_bounds__(kIrThreads, 1) k_inner_cg_resident(DiaT<MT> D, IrArgs a) {
-  extern __shared__ __align__(16) float ir_smem[];
+template <class VT, class MT, int NDG>
+__global__ void __launch_bounds__(kIrThreads, 1) k_cg_onchip(DiaT<MT> D, IrArgs a) {
+  extern __shared__ __align__(16) unsigned char ir_smem_raw[];
   __shared__ uint32_t s_tmem;
-  float *sp = ir_smem;          // p of the CTA's rows
-  float *sx = ir_smem + a.rpc;  // x of the CTA's rows
+  VT *sp = reinterpret_cast<VT *>(ir_smem_raw);  // p of the CTA's rows
+  VT *sx = sp + a.rpc;                           // x of the CTA's rows
   const int t = threadIdx.x;
   DevState *st = a.st;
   // The start conditions come from kernels that completed before this one,
   // so every CTA reads the same values and all of them return here together.
-  if (*(volatile const int *)a.outer_done) return;
-  if (*(volatile const int *)&st->k.done != kRunning) return;  // x stays 0 (A_XZERO)
+  if (a.outer_done && *(volatile const int *)a.outer_done) return;
+  if (*(volatile const int *)&st->k.done != kRunning) return;  // inner: x stays 0 (A_XZERO)
   if (t < 32) {
     tm_alloc(&s_tmem, kIrTmemCols);
     tm_relinquish();
@@ -403,21 +757,24 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_inner_cg_resident(DiaT<MT> D,
   long long L = 0;
   double alpha = 0.0, beta = 0.0, rr = 0.0;
   bool xw = false;
-  const int code = ir_body<MT, NDG>(D, a, sp, sx, tm, &L, &alpha, &beta, &rr, &xw);
+  const int code = ir_body<VT, MT, NDG>(D, a, sp, sx, tm, &L, &alpha, &beta, &rr, &xw);
   if (code >= 0) {
-    // x out; the state the kernel-per-step loop leaves (nothing pending)
+    // x out (a whole solve writes its zeros too)
     const int r0 = blockIdx.x * a.rpc;
     const int nr = max(0, min(a.rpc, a.n - r0));
-    if (xw)
-      for (int li = t; li < nr; li += kIrThreads) __stcg(a.x + r0 + li, sx[li]);
+    VT *x = (VT *)a.x;
+    if (xw || a.whole)
+      for (int li = t; li < nr; li += kIrThreads) __stcg(x + r0 + li, xw ? sx[li] : (VT)0);
     if (blockIdx.x == 0 && t == 0) {
-      st->k.done = code == kRunning ? kMaxLoop : code;
-      st->k.loop = code == kBreakdown || code == kNaN ? L : L + 1;
       st->k.s[S_ALPHA] = alpha;
       st->k.s[S_BETA] = beta;
-      st->k.s[S_RR] = rr;
-      st->k.aux[A_PENDING] = 0;
-      st->k.aux[A_XZERO] = xw ? 0 : 1;
+      if (!a.whole) {  // the state the kernel-per-step inner loop leaves (nothing pending)
+        st->k.done = code == kRunning ? kMaxLoop : code;
+        st->k.loop = code == kBreakdown || code == kNaN ? L : L + 1;
+        st->k.s[S_RR] = rr;
+        st->k.aux[A_PENDING] = 0;
+        st->k.aux[A_XZERO] = xw ? 0 : 1;
+      }
     }
   }
   // every thread's TMEM accesses are complete (each waited on its own); the
@@ -436,8 +793,9 @@ struct IrShape {
   size_t smem = 0;
 };
 
-// False when the system does not fit: r of a thread's rows in registers
-// (K <= kIrMaxK), p and q of a CTA's rows in shared memory.
+// False when the system does not fit: r and q of a thread's rows in its 64
+// TMEM words (K <= ir_max_k), p and x of a CTA's rows in shared memory.
+template <class VT>
 inline bool ir_shape(const ks_ctx *ctx, long long n, IrShape *s) {
   if (n < 1) return false;
   int optin = 0;
@@ -448,8 +806,8 @@ inline bool ir_shape(const ks_ctx *ctx, long long n, IrShape *s) {
   const long long G = ctx->num_sms;
   const long long rpc = ((n + G - 1) / G + 31) / 32 * 32;
   const long long K = (rpc + kIrThreads - 1) / kIrThreads;
-  const size_t smem = sizeof(float) * 2 * (size_t)rpc;
-  if (K > kIrMaxK || smem + 2048 > (size_t)optin) return false;  // room for the static shared arrays
+  const size_t smem = sizeof(VT) * 2 * (size_t)rpc;
+  if (K > ir_max_k<VT>() || G > kIrMaxGrid || smem + 2048 > (size_t)optin) return false;  // + the static arrays
   s->G = (int)G;
   s->rpc = (int)rpc;
   s->K = (int)K;
@@ -458,11 +816,11 @@ inline bool ir_shape(const ks_ctx *ctx, long long n, IrShape *s) {
 }
 
 // Cooperative launch of one CTA per SM; `probe`: only check that the grid
-// can be co-resident (sets *fits).
-template <class MT, int NDG>
+// can be co-resident (sets *fits). `cls`: its class in a profiled solve.
+template <class VT, class MT, int NDG>
 inline cudaError_t ir_launch_n(ks_ctx *ctx, const CsrDev &A, const IrArgs &a, const IrShape &sh, bool probe,
-                               bool *fits) {
-  auto fn = k_inner_cg_resident<MT, NDG>;
+                               bool *fits, int cls) {
+  auto fn = k_cg_onchip<VT, MT, NDG>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
   if (e != cudaSuccess) return e;
   if (probe) {
@@ -482,16 +840,16 @@ inline cudaError_t ir_launch_n(ks_ctx *ctx, const CsrDev &A, const IrArgs &a, co
   cfg.attrs = at;
   cfg.numAttrs = 1;
   ctx->launches++;
-  ProfLaunch pl(ctx, kOther);  // a whole inner solve: SpMVs, dots and updates
+  ProfLaunch pl(ctx, cls);
   return cudaLaunchKernelEx(&cfg, fn, dview<MT>(A), a);
 }
 
-template <class MT>
+template <class VT, class MT>
 inline cudaError_t ir_launch(ks_ctx *ctx, const CsrDev &A, const IrArgs &a, const IrShape &sh, bool probe,
-                             bool *fits) {
-  if (A.dia_nd == 7) return ir_launch_n<MT, 7>(ctx, A, a, sh, probe, fits);
-  if (A.dia_nd == 5) return ir_launch_n<MT, 5>(ctx, A, a, sh, probe, fits);
-  return ir_launch_n<MT, 0>(ctx, A, a, sh, probe, fits);
+                             bool *fits, int cls) {
+  if (A.dia_nd == 7) return ir_launch_n<VT, MT, 7>(ctx, A, a, sh, probe, fits, cls);
+  if (A.dia_nd == 5) return ir_launch_n<VT, MT, 5>(ctx, A, a, sh, probe, fits, cls);
+  return ir_launch_n<VT, MT, 0>(ctx, A, a, sh, probe, fits, cls);
 }
 
 }  // namespace ks

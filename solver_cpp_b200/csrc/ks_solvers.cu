@@ -797,11 +797,40 @@ inline bool run_cg_resident(const Env<double> &E, const double *b, double *x, ks
   return true;
 }
 
+// Larger systems whose vectors fit on chip across the GPU (up to about 14,400
+// rows per SM in FP64, one GPU, a diagonal copy; ks_params.cluster_solve 0):
+// the whole solve as one cooperative kernel of one CTA per SM, r and q in
+// TMEM, p and x in shared memory (k_cg_onchip, ks_inner_resident.cuh): no
+// kernel boundary and no vector pass through HBM per iteration, only the
+// matrix and the neighbouring CTAs' p. Returns false, having launched
+// nothing, when the system does not qualify.
+inline bool run_cg_onchip(const Env<double> &E, const double *b, double *x, double *P, ks_status *s) {
+  if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A->dia_nd || !E.A->dia_val) return false;
+  ks_ctx *ctx = E.ctx;
+  IrShape sh;
+  if (!ir_shape<double>(ctx, E.n, &sh)) return false;
+  bool fits = false;
+  const IrArgs probe{};
+  if (ir_launch<double, double>(ctx, *E.A, probe, sh, true, &fits, 0) != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  if (reinterpret_cast<uintptr_t>(P) % 32) return false;  // 32-byte vector loads of P
+  launch_scalar(ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  const IrArgs a{b, x, P, E.st, nullptr, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
+                 (int)E.n, sh.rpc, sh.K, 1};
+  cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes(sh.G), ctx->stream);
+  if (e == cudaSuccess) e = ir_launch<double, double>(ctx, *E.A, a, sh, false, &fits, kOther);
+  *s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip CG launch");
+  return true;
+}
+
 template <class VT>
 ks_status run_cg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   if constexpr (std::is_same<VT, double>::value) {
     ks_status s = KS_OK;
     if (run_cg_resident(E, b, x, &s)) return s;
+    if (run_cg_onchip(E, b, x, ws, &s)) return s;
   }
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take();
@@ -1943,12 +1972,12 @@ struct InnerResBufs {
 inline ks_status run_cg_inner_resident(const Env<float> &E, const InnerResBufs &B, const IrShape &sh) {
   ks_ctx *ctx = E.ctx;
   IrArgs a{B.r, B.x, B.P, E.st, E.outer_done, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
-           (int)E.n, sh.rpc, sh.K};
-  cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, sizeof(IrSync), ctx->stream);
+           (int)E.n, sh.rpc, sh.K, 0};
+  cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes(sh.G), ctx->stream);
   if (e == cudaSuccess) {
     bool fits = false;
-    e = E.mvals == KS_BF16 ? ir_launch<__nv_bfloat16>(ctx, *E.A, a, sh, false, &fits)
-                           : ir_launch<float>(ctx, *E.A, a, sh, false, &fits);
+    e = E.mvals == KS_BF16 ? ir_launch<float, __nv_bfloat16>(ctx, *E.A, a, sh, false, &fits, kMvLow)
+                           : ir_launch<float, float>(ctx, *E.A, a, sh, false, &fits, kMvLow);
   }
   return e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip inner CG launch");
 }
@@ -1985,19 +2014,20 @@ void InnerRunner<VT>::setup_resident() {
   if (method != KS_CG || iprec == KS_FP64 || E32.comm || !E32.A || !E32.A->dia_nd) return;
   if (iprec == KS_FP32 ? !E32.A->dia_val32 : !E32.A->dia_val16) return;
   if (vec_count(KS_CG, E32.sp, E32.n, sizeof(float), ctx->l2_bytes) < 2) return;
-  if (!ir_shape(ctx, E32.n, &sh)) return;
+  if (!ir_shape<float>(ctx, E32.n, &sh)) return;
   bool fits = false;
   const IrArgs none{};
-  const cudaError_t e = iprec == KS_BF16 ? ir_launch<__nv_bfloat16>(ctx, *E32.A, none, sh, true, &fits)
-                                         : ir_launch<float>(ctx, *E32.A, none, sh, true, &fits);
+  const cudaError_t e = iprec == KS_BF16 ? ir_launch<float, __nv_bfloat16>(ctx, *E32.A, none, sh, true, &fits, 0)
+                                         : ir_launch<float, float>(ctx, *E32.A, none, sh, true, &fits, 0);
   if (e != cudaSuccess || !fits) {
     (void)cudaGetLastError();
     return;
   }
   Ws<float> W{ws32, E32.ld, E32.off};
+  fb.P = W.take();  // the first slot: 16-byte vector loads of P need its alignment
   fb.r = W.take();
-  fb.P = W.take();
   fb.x = z32;
+  if (reinterpret_cast<uintptr_t>(fb.P) % 16) return;
   res_cg = true;
 }
 
@@ -2525,8 +2555,10 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     }
     if (prm->x_ref && !dist) {  // |x - x_ref| / |x_ref| over the solution
       launch_vec(ctx, n, DiffNormOp{x, prm->x_ref, ctx->d_result}, Stop{nullptr, nullptr});
-      double s2[2];
-      KS_CUDA(ctx, cudaMemcpy(s2, ctx->d_result, sizeof(s2), cudaMemcpyDeviceToHost));
+      KS_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, ctx->d_result, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+      KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      const double s2[2] = {ctx->h_pinned[0], ctx->h_pinned[1]};
       rep->x_rel_diff = s2[1] > 0.0 ? std::sqrt(s2[0]) / std::sqrt(s2[1]) : (s2[0] > 0.0 ? INFINITY : 0.0);
     }
     if (dist) {  // summed over the ranks after the solve
