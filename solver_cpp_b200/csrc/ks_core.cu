@@ -390,11 +390,14 @@ static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long lo
     free_dia(A);
     return false;
   };
-  if (!got(cudaMalloc(&A.dia_val, sizeof(double) * (size_t)len)) || !got(cudaMalloc(&A.dia_mask, (size_t)A.n))) {
+  // + 8 elements of tail: 4-row vector loads of the last diagonal's last rows
+  if (!got(cudaMalloc(&A.dia_val, sizeof(double) * (size_t)(len + 8))) ||
+      !got(cudaMalloc(&A.dia_mask, (size_t)A.n + 8))) {
     cudaFree(d_buf);
     return KS_OK;
   }
-  KS_CUDA(ctx, cudaMemsetAsync(A.dia_val, 0, sizeof(double) * (size_t)len, ctx->stream));
+  KS_CUDA(ctx, cudaMemsetAsync(A.dia_val, 0, sizeof(double) * (size_t)(len + 8), ctx->stream));
+  KS_CUDA(ctx, cudaMemsetAsync(A.dia_mask, 0, (size_t)A.n + 8, ctx->stream));
   k_dia_fill<<<g, 256, 0, ctx->stream>>>(A.ptr, A.col, A.val, A.n, o, A.dia_val, A.dia_mask);
   KS_CUDA(ctx, cudaGetLastError());
   // symmetric half storage
@@ -417,11 +420,15 @@ static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long lo
     sym = flag == 0;
   }
   cudaFree(d_buf);
-  long long ds = A.n, stored = len;
+  long long ds = A.n, stored = len + 8;
   int pad = 0;
   if (sym) {
-    pad = -o.off[0];
-    ds = (long long)pad + A.n;
+    // the lower diagonals' reads start up to -off[0] rows before row 0; the
+    // pad and the stride are whole multiples of 4 elements with 4 to spare
+    // either side, so 4-row vector loads of any diagonal stay inside the copy
+    // and aligned
+    pad = ((-o.off[0] + 3) / 4) * 4 + 4;
+    ds = ((long long)pad + A.n + 3) / 4 * 4 + 8;
     stored = (long long)(h + 1) * ds;
     double *sv = nullptr;
     if (cudaMalloc(&sv, sizeof(double) * (size_t)stored) == cudaSuccess) {
@@ -436,7 +443,7 @@ static ks_status build_diagonals(ks_ctx *ctx, CsrDev &A, unsigned flags, long lo
       (void)cudaGetLastError();
       sym = false;
       ds = A.n;
-      stored = len;
+      stored = len + 8;
       pad = 0;
     }
   }

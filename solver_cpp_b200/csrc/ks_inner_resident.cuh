@@ -5,7 +5,8 @@
 // times; launched kernel by kernel, each iteration streams r, p, q and x
 // through L2/HBM and pays three kernel boundaries. This kernel runs the whole
 // inner solve in one cooperative launch of one CTA per SM. CTA b owns rows
-// [b*rpc, (b+1)*rpc); thread t of it owns the rows b*rpc + t + 1024 k:
+// [b*rpc, (b+1)*rpc); thread t of it owns the quads of 4 consecutive rows
+// b*rpc + 4096 j + 4 t .. +3 (j = 0, 1, ...):
 //   * r and q of its rows live in tensor memory (TMEM, 256 KB per SM, which
 //     no tensor-core work needs here): warp w reaches TMEM lanes
 //     32 (w % 4) .. +31 and takes columns 64 (w / 4) .. +63 of them, so every
@@ -15,8 +16,8 @@
 //     also published to a global array P from which the other CTAs gather it,
 //     x is written out once, at the end,
 //   * the matrix (the diagonal copy, FP32 or BF16 values, either layout) is
-//     read from global memory (L2) every iteration; the registers left free
-//     keep the loads of two rows in flight per thread.
+//     read from global memory (L2) every iteration, one vector load per
+//     diagonal and quad where aligned.
 // The TMEM columns are allocated once per launch and released on every way
 // out of the kernel (a timed-out wait included).
 // Per iteration (cg.cpp:184-240):
@@ -72,7 +73,7 @@ struct IrArgs {
   void *P;          // published directions (the kernel's precision), n
   DevState *st;     // the method's state
   const int *outer_done;  // inner solve: the outer method's done; whole solve: null
-  double *partials;  // 4 per CTA (two generations of two sums)
+  double *partials;  // 2 kIrMaxSums per CTA (two generations)
   IrSync *sync;
   int *err;
   unsigned long long wait_ns;
@@ -92,52 +93,55 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Sums of two values over the CTA's 1024 threads in a fixed order; the
-// result is valid in thread 0.
-__device__ __forceinline__ void ir_block_sum(double (&v)[2], double (*sh)[kIrWarps]) {
+// Sums of N values over the CTA's 1024 threads in a fixed order; the result
+// is valid in thread 0.
+template <int N>
+__device__ __forceinline__ void ir_block_sum(double (&v)[N], double (*sh)[kIrWarps]) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-  for (int d = 0; d < 2; d++) {
+  for (int d = 0; d < N; d++) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[d] += __shfl_down_sync(0xffffffffu, v[d], o);
   }
   if (lane == 0) {
-    sh[0][w] = v[0];
-    sh[1][w] = v[1];
+#pragma unroll
+    for (int d = 0; d < N; d++) sh[d][w] = v[d];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s0 = 0.0, s1 = 0.0;
-    for (int i = 0; i < kIrWarps; i++) {
-      s0 += sh[0][i];
-      s1 += sh[1][i];
+#pragma unroll
+    for (int d = 0; d < N; d++) {
+      double s0 = 0.0;
+      for (int i = 0; i < kIrWarps; i++) s0 += sh[d][i];
+      v[d] = s0;
     }
-    v[0] = s0;
-    v[1] = s1;
   }
 }
 
-// Grid-wide sums of (v0, v1), the same in every CTA; also a barrier (every
+// Grid-wide sums of N values, the same in every CTA; also a barrier (every
 // store the CTA's threads made before it is visible to every CTA after it).
 // Each CTA writes its partials, counts itself in, waits (bounded) until all G
 // have, then sums all partials itself, every load issued before the first
 // add and the terms added in one fixed order, so every CTA obtains the same
 // bits. Returns false when a wait ran out (the timeout flag is then set).
 constexpr int kIrMaxGrid = 256;  // CTAs a reduction takes (one per SM)
+constexpr int kIrMaxSums = 2;    // values one reduction carries
 
-__device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long gen, double (&v)[2]) {
-  __shared__ double sh[2][kIrWarps];
-  __shared__ double s_res[2];
+template <int N>
+__device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long gen, double (&v)[N]) {
+  static_assert(N >= 1 && N <= kIrMaxSums, "values per reduction");
+  __shared__ double sh[kIrMaxSums][kIrWarps];
+  __shared__ double s_res[kIrMaxSums];
   __shared__ int s_ok;
-  ir_block_sum(v, sh);
+  ir_block_sum<N>(v, sh);
   const unsigned G = gridDim.x;
   // Two sets of partials, by the parity of the generation: a CTA writes
   // generation g + 2's only after every CTA has arrived at g + 1, i.e. after
   // every CTA has read generation g's.
-  double *part = a.partials + (size_t)(gen & 1) * 2 * G;
+  double *part = a.partials + (size_t)(gen & 1) * kIrMaxSums * G;
   if (threadIdx.x == 0) {
-    part[2 * blockIdx.x] = v[0];
-    part[2 * blockIdx.x + 1] = v[1];
+#pragma unroll
+    for (int d = 0; d < N; d++) part[(size_t)d * G + blockIdx.x] = v[d];
     __threadfence();
     atomicAdd(&a.sync->count, 1ull);
     s_ok = 1;
@@ -155,32 +159,25 @@ __device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long
   if (!s_ok) return false;
   if (threadIdx.x < 32) {
     constexpr int U = kIrMaxGrid / 32;
-    double p0[U], p1[U];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      const unsigned b = threadIdx.x + 32u * u;
-      p0[u] = b < G ? __ldcg(&part[2 * b]) : 0.0;
-      p1[u] = b < G ? __ldcg(&part[2 * b + 1]) : 0.0;
-    }
-    double s0 = 0.0, s1 = 0.0;
+    for (int d = 0; d < N; d++) {
+      double pv[U];
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      s0 += p0[u];
-      s1 += p1[u];
-    }
+      for (int u = 0; u < U; u++) {
+        const unsigned b = threadIdx.x + 32u * u;
+        pv[u] = b < G ? __ldcg(&part[(size_t)d * G + b]) : 0.0;
+      }
+      double s0 = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      s0 += __shfl_down_sync(0xffffffffu, s0, o);
-      s1 += __shfl_down_sync(0xffffffffu, s1, o);
-    }
-    if (threadIdx.x == 0) {
-      s_res[0] = s0;
-      s_res[1] = s1;
+      for (int u = 0; u < U; u++) s0 += pv[u];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s0 += __shfl_down_sync(0xffffffffu, s0, o);
+      if (threadIdx.x == 0) s_res[d] = s0;
     }
   }
   __syncthreads();
-  v[0] = s_res[0];
-  v[1] = s_res[1];
+#pragma unroll
+  for (int d = 0; d < N; d++) v[d] = s_res[d];
   return true;
 }
 
@@ -446,6 +443,18 @@ __device__ __forceinline__ void ir_vals(const MT *vp, bool full, int li0, int nr
   }
 }
 
+// A thread's own quad of a shared-memory vector: one vector access for a full
+// quad (a scalar one per row would hit 4 threads on one bank), else per row.
+template <class VT>
+__device__ __forceinline__ void ir_own4(const VT *v, int li0, int nr, VT (&o)[kIrQ]) {
+  if (li0 + kIrQ <= nr) {
+    lds4<VT>(v + li0, o);
+  } else {
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) o[e] = li0 + e < nr ? v[li0 + e] : (VT)0;
+  }
+}
+
 // p[c .. c+3] for an aligned column c: one vector load from the CTA's shared
 // copy or from P when the 4 columns are all on one side of the CTA's rows and
 // inside [cmin, cmax); else per column, clamped into the window (whose terms
@@ -575,13 +584,23 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
 #pragma unroll
     for (int e = 0; e < kIrQ; e++) {
       const int li = li0 + e;
-      v[e] = (VT)0;
-      if (li < nr) {
-        v[e] = __ldcg((const VT *)a.rin + r0 + li);
-        sp[li] = v[e];
-        sx[li] = (VT)0;
-        __stcg(P + r0 + li, v[e]);
-        acc = add_rn(acc, mul_rn(widen(v[e]), widen(v[e])));
+      v[e] = li < nr ? __ldcg((const VT *)a.rin + r0 + li) : (VT)0;
+      if (li < nr) acc = add_rn(acc, mul_rn(widen(v[e]), widen(v[e])));
+    }
+    if (li0 + kIrQ <= nr) {
+      const VT z[kIrQ] = {(VT)0, (VT)0, (VT)0, (VT)0};
+      sts4<VT>(sp + li0, v);
+      sts4<VT>(sx + li0, z);
+      stcg4<VT>(P + r0 + li0, v);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) {
+        const int li = li0 + e;
+        if (li < nr) {
+          sp[li] = v[e];
+          sx[li] = (VT)0;
+          __stcg(P + r0 + li, v[e]);
+        }
       }
     }
     TW::put(tr + TW::W * j, v);
@@ -623,16 +642,12 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
     acc = 0.0;
     for (int j = 0; j < quads; j++) {
       const int li0 = j * kIrTile + kIrQ * t;
-      VT q[kIrQ];
-      if (li0 < nr) {
-        ir_quad_mv<VT, MT, NDG>(D, a, sp, r0, nr, li0, nd, q);
+      VT q[kIrQ], pv[kIrQ];
+      ir_quad_mv<VT, MT, NDG>(D, a, sp, r0, nr, li0, nd, q);
+      ir_own4(sp, li0, nr, pv);
 #pragma unroll
-        for (int e = 0; e < kIrQ; e++)
-          if (li0 + e < nr) acc = add_rn(acc, mul_rn(widen(sp[li0 + e]), widen(q[e])));
-      } else {
-#pragma unroll
-        for (int e = 0; e < kIrQ; e++) q[e] = (VT)0;
-      }
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) acc = add_rn(acc, mul_rn(widen(pv[e]), widen(q[e])));
       TW::put(tq + TW::W * j, q);
     }
     tm_wait_st();
@@ -654,20 +669,36 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
     // B: x += alpha p, r -= alpha q, (r, r)
     const VT av = (VT)alpha;
     acc = 0.0;
-    for (int j = 0; j < quads; j++) {
+    auto update_b = [&](int j, VT (&rv)[kIrQ], const VT (&qv)[kIrQ]) {
       const int li0 = j * kIrTile + kIrQ * t;
-      VT rv[kIrQ], qv[kIrQ];
-      TW::get2(tr + TW::W * j, rv, tq + TW::W * j, qv);
+      if (li0 + kIrQ <= nr) {  // vector accesses: the 4 rows of a thread are one aligned quad
+        VT pv[kIrQ], xv[kIrQ];
+        lds4<VT>(sp + li0, pv);
+        lds4<VT>(sx + li0, xv);
 #pragma unroll
-      for (int e = 0; e < kIrQ; e++) {
-        const int li = li0 + e;
-        if (li < nr) {
-          sx[li] = add_rn(mul_rn(av, sp[li]), sx[li]);
+        for (int e = 0; e < kIrQ; e++) {
+          xv[e] = add_rn(mul_rn(av, pv[e]), xv[e]);
           rv[e] = add_rn(mul_rn((VT)(-av), qv[e]), rv[e]);
           acc = add_rn(acc, mul_rn(widen(rv[e]), widen(rv[e])));
         }
+        sts4<VT>(sx + li0, xv);
+      } else {
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          const int li = li0 + e;
+          if (li < nr) {
+            sx[li] = add_rn(mul_rn(av, sp[li]), sx[li]);
+            rv[e] = add_rn(mul_rn((VT)(-av), qv[e]), rv[e]);
+            acc = add_rn(acc, mul_rn(widen(rv[e]), widen(rv[e])));
+          }
+        }
       }
       TW::put(tr + TW::W * j, rv);
+    };
+    for (int j = 0; j < quads; j++) {
+      VT rv[kIrQ], qv[kIrQ];
+      TW::get2(tr + TW::W * j, rv, tq + TW::W * j, qv);
+      update_b(j, rv, qv);
     }
     tm_wait_st();
     *xw = true;
@@ -759,7 +790,10 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cg_onchip(DiaT<MT> D, IrArgs 
   bool xw = false;
   const int code = ir_body<VT, MT, NDG>(D, a, sp, sx, tm, &L, &alpha, &beta, &rr, &xw);
   if (code >= 0) {
-    // x out (a whole solve writes its zeros too)
+    // x out (a whole solve writes its zeros too): thread t reads rows other
+    // threads updated last (the loop may end right after an update pass), so
+    // the CTA synchronises first; code is the same in every thread
+    __syncthreads();
     const int r0 = blockIdx.x * a.rpc;
     const int nr = max(0, min(a.rpc, a.n - r0));
     VT *x = (VT *)a.x;
