@@ -81,7 +81,29 @@ struct IrArgs {
   int rpc;    // rows per CTA, a multiple of 32
   int K;      // rows per thread: ceil(rpc / kIrThreads) <= kIrMaxK (half for FP64)
   int whole;  // 1: a whole CG solve (|b|, the stopping state and the history of the method)
+  int stencil;  // 1: full quads take ir_quad_mv_st (ir_stencil_ok holds, P is zero-padded)
 };
+
+// P's zero pad on each side for the stencil path: beyond the largest offset
+// plus a quad, a multiple of 8 elements (keeps P's vector alignment).
+inline long long ir_p_pad(const CsrDev &A) {
+  int m = 0;
+  for (int k = 0; k < A.dia_nd; k++) m = std::max(m, std::abs(A.dia_off[k]));
+  return ((long long)m + 8 + 7) / 8 * 8;
+}
+
+// Whether a matrix takes the stencil path of the on-chip SpMV: 5 or 7
+// diagonals at offsets 0, -1, +1 and further pairs -o, +o with o a multiple
+// of 4, over the system's own columns (one GPU).
+inline bool ir_stencil_ok(const CsrDev &A, long long n) {
+  const int nd = A.dia_nd;
+  if ((nd != 5 && nd != 7) || A.dia_cmin != 0 || A.dia_cmax != n) return false;
+  const int h = nd / 2;
+  if (A.dia_off[h] != 0 || A.dia_off[h - 1] != -1 || A.dia_off[h + 1] != 1) return false;
+  for (int k = 0; k < h - 1; k++)
+    if (A.dia_off[k] % 4 != 0 || A.dia_off[k] != -A.dia_off[nd - 1 - k]) return false;
+  return true;
+}
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
   unsigned long long v;
@@ -550,6 +572,117 @@ __device__ __forceinline__ void ir_quad_mv(const DiaT<MT> &D, const IrArgs &a, c
   }
 }
 
+// Matrix values of one stored diagonal for 4 rows from an aligned address.
+template <class MT>
+__device__ __forceinline__ void ir_vals4(const MT *vp, IrVals<MT> &a) {
+  if constexpr (std::is_same<MT, __nv_bfloat16>::value)
+    a.u = __ldg(reinterpret_cast<const uint2 *>(vp));
+  else
+    ld4<MT>(vp, a.v, false);
+}
+template <class VT, class MT>
+__device__ __forceinline__ VT ir_val(const IrVals<MT> &a, int e) {
+  if constexpr (std::is_same<MT, __nv_bfloat16>::value)
+    return a.get(e);
+  else
+    return (VT)a.v[e];
+}
+
+// q = A p for a full quad (rows i0 .. i0+3 all in the CTA) of a 5- or
+// 7-point stencil whose diagonals lie at 0, +-1 and (+-b, +-c) with b and c
+// multiples of 4, P zero-padded beyond [0, n) by more than the largest
+// offset (ir_stencil_ok). Without per-diagonal alignment tests or clamps:
+//   * p of the +-1 diagonals is the own quad pv shifted by one row, plus
+//     p[i0-1] and p[i0+4]; each far diagonal's 4 columns are one aligned
+//     quad, from shared memory when inside the CTA's rows, else from P;
+//   * matrix values are one aligned vector per diagonal; in the symmetric
+//     layout the -1 diagonal of rows i0 .. i0+3 is the +1 diagonal of rows
+//     i0-1 .. i0+2: the +1 vector shifted by one row and one scalar.
+// A column outside [0, n) has a zero value and reads a zero of P's pad
+// (ir_quad_mv reads a clamped column instead): the term adds a zero to a sum
+// that starts at +0, which leaves it unchanged, so the terms and their order
+// are ir_quad_mv's and so are the results.
+template <class VT, class MT, int NDG>
+__device__ __forceinline__ void ir_quad_mv_st(const DiaT<MT> &D, const VT *P, const VT *sp, int r0, int nr, int li0,
+                                              const VT (&pv)[kIrQ], VT (&q)[kIrQ]) {
+  static_assert(NDG == 5 || NDG == 7, "stencil path: 5 or 7 diagonals");
+  constexpr int H = NDG / 2;  // the main diagonal
+  constexpr bool kMask = std::is_same<MT, double>::value;
+  const int i0 = r0 + li0;
+  const bool sym = D.vs[H - 1] != 0;  // -1 diagonal read from its +1 mirror
+  unsigned m = 0xffffffffu;
+  if constexpr (kMask) m = __ldg(reinterpret_cast<const unsigned *>(D.mask + i0));
+  // p: the -1 / +1 neighbours of the quad, then the far diagonals' quads
+  const VT pm1 = li0 >= 1 ? sp[li0 - 1] : __ldcg(P + (i0 - 1));
+  const VT pp4 = li0 + kIrQ < nr ? sp[li0 + kIrQ] : __ldcg(P + (i0 + kIrQ));
+  IrVals<MT> vm1, v1;
+  ir_vals4<MT>(D.vb[H + 1] + i0, v1);
+  MT m1s = (MT)0;
+  if (sym)
+    m1s = ir_ld<MT>(D.vb[H + 1] + (i0 - 1));
+  else
+    ir_vals4<MT>(D.vb[H - 1] + i0, vm1);
+#pragma unroll
+  for (int e = 0; e < kIrQ; e++) q[e] = (VT)0;
+  auto term = [&](int k, const VT (&val)[kIrQ], const VT (&p)[kIrQ]) {
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) {
+      const VT t = add_rn(q[e], mul_rn(val[e], p[e]));
+      if constexpr (kMask)
+        q[e] = ((m >> (8 * e + k)) & 1u) ? t : q[e];
+      else
+        q[e] = t;
+    }
+  };
+  auto far = [&](int k) {
+    const int off = D.off[k];
+    IrVals<MT> av;
+    ir_vals4<MT>(D.vb[k] + (i0 + D.vs[k]), av);
+    VT p[kIrQ], val[kIrQ];
+    const int lc = li0 + off;
+    if (lc >= 0 && lc + kIrQ <= nr)
+      lds4<VT>(sp + lc, p);
+    else
+      ld4<VT>(P + (i0 + off), p, true);
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) val[e] = ir_val<VT, MT>(av, e);
+    term(k, val, p);
+  };
+  // ascending offsets: the far lower diagonals, -1, 0, +1, the far upper ones
+#pragma unroll
+  for (int k = 0; k < H - 1; k++) far(k);
+  {
+    VT val[kIrQ];
+    const VT p[kIrQ] = {pm1, pv[0], pv[1], pv[2]};
+    if (sym) {
+      val[0] = (VT)mval<VT>(m1s);
+#pragma unroll
+      for (int e = 1; e < kIrQ; e++) val[e] = ir_val<VT, MT>(v1, e - 1);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) val[e] = ir_val<VT, MT>(vm1, e);
+    }
+    term(H - 1, val, p);
+  }
+  {
+    IrVals<MT> v0;
+    ir_vals4<MT>(D.vb[H] + i0, v0);
+    VT val[kIrQ];
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) val[e] = ir_val<VT, MT>(v0, e);
+    term(H, val, pv);
+  }
+  {
+    VT val[kIrQ];
+    const VT p[kIrQ] = {pv[1], pv[2], pv[3], pp4};
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) val[e] = ir_val<VT, MT>(v1, e);
+    term(H + 1, val, p);
+  }
+#pragma unroll
+  for (int k = H + 2; k < NDG; k++) far(k);
+}
+
 // The solve (see the top of this file). Returns the stopping code, or -1
 // when a wait ran out; *xw: x was written (one update at least).
 template <class VT, class MT, int NDG>
@@ -643,8 +776,15 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
     for (int j = 0; j < quads; j++) {
       const int li0 = j * kIrTile + kIrQ * t;
       VT q[kIrQ], pv[kIrQ];
-      ir_quad_mv<VT, MT, NDG>(D, a, sp, r0, nr, li0, nd, q);
       ir_own4(sp, li0, nr, pv);
+      bool st_done = false;
+      if constexpr (NDG == 5 || NDG == 7) {
+        if (a.stencil && li0 + kIrQ <= nr) {
+          ir_quad_mv_st<VT, MT, NDG>(D, P, sp, r0, nr, li0, pv, q);
+          st_done = true;
+        }
+      }
+      if (!st_done) ir_quad_mv<VT, MT, NDG>(D, a, sp, r0, nr, li0, nd, q);
 #pragma unroll
       for (int e = 0; e < kIrQ; e++)
         if (li0 + e < nr) acc = add_rn(acc, mul_rn(widen(pv[e]), widen(q[e])));

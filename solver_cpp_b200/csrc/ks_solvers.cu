@@ -815,11 +815,18 @@ inline bool run_cg_onchip(const Env<double> &E, const double *b, double *x, doub
     (void)cudaGetLastError();
     return false;
   }
-  if (reinterpret_cast<uintptr_t>(P) % 32) return false;  // 32-byte vector loads of P
+  // P takes the first two workspace slots: with the stencil path it sits
+  // between two zero pads wider than the largest offset
+  const long long pad = ir_p_pad(*E.A);
+  const bool stencil = ir_stencil_ok(*E.A, E.n) && 2 * E.ld >= E.n + 2 * pad;
+  double *const Pp = P + (stencil ? pad : 0);
+  if (reinterpret_cast<uintptr_t>(Pp) % 32) return false;  // 32-byte vector loads of P
   launch_scalar(ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
-  const IrArgs a{b, x, P, E.st, nullptr, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
-                 (int)E.n, sh.rpc, sh.K, 1};
+  const IrArgs a{b, x, Pp, E.st, nullptr, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
+                 (int)E.n, sh.rpc, sh.K, 1, stencil ? 1 : 0};
   cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes(sh.G), ctx->stream);
+  if (e == cudaSuccess && stencil) e = cudaMemsetAsync(P, 0, sizeof(double) * pad, ctx->stream);
+  if (e == cudaSuccess && stencil) e = cudaMemsetAsync(Pp + E.n, 0, sizeof(double) * pad, ctx->stream);
   if (e == cudaSuccess) e = ir_launch<double, double>(ctx, *E.A, a, sh, false, &fits, kOther);
   *s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip CG launch");
   return true;
@@ -1966,13 +1973,14 @@ struct VpXrStartOp {
 // published directions P and the solution x, in the inner workspace.
 struct InnerResBufs {
   float *r, *P, *x;
+  int stencil;  // P zero-padded for the stencil path (ir_stencil_ok)
 };
 
 // One inner solve with the on-chip kernel (its start already issued).
 inline ks_status run_cg_inner_resident(const Env<float> &E, const InnerResBufs &B, const IrShape &sh) {
   ks_ctx *ctx = E.ctx;
   IrArgs a{B.r, B.x, B.P, E.st, E.outer_done, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
-           (int)E.n, sh.rpc, sh.K, 0};
+           (int)E.n, sh.rpc, sh.K, 0, B.stencil};
   cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes(sh.G), ctx->stream);
   if (e == cudaSuccess) {
     bool fits = false;
@@ -2013,7 +2021,7 @@ void InnerRunner<VT>::setup_resident() {
   res_cg = false;
   if (method != KS_CG || iprec == KS_FP64 || E32.comm || !E32.A || !E32.A->dia_nd) return;
   if (iprec == KS_FP32 ? !E32.A->dia_val32 : !E32.A->dia_val16) return;
-  if (vec_count(KS_CG, E32.sp, E32.n, sizeof(float), ctx->l2_bytes) < 2) return;
+  if (vec_count(KS_CG, E32.sp, E32.n, sizeof(float), ctx->l2_bytes) < 3) return;  // P (two slots) and r
   if (!ir_shape<float>(ctx, E32.n, &sh)) return;
   bool fits = false;
   const IrArgs none{};
@@ -2023,11 +2031,21 @@ void InnerRunner<VT>::setup_resident() {
     (void)cudaGetLastError();
     return;
   }
+  // P in the first two slots (16-byte vector loads need their alignment),
+  // between two zero pads wider than the largest offset for the stencil path
   Ws<float> W{ws32, E32.ld, E32.off};
-  fb.P = W.take();  // the first slot: 16-byte vector loads of P need its alignment
+  const long long pad = ir_p_pad(*E32.A);
+  float *const preg = W.take(2);
+  fb.stencil = ir_stencil_ok(*E32.A, E32.n) && 2 * E32.ld >= E32.n + 2 * pad ? 1 : 0;
+  fb.P = preg + (fb.stencil ? pad : 0);
   fb.r = W.take();
   fb.x = z32;
   if (reinterpret_cast<uintptr_t>(fb.P) % 16) return;
+  if (fb.stencil && (cudaMemsetAsync(preg, 0, sizeof(float) * pad, ctx->stream) != cudaSuccess ||
+                     cudaMemsetAsync(fb.P + E32.n, 0, sizeof(float) * pad, ctx->stream) != cudaSuccess)) {
+    (void)cudaGetLastError();
+    return;
+  }
   res_cg = true;
 }
 

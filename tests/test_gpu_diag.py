@@ -163,7 +163,7 @@ def test_almost_symmetric_matrix_keeps_every_diagonal(ks, ctx, oracle):
     assert np.array_equal(Y.numpy(), oracle.spmv(oracle.Problem(B), x))
 
 
-@pytest.mark.parametrize("grid", [16, 28])
+@pytest.mark.parametrize("grid", [16, 18, 28])  # 18: offsets 18, 324 take the generic quad path
 @pytest.mark.parametrize("outer,inner,prec,kw", [
     ("VPCG", "CG", "fp32", {}), ("VPCG", "CG", "bf16", {}), ("VPGMRES", "CG", "fp32", {"R": 20, "l": 10}),
     ("VPGCR", "CG", "fp32", {"R": 20, "l": 10}), ("VPCR", "CG", "fp32", {"L": 40}),
