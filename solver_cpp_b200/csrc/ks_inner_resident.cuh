@@ -23,7 +23,8 @@
 // Per iteration (cg.cpp:184-240):
 //   A: q = A p (own p from shared memory, other CTAs' from P), (p, q) summed
 //      over the grid -> alpha = (r, r) / (p, q);
-//   B: x += alpha p, r -= alpha q, (r, r) summed -> beta, stopping test;
+//   B: r -= alpha q, (r, r) summed -> beta, stopping test; x += alpha p
+//      while the sum travels;
 //   C: p = beta p + r, published; each CTA then waits only for the CTAs
 //      whose rows its own rows read (release/acquire flags per CTA).
 // Each element sees the FP32 operations of the kernel-per-step loop
@@ -149,23 +150,36 @@ __device__ __forceinline__ void ir_block_sum(double (&v)[N], double (*sh)[kIrWar
 constexpr int kIrMaxGrid = 256;  // CTAs a reduction takes (one per SM)
 constexpr int kIrMaxSums = 2;    // values one reduction carries
 
+// A grid reduction in two halves, so that work which does not need the sums
+// runs while the other CTAs arrive: ir_red_post adds the CTA's values (a
+// block-wide step: every thread calls it) and counts the CTA in; ir_red_wait
+// (every thread) waits for all CTAs and returns the sums.
 template <int N>
-__device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long gen, double (&v)[N]) {
+__device__ __forceinline__ void ir_red_post(const IrArgs &a, unsigned long long gen, double (&v)[N]) {
   static_assert(N >= 1 && N <= kIrMaxSums, "values per reduction");
   __shared__ double sh[kIrMaxSums][kIrWarps];
-  __shared__ double s_res[kIrMaxSums];
-  __shared__ int s_ok;
   ir_block_sum<N>(v, sh);
-  const unsigned G = gridDim.x;
-  // Two sets of partials, by the parity of the generation: a CTA writes
-  // generation g + 2's only after every CTA has arrived at g + 1, i.e. after
-  // every CTA has read generation g's.
-  double *part = a.partials + (size_t)(gen & 1) * kIrMaxSums * G;
   if (threadIdx.x == 0) {
+    const unsigned G = gridDim.x;
+    // Two sets of partials, by the parity of the generation: a CTA writes
+    // generation g + 2's only after every CTA has arrived at g + 1, i.e.
+    // after every CTA has read generation g's.
+    double *part = a.partials + (size_t)(gen & 1) * kIrMaxSums * G;
 #pragma unroll
     for (int d = 0; d < N; d++) part[(size_t)d * G + blockIdx.x] = v[d];
     __threadfence();
     atomicAdd(&a.sync->count, 1ull);
+  }
+}
+
+// Returns false when the wait ran out (the timeout flag is then set).
+template <int N>
+__device__ __forceinline__ bool ir_red_wait(const IrArgs &a, unsigned long long gen, double (&v)[N]) {
+  __shared__ double s_res[kIrMaxSums];
+  __shared__ int s_ok;
+  const unsigned G = gridDim.x;
+  const double *part = a.partials + (size_t)(gen & 1) * kIrMaxSums * G;
+  if (threadIdx.x == 0) {
     s_ok = 1;
     const unsigned long long want = gen * (unsigned long long)G;
     const unsigned long long t0 = global_ns();
@@ -201,6 +215,12 @@ __device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long
 #pragma unroll
   for (int d = 0; d < N; d++) v[d] = s_res[d];
   return true;
+}
+
+template <int N>
+__device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long gen, double (&v)[N]) {
+  ir_red_post<N>(a, gen, v);
+  return ir_red_wait<N>(a, gen, v);
 }
 
 // After publishing its rows of p: release this CTA's flag, then wait until
@@ -740,7 +760,7 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
   }
   tm_wait_st();
   unsigned long long gen = 0, pgen = 1;  // reductions, publications of p
-  double v[2] = {0.0, 0.0};
+  double v[1] = {0.0};
   double rr, bnorm;
   int code = kRunning;
   if (a.whole) {
@@ -792,7 +812,6 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
     }
     tm_wait_st();
     v[0] = acc;
-    v[1] = 0.0;
     if (!ir_allreduce(a, ++gen, v)) return -1;
     // alpha = rr / (p, q)   (rdiv: a zero denominator is a breakdown)
     if (v[0] == 0.0) {
@@ -806,45 +825,43 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
       if (lead && a.whole) set_done(st, code);
       break;
     }
-    // B: x += alpha p, r -= alpha q, (r, r)
+    // B: r -= alpha q and (r, r), whose sum is posted; then x += alpha p
+    // (nothing waits for it) while the other CTAs arrive
     const VT av = (VT)alpha;
     acc = 0.0;
-    auto update_b = [&](int j, VT (&rv)[kIrQ], const VT (&qv)[kIrQ]) {
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      VT rv[kIrQ], qv[kIrQ];
+      TW::get2(tr + TW::W * j, rv, tq + TW::W * j, qv);
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) {
+        rv[e] = add_rn(mul_rn((VT)(-av), qv[e]), rv[e]);  // rows past nr: unused words
+        if (li0 + e < nr) acc = add_rn(acc, mul_rn(widen(rv[e]), widen(rv[e])));
+      }
+      TW::put(tr + TW::W * j, rv);
+    }
+    tm_wait_st();
+    v[0] = acc;
+    ir_red_post<1>(a, ++gen, v);
+    for (int j = 0; j < quads; j++) {
       const int li0 = j * kIrTile + kIrQ * t;
       if (li0 + kIrQ <= nr) {  // vector accesses: the 4 rows of a thread are one aligned quad
         VT pv[kIrQ], xv[kIrQ];
         lds4<VT>(sp + li0, pv);
         lds4<VT>(sx + li0, xv);
 #pragma unroll
-        for (int e = 0; e < kIrQ; e++) {
-          xv[e] = add_rn(mul_rn(av, pv[e]), xv[e]);
-          rv[e] = add_rn(mul_rn((VT)(-av), qv[e]), rv[e]);
-          acc = add_rn(acc, mul_rn(widen(rv[e]), widen(rv[e])));
-        }
+        for (int e = 0; e < kIrQ; e++) xv[e] = add_rn(mul_rn(av, pv[e]), xv[e]);
         sts4<VT>(sx + li0, xv);
       } else {
 #pragma unroll
         for (int e = 0; e < kIrQ; e++) {
           const int li = li0 + e;
-          if (li < nr) {
-            sx[li] = add_rn(mul_rn(av, sp[li]), sx[li]);
-            rv[e] = add_rn(mul_rn((VT)(-av), qv[e]), rv[e]);
-            acc = add_rn(acc, mul_rn(widen(rv[e]), widen(rv[e])));
-          }
+          if (li < nr) sx[li] = add_rn(mul_rn(av, sp[li]), sx[li]);
         }
       }
-      TW::put(tr + TW::W * j, rv);
-    };
-    for (int j = 0; j < quads; j++) {
-      VT rv[kIrQ], qv[kIrQ];
-      TW::get2(tr + TW::W * j, rv, tq + TW::W * j, qv);
-      update_b(j, rv, qv);
     }
-    tm_wait_st();
     *xw = true;
-    v[0] = acc;
-    v[1] = 0.0;
-    if (!ir_allreduce(a, ++gen, v)) return -1;
+    if (!ir_red_wait<1>(a, gen, v)) return -1;
     // beta = (r, r)_new / (r, r); then the stopping test at the top of
     // iteration L + 1 (check_top), whose verdict overrides beta's
     const double rr2 = v[0];
