@@ -672,6 +672,31 @@ def kernel_tour(args):
     ctx.close()
 
 
+def profile_solve(args):
+    """One solve of a workload's method (or, with --profile-plain, of its plain
+    FP64 counterpart) stopped after --profile-loops outer iterations; no
+    timing: the workload of the ncu launch lists and kernel captures whose
+    summaries are kept under profiles/."""
+    import solver_cpp_b200 as ks
+    from solver_cpp_b200.matrices import config_problem
+
+    W = WORKLOADS[args.profile_solve]
+    A, b, _ = config_problem(W["problem"], W["grid"])
+    ctx = ks.Context(0)
+    vals = W["spmv_values"]
+    M = ctx.matrix(A, transpose=W["transpose"], fp32=vals == "fp32", bf16=vals == "bf16")
+    if args.profile_plain and W["plain"]:
+        outer, inner, params = W["plain"]["outer"], "NONE", dict(W["plain"]["params"])
+    else:
+        outer, inner, params = W["outer"], W["inner"], dict(W["params"])
+    params["L"] = args.profile_loops
+    r = ks.solve(ctx, M, outer, b, inner=inner, **params)
+    print(json.dumps({"profile_solve": args.profile_solve, "method": outer, "inner": inner, "loop": r.loop,
+                      "status": r.status, "inner_calls": r.inner_calls}), flush=True)
+    M.close()
+    ctx.close()
+
+
 def ortho_only(args):
     """The GMRES orthogonalisation kernels alone on vectors of the workload's
     length: h = V^T w over k basis vectors (block dot) and w -= V h (block
@@ -738,11 +763,18 @@ def main():
                          "default row split of the one system over the ranks (strong scaling)")
     ap.add_argument("--ortho-only", type=int, nargs="+", default=None, metavar="K",
                     help="time only the GMRES block dot / block AXPY over K basis vectors (profiling)")
+    ap.add_argument("--profile-solve", choices=sorted(WORKLOADS), default=None,
+                    help="one untimed solve of the workload (a profiler's workload)")
+    ap.add_argument("--profile-loops", type=int, default=3, help="with --profile-solve: outer iterations")
+    ap.add_argument("--profile-plain", action="store_true", help="with --profile-solve: the plain FP64 method")
     ap.add_argument("--kernel-tour", action="store_true",
                     help="run a few iterations of every method on the 128^3 systems (profiler workload)")
     args = ap.parse_args()
     if args.kernel_tour:
         kernel_tour(args)
+        return
+    if args.profile_solve:
+        profile_solve(args)
         return
     if args.spmv_only:
         spmv_only(args)

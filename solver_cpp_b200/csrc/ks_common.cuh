@@ -293,6 +293,7 @@ struct ks_ctx {
   size_t l2_bytes = 0;  // L2 cache size of the device
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  bool ir_used = false;         // an on-chip CG kernel ran in this solve (ir_l2_release)
   double *partials = nullptr;   // reduction scratch
   size_t partials_len = 0;
   unsigned *counters = nullptr; // last-CTA-done counters

@@ -250,13 +250,62 @@ __device__ __forceinline__ bool ir_publish_sync(const IrArgs &a, unsigned long l
   return s_ok != 0;
 }
 
+// The matrix values (and FP64 row masks) are loaded with an L2 evict_last
+// policy: between two inner solves the outer method's kernels stream its
+// FP64 matrix and vectors through L2, and the diagonal copy, read 20 times
+// per inner solve, then stays in L2 ahead of them (measured: the inner solve
+// ran 425 us with L2 flushed before it and 570 us after the outer kernels,
+// without the hint). After the solve ir_l2_release lowers it again.
+__device__ __forceinline__ uint64_t ir_pol() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float ldl(const float *p) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(ir_pol()));
+  return v;
+}
+__device__ __forceinline__ double ldl(const double *p) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(ir_pol()));
+  return v;
+}
+__device__ __forceinline__ unsigned short ldl(const unsigned short *p) {
+  unsigned short v;
+  asm("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(ir_pol()));
+  return v;
+}
+__device__ __forceinline__ unsigned ldl(const unsigned *p) {
+  unsigned v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(ir_pol()));
+  return v;
+}
+__device__ __forceinline__ uint2 ldl2(const void *p) {
+  uint2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(ir_pol()));
+  return v;
+}
+__device__ __forceinline__ float4 ldl4(const float *p) {
+  float4 v;
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(p), "l"(ir_pol()));
+  return v;
+}
+__device__ __forceinline__ double2 ldl2d(const double *p) {
+  double2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(ir_pol()));
+  return v;
+}
+
 template <class MT>
 __device__ __forceinline__ MT ir_ld(const MT *p) {
-  return __ldg(p);
+  return ldl(p);
 }
 template <>
 __device__ __forceinline__ __nv_bfloat16 ir_ld<__nv_bfloat16>(const __nv_bfloat16 *p) {
-  return __ushort_as_bfloat16(__ldg(reinterpret_cast<const unsigned short *>(p)));
+  return __ushort_as_bfloat16(ldl(reinterpret_cast<const unsigned short *>(p)));
 }
 
 // ---------------------------------------------------------------- TMEM access
@@ -387,7 +436,7 @@ template <class T>
 __device__ __forceinline__ void ld4(const T *p, T (&v)[kIrQ], bool global_cg);
 template <>
 __device__ __forceinline__ void ld4<float>(const float *p, float (&v)[kIrQ], bool cg) {
-  const float4 u = cg ? __ldcg(reinterpret_cast<const float4 *>(p)) : __ldg(reinterpret_cast<const float4 *>(p));
+  const float4 u = cg ? __ldcg(reinterpret_cast<const float4 *>(p)) : ldl4(p);
   v[0] = u.x;
   v[1] = u.y;
   v[2] = u.z;
@@ -396,7 +445,7 @@ __device__ __forceinline__ void ld4<float>(const float *p, float (&v)[kIrQ], boo
 template <>
 __device__ __forceinline__ void ld4<double>(const double *p, double (&v)[kIrQ], bool cg) {
   const double2 *q = reinterpret_cast<const double2 *>(p);
-  const double2 a = cg ? __ldcg(q) : __ldg(q), b = cg ? __ldcg(q + 1) : __ldg(q + 1);
+  const double2 a = cg ? __ldcg(q) : ldl2d(p), b = cg ? __ldcg(q + 1) : ldl2d(p + 2);
   v[0] = a.x;
   v[1] = a.y;
   v[2] = b.x;
@@ -404,7 +453,7 @@ __device__ __forceinline__ void ld4<double>(const double *p, double (&v)[kIrQ], 
 }
 template <>
 __device__ __forceinline__ void ld4<__nv_bfloat16>(const __nv_bfloat16 *p, __nv_bfloat16 (&v)[kIrQ], bool) {
-  const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+  const uint2 u = ldl2(p);
   v[0] = __ushort_as_bfloat16((unsigned short)(u.x & 0xffffu));
   v[1] = __ushort_as_bfloat16((unsigned short)(u.x >> 16));
   v[2] = __ushort_as_bfloat16((unsigned short)(u.y & 0xffffu));
@@ -468,11 +517,11 @@ __device__ __forceinline__ void ir_vals(const MT *vp, bool full, int li0, int nr
   const bool aligned = (reinterpret_cast<uintptr_t>(vp) & (kIrQ * sizeof(MT) - 1)) == 0;
   if constexpr (std::is_same<MT, __nv_bfloat16>::value) {
     if (full && aligned) {
-      a.u = __ldg(reinterpret_cast<const uint2 *>(vp));
+      a.u = ldl2(vp);
     } else {
       unsigned short h[kIrQ];
 #pragma unroll
-      for (int e = 0; e < kIrQ; e++) h[e] = li0 + e < nr ? __ldg(reinterpret_cast<const unsigned short *>(vp) + e) : 0;
+      for (int e = 0; e < kIrQ; e++) h[e] = li0 + e < nr ? ldl(reinterpret_cast<const unsigned short *>(vp) + e) : 0;
       a.u = make_uint2(h[0] | ((unsigned)h[1] << 16), h[2] | ((unsigned)h[3] << 16));
     }
   } else {
@@ -480,7 +529,7 @@ __device__ __forceinline__ void ir_vals(const MT *vp, bool full, int li0, int nr
       ld4<MT>(vp, a.v, false);
     } else {
 #pragma unroll
-      for (int e = 0; e < kIrQ; e++) a.v[e] = li0 + e < nr ? __ldg(vp + e) : (MT)0;
+      for (int e = 0; e < kIrQ; e++) a.v[e] = li0 + e < nr ? ldl(vp + e) : (MT)0;
     }
   }
 }
@@ -538,7 +587,7 @@ __device__ __forceinline__ void ir_quad_mv(const DiaT<MT> &D, const IrArgs &a, c
   unsigned m = 0xffffffffu;  // the rows' mask bytes, row e in byte e
   if constexpr (kMask) {
     if (full) {
-      m = __ldg(reinterpret_cast<const unsigned *>(D.mask + i0));
+      m = ldl(reinterpret_cast<const unsigned *>(D.mask + i0));
     } else {
       m = 0;
       for (int e = 0; e < kIrQ; e++)
@@ -596,7 +645,7 @@ __device__ __forceinline__ void ir_quad_mv(const DiaT<MT> &D, const IrArgs &a, c
 template <class MT>
 __device__ __forceinline__ void ir_vals4(const MT *vp, IrVals<MT> &a) {
   if constexpr (std::is_same<MT, __nv_bfloat16>::value)
-    a.u = __ldg(reinterpret_cast<const uint2 *>(vp));
+    a.u = ldl2(vp);
   else
     ld4<MT>(vp, a.v, false);
 }
@@ -631,7 +680,7 @@ __device__ __forceinline__ void ir_quad_mv_st(const DiaT<MT> &D, const VT *P, co
   const int i0 = r0 + li0;
   const bool sym = D.vs[H - 1] != 0;  // -1 diagonal read from its +1 mirror
   unsigned m = 0xffffffffu;
-  if constexpr (kMask) m = __ldg(reinterpret_cast<const unsigned *>(D.mask + i0));
+  if constexpr (kMask) m = ldl(reinterpret_cast<const unsigned *>(D.mask + i0));
   // p: the -1 / +1 neighbours of the quad, then the far diagonals' quads
   const VT pm1 = li0 >= 1 ? sp[li0 - 1] : __ldcg(P + (i0 - 1));
   const VT pp4 = li0 + kIrQ < nr ? sp[li0 + kIrQ] : __ldcg(P + (i0 + kIrQ));
@@ -978,6 +1027,33 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cg_onchip(DiaT<MT> D, IrArgs 
   }
 }
 
+// Lowers the L2 eviction priority of [p, p + bytes) back to normal (the
+// lines stay cached), p 128-byte aligned: after the on-chip kernels' evict_last
+// loads, so that the diagonal copy does not keep its place in L2 ahead of
+// later work.
+__global__ void k_l2_normal(const char *p, unsigned long long bytes) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x * 128ull;
+  for (unsigned long long o = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) * 128ull; o < bytes;
+       o += stride)
+    asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(p + o) : "memory");
+}
+
+// The whole diagonal copy (every precision's values and the row masks).
+inline void ir_l2_release(ks_ctx *ctx, const CsrDev &A) {
+  const long long stored = A.dia_sym ? A.dia_nd / 2 + 1 : A.dia_nd;
+  auto one = [&](const void *p, unsigned long long bytes) {
+    if (!p || !bytes) return;
+    const uintptr_t a0 = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)127;
+    launch_k(ctx, k_l2_normal, dim3(ctx->num_sms * 2), dim3(256), 0, reinterpret_cast<const char *>(a0),
+             bytes + (reinterpret_cast<uintptr_t>(p) - a0));
+  };
+  const unsigned long long e = (unsigned long long)(stored * A.dia_ds);
+  one(A.dia_val, e * sizeof(double));
+  one(A.dia_val32, e * sizeof(float));
+  one(A.dia_val16, e * sizeof(__nv_bfloat16));
+  one(A.dia_mask, (unsigned long long)A.n);
+}
+
 // Launch shape: one CTA per SM, rows per CTA a multiple of 32.
 struct IrShape {
   int G = 0, rpc = 0, K = 0;
@@ -1031,6 +1107,7 @@ inline cudaError_t ir_launch_n(ks_ctx *ctx, const CsrDev &A, const IrArgs &a, co
   cfg.attrs = at;
   cfg.numAttrs = 1;
   ctx->launches++;
+  ctx->ir_used = true;  // its matrix lines are evict_last in L2 (ir_l2_release)
   ProfLaunch pl(ctx, cls);
   return cudaLaunchKernelEx(&cfg, fn, dview<MT>(A), a);
 }

@@ -2472,8 +2472,13 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
     ~ProfScope() { c->prof_on = 0; }
   } prof(ctx, prm->profile == 1);
   KS_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  ctx->ir_used = false;
   ks_status s = run_method<double>(outer, E, b, xs, ws, dws, vp ? &IR : nullptr);
   if (s == KS_OK && vp) s = IR.status;
+  if (ctx->ir_used) {
+    ir_l2_release(ctx, *A);
+    ctx->ir_used = false;
+  }
   KS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
   if (s == KS_OK && dist) {
     // true residual |b - A x| / |b| over all ranks (not gated by `done`: the
