@@ -195,18 +195,22 @@ def spmv_bytes(n, nnz, values, index_bytes=4, diagonals=0, symmetric=0):
 
 
 def onchip_inner_bytes(n, values, diagonals, symmetric, info, iters, sms=148):
-    """Algorithmic bytes of one launch of the on-chip inner CG (FP32 vectors
-    on chip, the matrix read every iteration): per iteration the stored
-    diagonals' values, p published (4 n) and the neighbouring CTAs' p read
-    (each CTA owns ceil(n / sms) rows, and reads the rows an offset reaches
-    beyond its own, at each end); once: the right-hand side read and x
-    written (8 n)."""
-    vb = {"fp32": 4, "bf16": 2}[values]
+    """Algorithmic bytes of one launch of the on-chip CG kernel (vectors on
+    chip, the matrix read every iteration): per iteration the stored
+    diagonals' values (and one mask byte per row with FP64 values), p
+    published (one vector) and the neighbouring CTAs' p read (each CTA owns
+    ceil(n / sms) rows, and reads the rows an offset reaches beyond its own,
+    at each end); once: the right-hand side read and x written. Vectors are
+    FP32 for the inner solve of a VP method (fp32 / bf16 values) and FP64 for
+    a whole FP64 solve (fp64 values)."""
+    vb = {"fp64": 8, "fp32": 4, "bf16": 2}[values]
+    xb = 8 if values == "fp64" else 4
     stored = diagonals // 2 + 1 if symmetric else diagonals
     rpc = -(-n // sms)
     offs = info.get("offsets") or []
     halo = sum(min(abs(int(o)), rpc) for o in offs if o) * sms
-    return iters * (stored * n * vb + 4 * n + 4 * halo) + 8 * n
+    mask = n if values == "fp64" else 0
+    return iters * (stored * n * vb + mask + xb * n + xb * halo) + 2 * xb * n
 
 
 def layout_key(info):
@@ -386,6 +390,19 @@ def run_ours(args, world, rank, local):
                     "alg_bytes_per_launch": alg, "launch_ms": round(per_launch_ms, 5),
                     "us_per_inner_iteration": round(per_launch_ms * 1e3 / iters, 3),
                     "timed": "in the solve (CUDA events around each launch, profile=1)", "peak_kind": peak_kind}
+    elif W["inner"] == "NONE" and W["outer"] == "CG" and prof["n_mv"] == 1 and prof["n_dot"] == 0:
+        # the whole FP64 CG solve as one on-chip launch (profiled as one SpMV-class launch)
+        iters = max(1, int(res.loop) - 1)  # the stopping test at the top of iteration `loop`
+        launch_ms = prof["t_mv"] * 1e3
+        alg = onchip_inner_bytes(nl, "fp64", nd, sym, minfo, iters)
+        if os.path.exists(tf):
+            traffic = json.load(open(tf)).get(f"{args.workload}:onchip_whole:fp64")
+        roofline = {"bound": "hbm", "achieved": round(alg / (launch_ms / 1e3) / 1e9, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(alg / (launch_ms / 1e3) / 1e9 / peak, 4), "traffic": traffic,
+                    "kernel": f"k_cg_onchip (the whole CG solve, {iters} iterations, vectors on chip, fp64)",
+                    "alg_bytes_per_launch": alg, "launch_ms": round(launch_ms, 5),
+                    "us_per_iteration": round(launch_ms * 1e3 / max(1, iters), 3),
+                    "timed": "in the solve (CUDA events around the launch, profile=1)", "peak_kind": peak_kind}
     else:
         w = spmv[vals]
         if os.path.exists(tf):

@@ -1044,6 +1044,7 @@ inline void ir_l2_release(ks_ctx *ctx, const CsrDev &A) {
   auto one = [&](const void *p, unsigned long long bytes) {
     if (!p || !bytes) return;
     const uintptr_t a0 = reinterpret_cast<uintptr_t>(p) & ~(uintptr_t)127;
+    ctx->next_class = kMemset;  // cache maintenance, profiled with the memsets
     launch_k(ctx, k_l2_normal, dim3(ctx->num_sms * 2), dim3(256), 0, reinterpret_cast<const char *>(a0),
              bytes + (reinterpret_cast<uintptr_t>(p) - a0));
   };

@@ -51,3 +51,5 @@ def test_onchip_inner_bytes():
     halo = 2 * (25600 + 160 + 1) * 148
     assert b.onchip_inner_bytes(n, "fp32", 7, 1, info, 20) == 20 * (16 * n + 4 * n + 4 * halo) + 8 * n
     assert b.onchip_inner_bytes(n, "bf16", 7, 1, info, 20) == 20 * (8 * n + 4 * n + 4 * halo) + 8 * n
+    # the whole FP64 solve: FP64 values, one mask byte per row, FP64 vectors
+    assert b.onchip_inner_bytes(n, "fp64", 7, 1, info, 20) == 20 * (32 * n + n + 8 * n + 8 * halo) + 16 * n
