@@ -656,7 +656,8 @@ def spmv_only(args):
 # hot kernel class for a profiler to capture by name (ncu -k regex:...).
 # (workload, method, inner, params)
 KERNEL_TOUR = [
-    ("c2_cg", "CG", "NONE", dict(E=1e-10, L=4)),                      # spmv_dia FP64, RUpdOp / XrUpdOp, XpbyToOp
+    ("c2_cg", "CG", "NONE", dict(E=1e-10, L=4)),                      # k_cg_onchip FP64 (the whole solve)
+    ("c2_cg", "CG", "NONE", dict(E=1e-10, L=4, cluster_solve=1)),     # the engine: spmv_dia FP64, RUpdOp, XpbyToOp
     ("c2_cr", "CR", "NONE", dict(E=1e-10, L=4)),
     ("c3_bicg", "BICG", "NONE", dict(E=1e-10, L=4)),                  # A^T SpMV
     ("c3_gmres30", "GMRES", "NONE", dict(E=1e-10, L=30, R=30)),       # block dot, basis kernel, Givens
