@@ -186,3 +186,24 @@ def test_on_chip_inner_cg_matches_kernel_per_step(ks, ctx, grid, outer, inner, p
     assert np.allclose(chip.hist_err[:m], step.hist_err[:m], rtol=1e-6, atol=0)
     if step.status == 0:
         assert np.linalg.norm(chip.x - step.x) <= 1e-6 * np.linalg.norm(step.x)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_on_chip_inner_cg_several_quads_per_thread(ks, ctx, prec):
+    """96^3 (884,736 rows, 5,984 per CTA): every thread owns two quads of
+    rows, so the on-chip kernel's passes span all 32 warps and its solution
+    write-out reads rows other warps updated last. Two solves give the same
+    bits, and they equal the kernel-per-step inner path's history and
+    solution bit for bit (alpha and beta are rounded to FP32, which absorbs
+    the different order of the FP64 dot sums)."""
+    A, b, _ = config_problem("varcoef3d", 96)
+    M = ctx.matrix(A, fp32=True, bf16=True)
+    p = dict(E=1e-10, L=2000, l=20, e=1e-30, inner_precision=prec, true_residual=2)
+    c1 = ks.solve(ctx, M, "VPCG", b, inner="CG", inner_fast=0, **p)
+    c2 = ks.solve(ctx, M, "VPCG", b, inner="CG", inner_fast=0, **p)
+    step = ks.solve(ctx, M, "VPCG", b, inner="CG", inner_fast=1, **p)
+    assert c1.status == 0 and c1.true_rel_res <= 1e-10
+    assert np.array_equal(c1.x, c2.x) and np.array_equal(c1.hist_err, c2.hist_err)
+    assert c1.loop == step.loop
+    assert np.array_equal(c1.hist_err, step.hist_err)
+    assert np.array_equal(c1.x, step.x)
