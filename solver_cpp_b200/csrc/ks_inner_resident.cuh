@@ -83,6 +83,7 @@ struct IrArgs {
   int K;      // rows per thread: ceil(rpc / kIrThreads) <= kIrMaxK (half for FP64)
   int whole;  // 1: a whole CG solve (|b|, the stopping state and the history of the method)
   int stencil;  // 1: full quads take ir_quad_mv_st (ir_stencil_ok holds, P is zero-padded)
+  void *P2;     // BiCG: the published p* (zero-padded as P)
 };
 
 // P's zero pad on each side for the stencil path: beyond the largest offset
@@ -576,12 +577,11 @@ __device__ __forceinline__ void ir_p4(const VT *sp, const VT *P, int r0, int nr,
 // warp). Every diagonal's value is loaded (zeros where a row has none); FP64
 // adds only the terms the row's mask names, FP32 adds every one.
 template <class VT, class MT, int NDG>
-__device__ __forceinline__ void ir_quad_mv(const DiaT<MT> &D, const IrArgs &a, const VT *sp, int r0, int nr, int li0,
+__device__ __forceinline__ void ir_quad_mv(const DiaT<MT> &D, const VT *P, const VT *sp, int r0, int nr, int li0,
                                            int nd, VT (&q)[kIrQ]) {
   constexpr int KD = NDG > 0 ? NDG : kMaxDiag;
   constexpr int B = sizeof(MT) == 2 ? KD : (sizeof(MT) == 4 ? 4 : 2);  // diagonals per batch
   constexpr bool kMask = std::is_same<MT, double>::value;
-  const VT *P = (const VT *)a.P;
   const int i0 = r0 + li0;
   const bool full = li0 + kIrQ <= nr;
   unsigned m = 0xffffffffu;  // the rows' mask bytes, row e in byte e
@@ -853,7 +853,7 @@ __device__ __forceinline__ int ir_body(const DiaT<MT> &D, const IrArgs &a, VT *s
           st_done = true;
         }
       }
-      if (!st_done) ir_quad_mv<VT, MT, NDG>(D, a, sp, r0, nr, li0, nd, q);
+      if (!st_done) ir_quad_mv<VT, MT, NDG>(D, P, sp, r0, nr, li0, nd, q);
 #pragma unroll
       for (int e = 0; e < kIrQ; e++)
         if (li0 + e < nr) acc = add_rn(acc, mul_rn(widen(pv[e]), widen(q[e])));
@@ -1025,6 +1025,262 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cg_onchip(DiaT<MT> D, IrArgs 
     tm_fence_after();
     tm_dealloc(s_tmem, kIrTmemCols);
   }
+}
+
+
+// ---------------------------------------------------------------- BiCG on chip
+// BiCG (bicg.cpp:148-260) as one cooperative launch of one CTA per SM, for
+// FP64 systems above the thread-block-cluster limit whose six vectors fit in
+// shared memory with one quad of rows per thread (rpc <= kIrTile: up to
+// about 606K rows), A and A^T both stencils with a diagonal copy
+// (ir_stencil_ok): x, r, r*, p, p* and q = A p of the CTA's rows in shared
+// memory; p and p* also published to P and P* (zero-padded), from which the
+// other CTAs gather the columns their rows reach. Per iteration, in the
+// engine's order:
+//   A: q = A p, (p*, q) summed over the grid -> alpha = (r*, r) / (p*, q);
+//   B: x += alpha p, r -= alpha q, r* -= alpha A^T p*, then (r, r) and
+//      (r*, r) in one reduction -> the stopping test on |r| / |b| at the top
+//      of iteration L + 1 (the engine's XrUpdOp) and, unless it stops, beta =
+//      (r*, r)_new / (r*, r);
+//   C: p = beta p + r, p* = beta p* + r*, published; each CTA then waits for
+//      the CTAs owning the columns its rows read through A or A^T.
+// Element operations are the engine's (CgMvEpi, XrUpdOp, BicgMvTEpi,
+// Xpby2PlainOp) in the same order; only the dot products add their terms in
+// another order (per thread, a fixed tree over the CTA, the CTAs' partials in
+// index order). Every wait is bounded (ir_allreduce, ir_publish_sync).
+constexpr int kIbVecs = 6;
+
+template <int NDG>
+__global__ void __launch_bounds__(kIrThreads, 1) k_bicg_onchip(DiaT<double> DA, DiaT<double> DT, IrArgs a) {
+  extern __shared__ __align__(16) unsigned char ir_smem_raw[];
+  double *sx = reinterpret_cast<double *>(ir_smem_raw);
+  double *sr = sx + a.rpc, *srs = sr + a.rpc, *sp = srs + a.rpc, *sps = sp + a.rpc, *sq = sps + a.rpc;
+  const int t = threadIdx.x;
+  const int r0 = blockIdx.x * a.rpc;
+  const int nr = max(0, min(a.rpc, a.n - r0));
+  const int li0 = kIrQ * t;  // the thread's quad of rows (rpc <= kIrTile)
+  const bool mine = li0 < nr, full = li0 + kIrQ <= nr;
+  const bool lead = blockIdx.x == 0 && t == 0;
+  DevState *st = a.st;
+  double *P = (double *)a.P, *Ps = (double *)a.P2;
+  const double eps = st->k.s[S_EPS];
+  const long long maxloop = st->k.aux[A_MAXLOOP];
+  // the CTAs owning the columns this CTA's rows read through A or A^T
+  int bl = blockIdx.x, bh = blockIdx.x;
+  if (nr > 0) {
+    const int lo = max(r0 + min(DA.off[0], DT.off[0]), 0);
+    const int hi = min(r0 + nr - 1 + max(DA.off[NDG - 1], DT.off[NDG - 1]), a.n - 1);
+    bl = min(bl, lo / a.rpc);
+    bh = max(bh, hi / a.rpc);
+  }
+  // one quad of a shared-memory vector in / out (vector access where full)
+  auto get = [&](const double *v, double (&o)[kIrQ]) { ir_own4(v, li0, nr, o); };
+  auto put = [&](double *v, const double (&o)[kIrQ]) {
+    if (full) {
+      sts4<double>(v + li0, o);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) v[li0 + e] = o[e];
+    }
+  };
+  auto publish = [&](double *G, const double (&o)[kIrQ]) {
+    if (full) {
+      stcg4<double>(G + r0 + li0, o);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) __stcg(G + r0 + li0 + e, o[e]);
+    }
+  };
+  auto mv = [&](const DiaT<double> &D, const double *G, const double *sv, const double (&own)[kIrQ],
+                double (&y)[kIrQ]) {
+    if (full)
+      ir_quad_mv_st<double, double, NDG>(D, G, sv, r0, nr, li0, own, y);
+    else
+      ir_quad_mv<double, double, NDG>(D, G, sv, r0, nr, li0, NDG, y);
+  };
+
+  // start (x0 = 0): r = r* = p = p* = b, x = 0; (r, r) -> |b| and the
+  // stopping test at the top of iteration 1 (NormBOp, StartEpi)
+  double acc = 0.0;
+  if (mine) {
+    double v[kIrQ], z[kIrQ];
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) {
+      const int li = li0 + e;
+      v[e] = li < nr ? __ldcg((const double *)a.rin + r0 + li) : 0.0;
+      z[e] = 0.0;
+      if (li < nr) acc = add_rn(acc, mul_rn(v[e], v[e]));
+    }
+    put(sx, z);
+    put(sr, v);
+    put(srs, v);
+    put(sp, v);
+    put(sps, v);
+    publish(P, v);
+    publish(Ps, v);
+  }
+  unsigned long long gen = 0, pgen = 1;
+  double s1[1] = {acc};
+  if (!ir_allreduce(a, ++gen, s1)) return;
+  double rr = s1[0];
+  const double bnorm = sqrt(rr);
+  int code = kRunning;
+  {
+    const double err = sqrt(rr) / bnorm;
+    if (1 > maxloop)
+      code = kMaxLoop;
+    else if (err <= eps)
+      code = kConverged;
+    else if (err != err)
+      code = kNaN;
+    if (lead) {
+      st->k.s[S_BNORM] = bnorm;
+      st->k.s[S_RR] = rr;
+      check_top(st, 1, err);
+    }
+  }
+  bool xw = false;
+  double alpha = 0.0, beta = 0.0;
+  if (code == kRunning) {
+    if (!ir_publish_sync(a, pgen, bl, bh)) return;
+    for (long long L = 1; L <= maxloop; L++) {
+      // A: q = A p, (p*, q) -> alpha
+      acc = 0.0;
+      if (mine) {
+        double pv[kIrQ], psv[kIrQ], q[kIrQ];
+        get(sp, pv);
+        mv(DA, P, sp, pv, q);
+        get(sps, psv);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++)
+          if (li0 + e < nr) acc = add_rn(acc, mul_rn(psv[e], q[e]));
+        put(sq, q);
+      }
+      s1[0] = acc;
+      if (!ir_allreduce(a, ++gen, s1)) return;
+      if (s1[0] == 0.0) {
+        code = kBreakdown;
+        alpha = 0.0;
+      } else {
+        alpha = div_rn(rr, s1[0]);
+        if (!isfinite(alpha)) code = kNaN;
+      }
+      if (code != kRunning) {
+        if (lead) set_done(st, code);
+        break;
+      }
+      // B: x += alpha p, r -= alpha q, r* -= alpha A^T p*; (r, r), (r*, r)
+      double s2[2] = {0.0, 0.0};
+      if (mine) {
+        double psv[kIrQ], w[kIrQ];
+        get(sps, psv);
+        mv(DT, Ps, sps, psv, w);
+        double pv[kIrQ], qv[kIrQ], xv[kIrQ], rv[kIrQ], rsv[kIrQ];
+        get(sp, pv);
+        get(sq, qv);
+        get(sx, xv);
+        get(sr, rv);
+        get(srs, rsv);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          xv[e] = add_rn(mul_rn(alpha, pv[e]), xv[e]);
+          rv[e] = add_rn(mul_rn(-alpha, qv[e]), rv[e]);
+          rsv[e] = add_rn(mul_rn(-alpha, w[e]), rsv[e]);
+          if (li0 + e < nr) {
+            s2[0] = add_rn(s2[0], mul_rn(rv[e], rv[e]));
+            s2[1] = add_rn(s2[1], mul_rn(rsv[e], rv[e]));
+          }
+        }
+        put(sx, xv);
+        put(sr, rv);
+        put(srs, rsv);
+      }
+      xw = true;
+      if (!ir_allreduce(a, ++gen, s2)) return;
+      // the stopping test at the top of iteration L + 1 comes first; beta
+      // only where the method goes on
+      const double err = sqrt(s2[0]) / bnorm;
+      if (L + 1 > maxloop)
+        code = kMaxLoop;
+      else if (err <= eps)
+        code = kConverged;
+      else if (err != err)
+        code = kNaN;
+      if (lead) check_top(st, L + 1, err);
+      if (code != kRunning) break;
+      if (rr == 0.0) {
+        code = kBreakdown;
+        beta = 0.0;
+      } else {
+        beta = div_rn(s2[1], rr);
+        if (!isfinite(beta)) code = kNaN;
+      }
+      rr = s2[1];
+      if (lead) {
+        st->k.s[S_BETA] = beta;
+        st->k.s[S_RR] = rr;
+        if (code != kRunning) set_done(st, code);
+      }
+      if (code != kRunning) break;
+      // C: p = beta p + r, p* = beta p* + r*, published
+      if (mine) {
+        double pv[kIrQ], rv[kIrQ], psv[kIrQ], rsv[kIrQ];
+        get(sp, pv);
+        get(sr, rv);
+        get(sps, psv);
+        get(srs, rsv);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          pv[e] = add_rn(mul_rn(beta, pv[e]), rv[e]);
+          psv[e] = add_rn(mul_rn(beta, psv[e]), rsv[e]);
+        }
+        put(sp, pv);
+        put(sps, psv);
+        publish(P, pv);
+        publish(Ps, psv);
+      }
+      if (!ir_publish_sync(a, ++pgen, bl, bh)) return;
+    }
+  }
+  // x out (zeros if the method stopped before its first update); thread t
+  // reads rows other threads updated last
+  __syncthreads();
+  double *x = (double *)a.x;
+  for (int li = t; li < nr; li += kIrThreads) __stcg(x + r0 + li, xw ? sx[li] : 0.0);
+  if (lead) {
+    st->k.s[S_ALPHA] = alpha;
+    if (code == kRunning) st->k.done = kMaxLoop;
+  }
+}
+
+template <int NDG>
+inline cudaError_t ib_launch_n(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, const IrArgs &a, size_t smem,
+                               int G, bool probe, bool *fits) {
+  auto fn = k_bicg_onchip<NDG>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (probe) {
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kIrThreads, smem);
+    *fits = e == cudaSuccess && b >= 1;
+    return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G);
+  cfg.blockDim = dim3(kIrThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ctx->launches++;
+  ctx->ir_used = true;  // its matrix lines are evict_last in L2 (ir_l2_release)
+  ProfLaunch pl(ctx, kMv);  // a profiled solve counts the whole solve as one SpMV-class launch
+  return cudaLaunchKernelEx(&cfg, fn, dview<double>(A), dview<double>(T), a);
 }
 
 // Lowers the L2 eviction priority of [p, p + bytes) back to normal (the

@@ -1083,11 +1083,61 @@ inline bool run_bicg_resident(const Env<double> &E, const double *b, double *x, 
 // bicg::solve. On systems of up to kGraphMaxN rows with a diagonal copy the
 // A-SpMV forms both directions (as run_cg does for p), and the separate
 // direction update is gone: three kernels per iteration instead of four.
+// BiCG above the thread-block-cluster limit with its six vectors in shared
+// memory (k_bicg_onchip, ks_inner_resident.cuh: one GPU, FP64, A and A^T
+// stencils with a diagonal copy, up to kIrTile rows per SM; ks_params.
+// cluster_solve 0): the whole solve as one cooperative launch. P and P*, the
+// published directions, take workspace slots 0-1 and 2-3, each between two
+// zero pads wider than the largest offset. Returns false, having launched
+// nothing, when the system does not qualify.
+inline bool run_bicg_onchip(const Env<double> &E, const double *b, double *x, double *ws, ks_status *s) {
+  if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A || !E.AT) return false;
+  const CsrDev &A = *E.A, &T = *E.AT;
+  if (!A.dia_nd || !A.dia_val || A.dia_nd != T.dia_nd || !T.dia_val) return false;
+  if (!ir_stencil_ok(A, E.n) || !ir_stencil_ok(T, E.n)) return false;
+  ks_ctx *ctx = E.ctx;
+  const long long G = ctx->num_sms;
+  const long long rpc = ((E.n + G - 1) / G + 31) / 32 * 32;
+  if (G > kIrMaxGrid || rpc > kIrTile) return false;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  const size_t smem = sizeof(double) * kIbVecs * (size_t)rpc;
+  if (smem + 2048 > (size_t)optin) return false;
+  const long long pad = std::max(ir_p_pad(A), ir_p_pad(T));
+  if (2 * E.ld < E.n + 2 * pad) return false;
+  bool fits = false;
+  const IrArgs probe{};
+  const cudaError_t pe = A.dia_nd == 7 ? ib_launch_n<7>(ctx, A, T, probe, smem, (int)G, true, &fits)
+                                       : ib_launch_n<5>(ctx, A, T, probe, smem, (int)G, true, &fits);
+  if (pe != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  double *const P = ws + pad, *const Ps = ws + 2 * E.ld + pad;
+  if (reinterpret_cast<uintptr_t>(P) % 32 || reinterpret_cast<uintptr_t>(Ps) % 32) return false;
+  launch_scalar(ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  IrArgs a{b, x, P, E.st, nullptr, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
+           (int)E.n, (int)rpc, 1, 1, 1};
+  a.P2 = Ps;
+  cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes((int)G), ctx->stream);
+  for (double *z : {ws, P + E.n, ws + 2 * E.ld, Ps + E.n})
+    if (e == cudaSuccess) e = cudaMemsetAsync(z, 0, sizeof(double) * pad, ctx->stream);
+  if (e == cudaSuccess)
+    e = A.dia_nd == 7 ? ib_launch_n<7>(ctx, A, T, a, smem, (int)G, false, &fits)
+                      : ib_launch_n<5>(ctx, A, T, a, smem, (int)G, false, &fits);
+  *s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip BiCG launch");
+  return true;
+}
+
 template <class VT>
 ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   if constexpr (std::is_same<VT, double>::value) {
     ks_status s = KS_OK;
     if (run_bicg_resident(E, b, x, &s)) return s;
+    if (run_bicg_onchip(E, b, x, ws, &s)) return s;
   }
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *rs = W.take(), *ps = W.take(), *mvv = W.take();
@@ -2477,7 +2527,8 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   ks_status s = run_method<double>(outer, E, b, xs, ws, dws, vp ? &IR : nullptr);
   if (s == KS_OK && vp) s = IR.status;
   if (ctx->ir_used) {
-    ir_l2_release(ctx, *A);
+    ir_l2_release(ctx, mat->A);
+    if (mat->has_T) ir_l2_release(ctx, mat->T);
     ctx->ir_used = false;
   }
   KS_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));

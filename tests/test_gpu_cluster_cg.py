@@ -214,3 +214,55 @@ def test_onchip_cg_within_reference_envelope(ks, ctx, oracle, prob, g):
         check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
         assert r.true_res_log10 < -9.5
     assert np.linalg.norm(chip.x - step.x) <= 1e-8 * np.linalg.norm(step.x)
+
+
+@pytest.mark.parametrize("prob,g", [("convdiff2d", 200), ("convdiff3d", 40), ("convdiff2d", 256), ("varcoef2d", 256)])
+def test_onchip_bicg_against_oracle_and_engine(ks, ctx, oracle, prob, g):
+    """BiCG above one cluster's reach, its six vectors in shared memory across
+    the GPU: one cooperative launch (cluster_solve 0; the profile counts the
+    whole solve as one SpMV-class launch and no dot kernels). It applies the
+    engine's element operations and adds the dot products in another order.
+    BiCG's iteration count on the upwind systems moves with that order alone
+    (convdiff2d 200^2: the oracle takes 791 iterations with sequential sums,
+    749 / 704 / 663 with 16 / 256 / 4096 partial sums, 654 pairwise), so the
+    count of either GPU path must lie in the range of the oracle's orders
+    (+-2 %). Then the oracle's verdict, a true residual within 3x the
+    oracle's, the engine's solution to 1e-7 and the first history entries to
+    1e-9. varcoef2d is symmetric (symmetric diagonal storage for A and its
+    transpose)."""
+    A, b, _ = config_problem(prob, g)
+    M = ctx.matrix(A, transpose=True)
+    chip = ks.solve(ctx, M, "BICG", b, E=1e-12, L=20000, cluster_solve=0, profile=1)
+    step = ks.solve(ctx, M, "BICG", b, E=1e-12, L=20000, cluster_solve=1)
+    assert chip.report["n_mv"] == 1 and chip.report["n_dot"] == 0, chip.report
+    o, _, _ = oracle_envelope(oracle, A, b, "BICG", E=1e-12, L=20000)
+    o_true = np.linalg.norm(b - A.to_scipy() @ o["x"]) / np.linalg.norm(b)
+    P = oracle.Problem(A)
+    loops = [oracle.solve(P, b, "BICG", E=1e-12, L=20000, sum_chunks=c)["loop"] for c in (0, 16, 256, 4096, -1)]
+    lo, hi = min(loops) * 0.98 - 1, max(loops) * 1.02 + 1
+    assert chip.status == step.status == o["status"] == 0
+    assert lo <= chip.loop <= hi, (chip.loop, loops)
+    assert lo <= step.loop <= hi, (step.loop, loops)
+    assert chip.true_rel_res < 3 * max(o_true, 1e-12)
+    assert np.linalg.norm(chip.x - step.x) <= 1e-7 * np.linalg.norm(step.x)
+    m = min(len(chip.hist_err), len(step.hist_err), 10)
+    assert np.allclose(chip.hist_err[:m], step.hist_err[:m], rtol=1e-9, atol=0)
+
+
+def test_onchip_bicg_maxloop_and_zero_rhs(ks, ctx):
+    """The on-chip BiCG stops at maxloop with the engine's loop count and
+    history labels, and a zero right-hand side stops at once (NaN test of
+    0/0), as the engine does."""
+    A, b, _ = config_problem("convdiff2d", 200)
+    M = ctx.matrix(A, transpose=True)
+    for L in (1, 7, 300):
+        chip = ks.solve(ctx, M, "BICG", b, E=1e-30, L=L, cluster_solve=0)
+        step = ks.solve(ctx, M, "BICG", b, E=1e-30, L=L, cluster_solve=1)
+        assert chip.status == step.status == 2
+        assert chip.loop == step.loop
+        assert np.array_equal(chip.hist_iter, step.hist_iter)
+    z = np.zeros(A.n)
+    chip = ks.solve(ctx, M, "BICG", z, E=1e-10, L=100, cluster_solve=0)
+    step = ks.solve(ctx, M, "BICG", z, E=1e-10, L=100, cluster_solve=1)
+    assert chip.status == step.status
+    assert chip.loop == step.loop
