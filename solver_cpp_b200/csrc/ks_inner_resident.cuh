@@ -1283,6 +1283,280 @@ inline cudaError_t ib_launch_n(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, co
   return cudaLaunchKernelEx(&cfg, fn, dview<double>(A), dview<double>(T), a);
 }
 
+
+// ---------------------------------------------------------------- CR on chip
+// CR (cr.cpp:151-250) as one cooperative launch of one CTA per SM, for FP64
+// stencil systems above the cluster limit up to ~2.1M rows (ir_shape<double>):
+// r and p of the CTA's rows in shared memory, q = A p and s = A r in TMEM
+// (lanes and columns as in k_cg_onchip), x in global memory, updated in
+// place. r, the SpMV's input, is also published to a zero-padded array R.
+// Per iteration, in the engine's order (XrUpdOp, CrMvEpi, Xpby2ToOp):
+//   B: r -= alpha q, stored and published, (r, r) posted; x += alpha p in the
+//      reduction's shadow -> the stopping test at the top of iteration L + 1;
+//      the reduction is also the barrier after which every CTA reads R;
+//   A: s = A r, (r, s) -> beta = (r, s) / rs, rs = (r, s);
+//   C: p = beta p + r, q = beta q + s, (q, q) -> alpha = rs / (q, q).
+// Three grid reductions and no publication wait per iteration; element
+// operations are the engine's, only the dot sums' order differs.
+template <int NDG>
+__global__ void __launch_bounds__(kIrThreads, 1) k_cr_onchip(DiaT<double> D, IrArgs a) {
+  using TW = IrWords<double>;
+  extern __shared__ __align__(16) unsigned char ir_smem_raw[];
+  __shared__ uint32_t s_tmem;
+  double *sr = reinterpret_cast<double *>(ir_smem_raw);  // r of the CTA's rows
+  double *sp = sr + a.rpc;                                // p of the CTA's rows
+  const int t = threadIdx.x;
+  const int r0 = blockIdx.x * a.rpc;
+  const int nr = max(0, min(a.rpc, a.n - r0));
+  const int quads = (a.rpc + kIrTile - 1) / kIrTile;
+  const bool lead = blockIdx.x == 0 && t == 0;
+  DevState *st = a.st;
+  double *R = (double *)a.P, *x = (double *)a.x;
+  const double eps = st->k.s[S_EPS];
+  const long long maxloop = st->k.aux[A_MAXLOOP];
+  if (t < 32) {
+    tm_alloc(&s_tmem, kIrTmemCols);
+    tm_relinquish();
+    tm_fence_before();
+  }
+  __syncthreads();
+  tm_fence_after();
+  const uint32_t w = t >> 5;
+  const uint32_t tm = s_tmem + ((32u * (w & 3u)) << 16) + 64u * (w >> 2);
+  const uint32_t tq = tm, ts = tm + 32;  // q and s of the thread's quads, TW::W words apart
+  auto own = [&](const double *v, int li0, double (&o)[kIrQ]) { ir_own4(v, li0, nr, o); };
+  auto put = [&](double *v, int li0, const double (&o)[kIrQ]) {
+    if (li0 + kIrQ <= nr) {
+      sts4<double>(v + li0, o);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) v[li0 + e] = o[e];
+    }
+  };
+  auto gput = [&](double *G, int li0, const double (&o)[kIrQ]) {
+    if (li0 + kIrQ <= nr) {
+      stcg4<double>(G + r0 + li0, o);
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) __stcg(G + r0 + li0 + e, o[e]);
+    }
+  };
+  auto mv = [&](int li0, const double (&own4)[kIrQ], double (&y)[kIrQ]) {
+    bool done = false;
+    if constexpr (NDG == 5 || NDG == 7) {
+      if (a.stencil && li0 + kIrQ <= nr) {
+        ir_quad_mv_st<double, double, NDG>(D, R, sr, r0, nr, li0, own4, y);
+        done = true;
+      }
+    }
+    if (!done) ir_quad_mv<double, double, NDG>(D, R, sr, r0, nr, li0, NDG > 0 ? NDG : D.nd, y);
+  };
+  unsigned long long gen = 0;
+  int code = kRunning;
+  double alpha = 0.0, beta = 0.0, rs = 0.0, bnorm = 0.0;
+  bool ok = true;  // no wait ran out
+  // start (x0 = 0): r = b, p = r, x = 0, R published; (r, r) -> |b| and the
+  // stopping test at the top of iteration 1
+  double acc = 0.0;
+  for (int j = 0; j < quads; j++) {
+    const int li0 = j * kIrTile + kIrQ * t;
+    if (li0 >= nr) continue;
+    double v[kIrQ];
+    const double z[kIrQ] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int e = 0; e < kIrQ; e++) {
+      const int li = li0 + e;
+      v[e] = li < nr ? __ldcg((const double *)a.rin + r0 + li) : 0.0;
+      if (li < nr) acc = add_rn(acc, mul_rn(v[e], v[e]));
+    }
+    put(sr, li0, v);
+    put(sp, li0, v);
+    gput(R, li0, v);
+    gput(x, li0, z);
+  }
+  double s1[1] = {acc};
+  ok = ir_allreduce(a, ++gen, s1);
+  if (ok) {
+    const double rr = s1[0];
+    bnorm = sqrt(rr);
+    const double err = sqrt(rr) / bnorm;
+    if (1 > maxloop)
+      code = kMaxLoop;
+    else if (err <= eps)
+      code = kConverged;
+    else if (err != err)
+      code = kNaN;
+    if (lead) {
+      st->k.s[S_BNORM] = bnorm;
+      check_top(st, 1, err);
+    }
+  }
+  // q = A p (p = r) = s; rs = (r, s), alpha = rs / (q, q)   (CrStartMvEpi)
+  if (ok && code == kRunning) {
+    double s2[2] = {0.0, 0.0};
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      double rv[kIrQ], y[kIrQ] = {0.0, 0.0, 0.0, 0.0};
+      if (li0 < nr) {
+        own(sr, li0, rv);
+        mv(li0, rv, y);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          if (li0 + e < nr) {
+            s2[0] = add_rn(s2[0], mul_rn(rv[e], y[e]));
+            s2[1] = add_rn(s2[1], mul_rn(y[e], y[e]));
+          }
+        }
+      }
+      TW::put(tq + TW::W * j, y);
+      TW::put(ts + TW::W * j, y);
+    }
+    tm_wait_st();
+    ok = ir_allreduce(a, ++gen, s2);
+    if (ok) {
+      rs = s2[0];
+      if (s2[1] == 0.0) {
+        code = kBreakdown;
+      } else {
+        alpha = div_rn(rs, s2[1]);
+        if (!isfinite(alpha)) code = kNaN;
+      }
+      if (lead) {
+        st->k.s[S_RR] = rs;
+        st->k.s[S_ALPHA] = alpha;
+        if (code != kRunning) set_done(st, code);
+      }
+    }
+  }
+  for (long long L = 1; ok && code == kRunning && L <= maxloop; L++) {
+    // B: r -= alpha q, stored and published; (r, r) posted; x += alpha p
+    acc = 0.0;
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      double qv[kIrQ];
+      TW::get(tq + TW::W * j, qv);
+      if (li0 < nr) {
+        double rv[kIrQ];
+        own(sr, li0, rv);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          rv[e] = add_rn(mul_rn(-alpha, qv[e]), rv[e]);
+          if (li0 + e < nr) acc = add_rn(acc, mul_rn(rv[e], rv[e]));
+        }
+        put(sr, li0, rv);
+        gput(R, li0, rv);
+      }
+    }
+    s1[0] = acc;
+    ir_red_post<1>(a, ++gen, s1);
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      if (li0 >= nr) continue;
+      double pv[kIrQ], xv[kIrQ];
+      own(sp, li0, pv);
+      if (li0 + kIrQ <= nr) {
+        ld4<double>(x + r0 + li0, xv, true);
+      } else {
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) xv[e] = li0 + e < nr ? __ldcg(x + r0 + li0 + e) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) xv[e] = add_rn(mul_rn(alpha, pv[e]), xv[e]);
+      gput(x, li0, xv);
+    }
+    if (!(ok = ir_red_wait<1>(a, gen, s1))) break;
+    {
+      const double err = sqrt(s1[0]) / bnorm;
+      if (L + 1 > maxloop)
+        code = kMaxLoop;
+      else if (err <= eps)
+        code = kConverged;
+      else if (err != err)
+        code = kNaN;
+      if (lead) check_top(st, L + 1, err);
+      if (code != kRunning) break;
+    }
+    // A: s = A r; (r, s) -> beta
+    acc = 0.0;
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      double y[kIrQ] = {0.0, 0.0, 0.0, 0.0};
+      if (li0 < nr) {
+        double rv[kIrQ];
+        own(sr, li0, rv);
+        mv(li0, rv, y);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++)
+          if (li0 + e < nr) acc = add_rn(acc, mul_rn(rv[e], y[e]));
+      }
+      TW::put(ts + TW::W * j, y);
+    }
+    tm_wait_st();
+    s1[0] = acc;
+    if (!(ok = ir_allreduce(a, ++gen, s1))) break;
+    if (rs == 0.0) {
+      code = kBreakdown;
+      beta = 0.0;
+    } else {
+      beta = div_rn(s1[0], rs);
+      if (!isfinite(beta)) code = kNaN;
+    }
+    rs = s1[0];
+    if (lead) {
+      st->k.s[S_BETA] = beta;
+      st->k.s[S_RR] = rs;
+      if (code != kRunning) set_done(st, code);
+    }
+    if (code != kRunning) break;
+    // C: p = beta p + r, q = beta q + s; (q, q) -> alpha
+    acc = 0.0;
+    for (int j = 0; j < quads; j++) {
+      const int li0 = j * kIrTile + kIrQ * t;
+      double qv[kIrQ], sv[kIrQ];
+      TW::get2(tq + TW::W * j, qv, ts + TW::W * j, sv);
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) qv[e] = add_rn(mul_rn(beta, qv[e]), sv[e]);
+      if (li0 < nr) {
+        double pv[kIrQ], rv[kIrQ];
+        own(sp, li0, pv);
+        own(sr, li0, rv);
+#pragma unroll
+        for (int e = 0; e < kIrQ; e++) {
+          pv[e] = add_rn(mul_rn(beta, pv[e]), rv[e]);
+          if (li0 + e < nr) acc = add_rn(acc, mul_rn(qv[e], qv[e]));
+        }
+        put(sp, li0, pv);
+      }
+      TW::put(tq + TW::W * j, qv);
+    }
+    tm_wait_st();
+    s1[0] = acc;
+    if (!(ok = ir_allreduce(a, ++gen, s1))) break;
+    if (s1[0] == 0.0) {
+      code = kBreakdown;
+      alpha = 0.0;
+    } else {
+      alpha = div_rn(rs, s1[0]);
+      if (!isfinite(alpha)) code = kNaN;
+    }
+    if (lead) {
+      st->k.s[S_ALPHA] = alpha;
+      if (code != kRunning) set_done(st, code);
+    }
+  }
+  if (ok && lead && code == kRunning) set_done(st, kMaxLoop);
+  // every thread's TMEM accesses are complete (each waited on its own); the
+  // columns go back on every path out of the loop
+  tm_fence_before();
+  __syncthreads();
+  if (t < 32) {
+    tm_fence_after();
+    tm_dealloc(s_tmem, kIrTmemCols);
+  }
+}
+
 // Lowers the L2 eviction priority of [p, p + bytes) back to normal (the
 // lines stay cached), p 128-byte aligned: after the on-chip kernels' evict_last
 // loads, so that the diagonal copy does not keep its place in L2 ahead of
@@ -1375,6 +1649,34 @@ inline cudaError_t ir_launch(ks_ctx *ctx, const CsrDev &A, const IrArgs &a, cons
   if (A.dia_nd == 7) return ir_launch_n<VT, MT, 7>(ctx, A, a, sh, probe, fits, cls);
   if (A.dia_nd == 5) return ir_launch_n<VT, MT, 5>(ctx, A, a, sh, probe, fits, cls);
   return ir_launch_n<VT, MT, 0>(ctx, A, a, sh, probe, fits, cls);
+}
+
+template <int NDG>
+inline cudaError_t icr_launch_n(ks_ctx *ctx, const CsrDev &A, const IrArgs &a, const IrShape &sh, bool probe,
+                                bool *fits) {
+  auto fn = k_cr_onchip<NDG>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
+  if (e != cudaSuccess) return e;
+  if (probe) {
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kIrThreads, sh.smem);
+    *fits = e == cudaSuccess && b >= 1;
+    return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sh.G);
+  cfg.blockDim = dim3(kIrThreads);
+  cfg.dynamicSmemBytes = sh.smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  ctx->launches++;
+  ctx->ir_used = true;  // its matrix lines are evict_last in L2 (ir_l2_release)
+  ProfLaunch pl(ctx, kMv);  // a profiled solve counts the whole solve as one SpMV-class launch
+  return cudaLaunchKernelEx(&cfg, fn, dview<double>(A), a);
 }
 
 }  // namespace ks

@@ -957,11 +957,52 @@ inline bool run_cr_resident(const Env<double> &E, const double *b, double *x, ks
   return true;
 }
 
+// CR above the thread-block-cluster limit with r and p in shared memory, q
+// and s in TMEM and x in place in global memory (k_cr_onchip,
+// ks_inner_resident.cuh: one GPU, FP64, a diagonal copy, up to ~2.1M rows;
+// ks_params.cluster_solve 0): the whole solve as one cooperative launch. R,
+// the published r, takes workspace slots 0-1, between two zero pads for the
+// stencil path. Returns false, having launched nothing, when the system does
+// not qualify.
+inline bool run_cr_onchip(const Env<double> &E, const double *b, double *x, double *ws, ks_status *s) {
+  if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A->dia_nd || !E.A->dia_val) return false;
+  if (reinterpret_cast<uintptr_t>(x) % 16) return false;  // 16-byte vector accesses of x
+  ks_ctx *ctx = E.ctx;
+  const CsrDev &A = *E.A;
+  IrShape sh;
+  if (!ir_shape<double>(ctx, E.n, &sh)) return false;
+  bool fits = false;
+  const IrArgs probe{};
+  auto launch = [&](const IrArgs &a, bool pr) {
+    return A.dia_nd == 7 ? icr_launch_n<7>(ctx, A, a, sh, pr, &fits)
+                         : A.dia_nd == 5 ? icr_launch_n<5>(ctx, A, a, sh, pr, &fits)
+                                         : icr_launch_n<0>(ctx, A, a, sh, pr, &fits);
+  };
+  if (launch(probe, true) != cudaSuccess || !fits) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  const long long pad = ir_p_pad(A);
+  const bool stencil = ir_stencil_ok(A, E.n) && 2 * E.ld >= E.n + 2 * pad;
+  double *const R = ws + (stencil ? pad : 0);
+  if (reinterpret_cast<uintptr_t>(R) % 32) return false;  // 32-byte vector loads of R
+  launch_scalar(ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
+  const IrArgs a{b, x, R, E.st, nullptr, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
+                 (int)E.n, sh.rpc, sh.K, 1, stencil ? 1 : 0};
+  cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes(sh.G), ctx->stream);
+  if (e == cudaSuccess && stencil) e = cudaMemsetAsync(ws, 0, sizeof(double) * pad, ctx->stream);
+  if (e == cudaSuccess && stencil) e = cudaMemsetAsync(R + E.n, 0, sizeof(double) * pad, ctx->stream);
+  if (e == cudaSuccess) e = launch(a, false);
+  *s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip CR launch");
+  return true;
+}
+
 template <class VT>
 ks_status run_cr(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   if constexpr (std::is_same<VT, double>::value) {
     ks_status s = KS_OK;
     if (run_cr_resident(E, b, x, &s)) return s;
+    if (run_cr_onchip(E, b, x, ws, &s)) return s;
   }
   Ws<VT> W{ws, E.ld, E.off};
   VT *r = W.take(), *q = W.take(), *s = W.take();

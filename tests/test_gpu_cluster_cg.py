@@ -266,3 +266,41 @@ def test_onchip_bicg_maxloop_and_zero_rhs(ks, ctx):
     step = ks.solve(ctx, M, "BICG", z, E=1e-10, L=100, cluster_solve=1)
     assert chip.status == step.status
     assert chip.loop == step.loop
+
+
+@pytest.mark.parametrize("prob,g", [("varcoef3d", 40), ("poisson3d", 64), ("varcoef2d", 256), ("poisson2d", 300)])
+def test_onchip_cr_within_reference_envelope(ks, ctx, oracle, prob, g):
+    """CR above one cluster's reach, r and p in shared memory, q and s in TMEM
+    and x in global memory: one cooperative launch (cluster_solve 0; the
+    profile counts the whole solve as one SpMV-class launch). It must meet the
+    reference's parity criterion against the oracle (envelope of the
+    oracle's chunked-sum runs) as the engine (cluster_solve 1) does, with the
+    same verdict and solution. poisson2d 300^2 has offsets +-300, multiples
+    of 4; 64^3 has 4 quads of rows per thread."""
+    A, b, _ = config_problem(prob, g)
+    M = ctx.matrix(A)
+    chip = ks.solve(ctx, M, "CR", b, E=1e-10, L=20000, cluster_solve=0, profile=1)
+    step = ks.solve(ctx, M, "CR", b, E=1e-10, L=20000, cluster_solve=1)
+    assert chip.report["n_mv"] == 1 and chip.report["n_dot"] == 0, chip.report
+    o, env, lr = oracle_envelope(oracle, A, b, "CR", E=1e-10, L=20000)
+    for r in (chip, step):
+        assert r.converged and o["status"] == 0
+        check_history(r.hist_iter, r.hist_err, o["hist_iter"], o["hist_err"], env, r.loop, o["loop"], lr)
+        assert r.true_res_log10 < -9.5
+    assert np.linalg.norm(chip.x - step.x) <= 1e-8 * np.linalg.norm(step.x)
+
+
+def test_onchip_cr_maxloop_and_generic_offsets(ks, ctx):
+    """The on-chip CR stops at maxloop with the engine's loop count and
+    history labels; varcoef3d 37^3 has offsets 37 and 1369 (not multiples of
+    4: the generic quad path) and agrees with the engine to rounding."""
+    A, b, _ = config_problem("varcoef3d", 37)
+    M = ctx.matrix(A)
+    for L in (1, 7, 300):
+        chip = ks.solve(ctx, M, "CR", b, E=1e-30, L=L, cluster_solve=0)
+        step = ks.solve(ctx, M, "CR", b, E=1e-30, L=L, cluster_solve=1)
+        assert chip.status == step.status == 2
+        assert chip.loop == step.loop
+        assert np.array_equal(chip.hist_iter, step.hist_iter)
+        m = min(len(chip.hist_err), 20)
+        assert np.allclose(chip.hist_err[:m], step.hist_err[:m], rtol=1e-9, atol=0)
