@@ -213,6 +213,19 @@ def onchip_inner_bytes(n, values, diagonals, symmetric, info, iters, sms=148):
     return iters * (stored * n * vb + mask + xb * n + xb * halo) + 2 * xb * n
 
 
+def onchip_whole_bytes(method, n, diagonals, symmetric, info, iters, sms=148):
+    """Algorithmic bytes of a whole FP64 solve as one on-chip launch: CG as
+    onchip_inner_bytes; CR also updates x in place in global memory (read and
+    written every iteration, 16 n); BiCG runs two SpMVs per iteration (A and
+    A^T: both diagonal copies, masks, published vectors and halos)."""
+    one = onchip_inner_bytes(n, "fp64", diagonals, symmetric, info, iters, sms)
+    if method == "CR":
+        return one + iters * 16 * n
+    if method == "BICG":
+        return 2 * one - 16 * n
+    return one
+
+
 def layout_key(info):
     """Short name of the layout the SpMV reads: d<diagonals> or i<index bytes>."""
     return f"d{info['diagonals']}" if info.get("diagonals") else f"i{info['index_bytes']}"
@@ -393,16 +406,18 @@ def run_ours(args, world, rank, local):
                              "the outer iteration's kernels, which stream ~600 MB through L2, so this is "
                              "also the cold figure (frac_cold)", "peak_kind": peak_kind}
         roofline["frac_cold"] = roofline["frac"]
-    elif W["inner"] == "NONE" and W["outer"] == "CG" and prof["n_mv"] == 1 and prof["n_dot"] == 0:
-        # the whole FP64 CG solve as one on-chip launch (profiled as one SpMV-class launch)
+    elif (W["inner"] == "NONE" and W["outer"] in ("CG", "CR", "BICG") and prof["n_mv"] == 1
+          and prof["n_dot"] == 0):
+        # the whole FP64 solve as one on-chip launch (profiled as one SpMV-class launch)
         iters = max(1, int(res.loop) - 1)  # the stopping test at the top of iteration `loop`
         launch_ms = prof["t_mv"] * 1e3
-        alg = onchip_inner_bytes(nl, "fp64", nd, sym, minfo, iters)
+        alg = onchip_whole_bytes(W["outer"], nl, nd, sym, minfo, iters)
+        kname = {"CG": "k_cg_onchip", "CR": "k_cr_onchip", "BICG": "k_bicg_onchip"}[W["outer"]]
         if os.path.exists(tf):
             traffic = json.load(open(tf)).get(f"{args.workload}:onchip_whole:fp64")
         roofline = {"bound": "hbm", "achieved": round(alg / (launch_ms / 1e3) / 1e9, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(alg / (launch_ms / 1e3) / 1e9 / peak, 4), "traffic": traffic,
-                    "kernel": f"k_cg_onchip (the whole CG solve, {iters} iterations, vectors on chip, fp64)",
+                    "kernel": f"{kname} (the whole {W['outer']} solve, {iters} iterations, vectors on chip, fp64)",
                     "alg_bytes_per_launch": alg, "launch_ms": round(launch_ms, 5),
                     "us_per_iteration": round(launch_ms * 1e3 / max(1, iters), 3),
                     "timed": "in the solve (CUDA events around the launch, profile=1)", "peak_kind": peak_kind}

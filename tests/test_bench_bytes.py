@@ -53,3 +53,7 @@ def test_onchip_inner_bytes():
     assert b.onchip_inner_bytes(n, "bf16", 7, 1, info, 20) == 20 * (8 * n + 4 * n + 4 * halo) + 8 * n
     # the whole FP64 solve: FP64 values, one mask byte per row, FP64 vectors
     assert b.onchip_inner_bytes(n, "fp64", 7, 1, info, 20) == 20 * (32 * n + n + 8 * n + 8 * halo) + 16 * n
+    one = b.onchip_inner_bytes(n, "fp64", 7, 1, info, 20)
+    assert b.onchip_whole_bytes("CG", n, 7, 1, info, 20) == one
+    assert b.onchip_whole_bytes("CR", n, 7, 1, info, 20) == one + 20 * 16 * n  # x read and written in place
+    assert b.onchip_whole_bytes("BICG", n, 7, 1, info, 20) == 2 * one - 16 * n  # A and A^T, b and x once
