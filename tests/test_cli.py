@@ -171,8 +171,10 @@ def test_cli_report_parses_like_data2csv(cli, tmp_path):
     """The log carries the reference's header and times report (times.cpp:44-76)
     line for line: every field data2csv.sh reads is there and numeric, the
     GPU Dot + MV + other add up to the solve time."""
-    A, b, rd = _problem_dir(tmp_path, "p3", "poisson3d", 40)  # BiCG: one kernel per step
-    r = run(["-S", "bicg", "-E", "1e-10", "-m", "p3", "-p", str(tmp_path)], rd)
+    # GMRES(30): one kernel per step (CG, CR and BiCG run this system as one
+    # on-chip launch, without separate dot kernels to time)
+    A, b, rd = _problem_dir(tmp_path, "p3", "poisson3d", 40)
+    r = run(["-S", "gmres", "-R", "30", "-E", "1e-10", "-m", "p3", "-p", str(tmp_path)], rd)
     assert r.returncode == 0, r.stderr
     f = _data2csv_fields(r.stdout)
     assert f["CUDA"] == "On" and f["MultiGPU"] == "Off"

@@ -131,7 +131,14 @@ def test_adjoint_gradient_fd_512(ks, ctx, prob, solver):
     quotient is formed from the exact identity for the two perturbed
     solutions, so that it does not cancel in the loss (L ~ n/2): with
     A+- = A +- h e_i e_c^T and A- x- = b, the difference d = x+ - x- solves
-    A+ d = -2 h x-_c e_i, and L(x+) - L(x-) = d^T (x- + d/2 - x*)."""
+    A+ d = -2 h x-_c e_i, and L(x+) - L(x-) = d^T (x- + d/2 - x*).
+    The gradient is the library's default path (BiCG: the on-chip kernel);
+    the finite-difference solves use the kernel-per-step engine
+    (cluster_solve 1). BiCG on the upwind system lets its residual grow
+    about 1000-fold before it converges, and from there its trajectory
+    depends on the rounding of its dot sums: with the on-chip kernel's order
+    one of these 64 perturbed systems (entry 46693) stalls at a residual of
+    O(1) for 40,000 iterations, where the engine's order converges in 2,174."""
     from solver_cpp_b200.matrices import CSR
 
     A, b, _ = config_problem(prob, 512)
@@ -157,12 +164,12 @@ def test_adjoint_gradient_fd_512(ks, ctx, prob, solver):
         vm[j] -= step
         vp[j] += step
         Mm = ctx.matrix(CSR(A.ptr, A.col, vm), transpose=tr)
-        xm = ks.solve(ctx, Mm, solver, b, **kw)
+        xm = ks.solve(ctx, Mm, solver, b, cluster_solve=1, **kw)
         Mm.close()
         rhs = np.zeros(A.n)
         rhs[i] = -2.0 * step * xm.x[c]
         Mp = ctx.matrix(CSR(A.ptr, A.col, vp), transpose=tr)
-        d = ks.solve(ctx, Mp, solver, rhs, **kw)
+        d = ks.solve(ctx, Mp, solver, rhs, cluster_solve=1, **kw)
         Mp.close()
         assert xm.converged and d.converged
         fd = d.x @ (xm.x + 0.5 * d.x - xstar) / (2.0 * step)
@@ -171,7 +178,7 @@ def test_adjoint_gradient_fd_512(ks, ctx, prob, solver):
     for i in rng.choice(A.n, 8, replace=False):
         rhs = np.zeros(A.n)
         rhs[i] = 2e-6
-        d = ks.solve(ctx, M, solver, rhs, **kw)
+        d = ks.solve(ctx, M, solver, rhs, cluster_solve=1, **kw)
         fd = d.x @ (fw.x - xstar) / 2e-6
         worst.append(abs(gb[i] - fd) / (abs(fd) + 1e-9 * np.max(np.abs(gb))))
     assert max(worst) <= 1e-6, f"largest relative deviation {max(worst):.3e}"
