@@ -91,3 +91,31 @@ def test_zero_rhs_is_nan_detected(ks, ctx):
     M = ctx.matrix(A)
     r = ks.solve(ctx, M, "CG", np.zeros(A.n), E=1e-10, cluster_solve=1)
     assert r.status == 4
+
+
+@pytest.mark.parametrize("case", ["cg", "cr", "bicg", "vpcg"])
+def test_on_chip_wait_runs_out_and_context_survives(ks, ctx, case):
+    """The cooperative on-chip kernels (whole CG / CR / BiCG solves, the VP
+    methods' FP32 inner CG) bound every grid reduction and publication wait
+    by the context's wait limit. With a limit of 1 ns the waits give up: the
+    kernel sets the timeout flag, releases its TMEM columns and returns, the
+    solve reports KS_TIMEOUT, and the context keeps working (the same solve
+    converges once the limit is back)."""
+    prob, g, method, kw = {
+        "cg": ("poisson3d", 40, "CG", {}),
+        "cr": ("poisson3d", 40, "CR", {}),
+        "bicg": ("convdiff2d", 200, "BICG", {}),
+        "vpcg": ("varcoef3d", 24, "VPCG", dict(inner="CG", l=20, e=1e-30, inner_precision="fp32")),
+    }[case]
+    A, b, _ = config_problem(prob, g)
+    M = ctx.matrix(A, transpose=True, fp32=True)
+    ctx.set_wait_limit(1)
+    try:
+        with pytest.raises(ks.KrylovError) as e:
+            ks.solve(ctx, M, method, b, E=1e-10, L=5, **kw)
+        assert e.value.status == 7  # KS_TIMEOUT
+    finally:
+        ctx.set_wait_limit(0)
+    ctx.synchronize()
+    r = ks.solve(ctx, M, method, b, E=1e-10, L=20000, **kw)
+    assert r.converged and r.true_rel_res < 1e-9, (r.status, r.true_rel_res)
