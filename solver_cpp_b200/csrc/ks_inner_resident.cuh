@@ -1289,7 +1289,8 @@ inline cudaError_t ib_launch_n(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, co
 // stencil systems above the cluster limit up to ~2.1M rows (ir_shape<double>):
 // r and p of the CTA's rows in shared memory, q = A p and s = A r in TMEM
 // (lanes and columns as in k_cg_onchip), x in global memory, updated in
-// place. r, the SpMV's input, is also published to a zero-padded array R.
+// place with streaming (evict-first) accesses. r, the SpMV's input, is also
+// published to a zero-padded array R.
 // Per iteration, in the engine's order (XrUpdOp, CrMvEpi, Xpby2ToOp):
 //   B: r -= alpha q, stored and published, (r, r) posted; x += alpha p in the
 //      reduction's shadow -> the stopping test at the top of iteration L + 1;
@@ -1343,6 +1344,32 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cr_onchip(DiaT<double> D, IrA
         if (li0 + e < nr) __stcg(G + r0 + li0 + e, o[e]);
     }
   };
+  // x is read and written once per iteration: streamed (evict-first), so
+  // that its lines do not push the matrix and R out of L2
+  auto xget = [&](int li0, double (&o)[kIrQ]) {
+    if (li0 + kIrQ <= nr) {
+      const double2 *q2 = reinterpret_cast<const double2 *>(x + r0 + li0);
+      const double2 u = __ldcs(q2), v = __ldcs(q2 + 1);
+      o[0] = u.x;
+      o[1] = u.y;
+      o[2] = v.x;
+      o[3] = v.y;
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++) o[e] = li0 + e < nr ? __ldcs(x + r0 + li0 + e) : 0.0;
+    }
+  };
+  auto xput = [&](int li0, const double (&o)[kIrQ]) {
+    if (li0 + kIrQ <= nr) {
+      double2 *q2 = reinterpret_cast<double2 *>(x + r0 + li0);
+      __stcs(q2, make_double2(o[0], o[1]));
+      __stcs(q2 + 1, make_double2(o[2], o[3]));
+    } else {
+#pragma unroll
+      for (int e = 0; e < kIrQ; e++)
+        if (li0 + e < nr) __stcs(x + r0 + li0 + e, o[e]);
+    }
+  };
   auto mv = [&](int li0, const double (&own4)[kIrQ], double (&y)[kIrQ]) {
     bool done = false;
     if constexpr (NDG == 5 || NDG == 7) {
@@ -1374,7 +1401,7 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cr_onchip(DiaT<double> D, IrA
     put(sr, li0, v);
     put(sp, li0, v);
     gput(R, li0, v);
-    gput(x, li0, z);
+    xput(li0, z);
   }
   double s1[1] = {acc};
   ok = ir_allreduce(a, ++gen, s1);
@@ -1456,15 +1483,10 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cr_onchip(DiaT<double> D, IrA
       if (li0 >= nr) continue;
       double pv[kIrQ], xv[kIrQ];
       own(sp, li0, pv);
-      if (li0 + kIrQ <= nr) {
-        ld4<double>(x + r0 + li0, xv, true);
-      } else {
-#pragma unroll
-        for (int e = 0; e < kIrQ; e++) xv[e] = li0 + e < nr ? __ldcg(x + r0 + li0 + e) : 0.0;
-      }
+      xget(li0, xv);
 #pragma unroll
       for (int e = 0; e < kIrQ; e++) xv[e] = add_rn(mul_rn(alpha, pv[e]), xv[e]);
-      gput(x, li0, xv);
+      xput(li0, xv);
     }
     if (!(ok = ir_red_wait<1>(a, gen, s1))) break;
     {
