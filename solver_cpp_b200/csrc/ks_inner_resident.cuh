@@ -1032,8 +1032,9 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_cg_onchip(DiaT<MT> D, IrArgs 
 // BiCG (bicg.cpp:148-260) as one cooperative launch of one CTA per SM, for
 // FP64 systems above the thread-block-cluster limit whose six vectors fit in
 // shared memory with one quad of rows per thread (rpc <= kIrTile: up to
-// about 606K rows), A and A^T both stencils with a diagonal copy
-// (ir_stencil_ok): x, r, r*, p, p* and q = A p of the CTA's rows in shared
+// about 606K rows), A and A^T with a diagonal copy (the stencil quad path
+// where ir_stencil_ok holds for both, else the generic one): x, r, r*, p, p*
+// and q = A p of the CTA's rows in shared
 // memory; p and p* also published to P and P* (zero-padded), from which the
 // other CTAs gather the columns their rows reach. Per iteration, in the
 // engine's order:
@@ -1068,8 +1069,9 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_bicg_onchip(DiaT<double> DA, 
   // the CTAs owning the columns this CTA's rows read through A or A^T
   int bl = blockIdx.x, bh = blockIdx.x;
   if (nr > 0) {
+    const int nda = NDG > 0 ? NDG : DA.nd, ndt = NDG > 0 ? NDG : DT.nd;
     const int lo = max(r0 + min(DA.off[0], DT.off[0]), 0);
-    const int hi = min(r0 + nr - 1 + max(DA.off[NDG - 1], DT.off[NDG - 1]), a.n - 1);
+    const int hi = min(r0 + nr - 1 + max(DA.off[nda - 1], DT.off[ndt - 1]), a.n - 1);
     bl = min(bl, lo / a.rpc);
     bh = max(bh, hi / a.rpc);
   }
@@ -1095,10 +1097,14 @@ __global__ void __launch_bounds__(kIrThreads, 1) k_bicg_onchip(DiaT<double> DA, 
   };
   auto mv = [&](const DiaT<double> &D, const double *G, const double *sv, const double (&own)[kIrQ],
                 double (&y)[kIrQ]) {
-    if (full)
-      ir_quad_mv_st<double, double, NDG>(D, G, sv, r0, nr, li0, own, y);
-    else
-      ir_quad_mv<double, double, NDG>(D, G, sv, r0, nr, li0, NDG, y);
+    bool done = false;
+    if constexpr (NDG == 5 || NDG == 7) {
+      if (a.stencil && full) {
+        ir_quad_mv_st<double, double, NDG>(D, G, sv, r0, nr, li0, own, y);
+        done = true;
+      }
+    }
+    if (!done) ir_quad_mv<double, double, NDG>(D, G, sv, r0, nr, li0, NDG > 0 ? NDG : D.nd, y);
   };
 
   // start (x0 = 0): r = r* = p = p* = b, x = 0; (r, r) -> |b| and the

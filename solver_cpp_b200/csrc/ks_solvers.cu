@@ -1126,16 +1126,16 @@ inline bool run_bicg_resident(const Env<double> &E, const double *b, double *x, 
 // direction update is gone: three kernels per iteration instead of four.
 // BiCG above the thread-block-cluster limit with its six vectors in shared
 // memory (k_bicg_onchip, ks_inner_resident.cuh: one GPU, FP64, A and A^T
-// stencils with a diagonal copy, up to kIrTile rows per SM; ks_params.
+// with a diagonal copy, up to kIrTile rows per SM; ks_params.
 // cluster_solve 0): the whole solve as one cooperative launch. P and P*, the
-// published directions, take workspace slots 0-1 and 2-3, each between two
-// zero pads wider than the largest offset. Returns false, having launched
+// published directions, take workspace slots 0-1 and from 2 on, each between
+// two zero pads wider than the largest offset. Returns false, having launched
 // nothing, when the system does not qualify.
 inline bool run_bicg_onchip(const Env<double> &E, const double *b, double *x, double *ws, ks_status *s) {
   if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A || !E.AT) return false;
   const CsrDev &A = *E.A, &T = *E.AT;
   if (!A.dia_nd || !A.dia_val || A.dia_nd != T.dia_nd || !T.dia_val) return false;
-  if (!ir_stencil_ok(A, E.n) || !ir_stencil_ok(T, E.n)) return false;
+  if (A.dia_cmin != 0 || A.dia_cmax != E.n || T.dia_cmin != 0 || T.dia_cmax != E.n) return false;
   ks_ctx *ctx = E.ctx;
   const long long G = ctx->num_sms;
   const long long rpc = ((E.n + G - 1) / G + 31) / 32 * 32;
@@ -1147,28 +1147,37 @@ inline bool run_bicg_onchip(const Env<double> &E, const double *b, double *x, do
   }
   const size_t smem = sizeof(double) * kIbVecs * (size_t)rpc;
   if (smem + 2048 > (size_t)optin) return false;
-  const long long pad = std::max(ir_p_pad(A), ir_p_pad(T));
+  // the stencil quad path where both qualify (P and P* zero-padded), else
+  // the generic quad path (clamped columns)
+  const bool stencil = ir_stencil_ok(A, E.n) && ir_stencil_ok(T, E.n);
+  const long long pad = stencil ? std::max(ir_p_pad(A), ir_p_pad(T)) : 0;
   if (2 * E.ld < E.n + 2 * pad) return false;
   bool fits = false;
+  auto launch = [&](const IrArgs &a, bool pr) {
+    return A.dia_nd == 7 ? ib_launch_n<7>(ctx, A, T, a, smem, (int)G, pr, &fits)
+                         : A.dia_nd == 5 ? ib_launch_n<5>(ctx, A, T, a, smem, (int)G, pr, &fits)
+                                         : ib_launch_n<0>(ctx, A, T, a, smem, (int)G, pr, &fits);
+  };
   const IrArgs probe{};
-  const cudaError_t pe = A.dia_nd == 7 ? ib_launch_n<7>(ctx, A, T, probe, smem, (int)G, true, &fits)
-                                       : ib_launch_n<5>(ctx, A, T, probe, smem, (int)G, true, &fits);
-  if (pe != cudaSuccess || !fits) {
+  if (launch(probe, true) != cudaSuccess || !fits) {
     (void)cudaGetLastError();
     return false;
   }
-  double *const P = ws + pad, *const Ps = ws + 2 * E.ld + pad;
+  // P in slots 0-1, P* from the next 4-element boundary (32-byte vector
+  // loads of both), within BiCG's six or more slots
+  const long long ps0 = (2 * E.ld + 3) / 4 * 4;
+  if (ps0 + E.n + 2 * pad > 6 * E.ld) return false;
+  double *const P = ws + pad, *const Ps = ws + ps0 + pad;
   if (reinterpret_cast<uintptr_t>(P) % 32 || reinterpret_cast<uintptr_t>(Ps) % 32) return false;
   launch_scalar(ctx, InitOp{E.st, E.sp.eps, E.sp.maxloop, E.record ? 1 : 0}, Stop{nullptr, E.outer_done});
   IrArgs a{b, x, P, E.st, nullptr, ctx->partials, (IrSync *)ctx->ir_sync, ctx->d_err, ctx->wait_ns,
-           (int)E.n, (int)rpc, 1, 1, 1};
+           (int)E.n, (int)rpc, 1, 1, stencil ? 1 : 0};
   a.P2 = Ps;
   cudaError_t e = cudaMemsetAsync(ctx->ir_sync, 0, ir_sync_bytes((int)G), ctx->stream);
-  for (double *z : {ws, P + E.n, ws + 2 * E.ld, Ps + E.n})
-    if (e == cudaSuccess) e = cudaMemsetAsync(z, 0, sizeof(double) * pad, ctx->stream);
-  if (e == cudaSuccess)
-    e = A.dia_nd == 7 ? ib_launch_n<7>(ctx, A, T, a, smem, (int)G, false, &fits)
-                      : ib_launch_n<5>(ctx, A, T, a, smem, (int)G, false, &fits);
+  if (stencil)
+    for (double *z : {ws, P + E.n, ws + ps0, Ps + E.n})
+      if (e == cudaSuccess) e = cudaMemsetAsync(z, 0, sizeof(double) * pad, ctx->stream);
+  if (e == cudaSuccess) e = launch(a, false);
   *s = e == cudaSuccess ? KS_OK : cuda_fail(ctx, e, "on-chip BiCG launch");
   return true;
 }

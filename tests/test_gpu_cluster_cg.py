@@ -216,7 +216,8 @@ def test_onchip_cg_within_reference_envelope(ks, ctx, oracle, prob, g):
     assert np.linalg.norm(chip.x - step.x) <= 1e-8 * np.linalg.norm(step.x)
 
 
-@pytest.mark.parametrize("prob,g", [("convdiff2d", 200), ("convdiff3d", 40), ("convdiff2d", 256), ("varcoef2d", 256)])
+@pytest.mark.parametrize("prob,g", [("convdiff2d", 200), ("convdiff3d", 40), ("convdiff2d", 256), ("varcoef2d", 256),
+                                    ("convdiff2d", 182), ("convdiff3d", 37)])
 def test_onchip_bicg_against_oracle_and_engine(ks, ctx, oracle, prob, g):
     """BiCG above one cluster's reach, its six vectors in shared memory across
     the GPU: one cooperative launch (cluster_solve 0; the profile counts the
@@ -229,7 +230,8 @@ def test_onchip_bicg_against_oracle_and_engine(ks, ctx, oracle, prob, g):
     (+-2 %). Then the oracle's verdict, a true residual within 3x the
     oracle's, the engine's solution to 1e-7 and the first history entries to
     1e-9. varcoef2d is symmetric (symmetric diagonal storage for A and its
-    transpose)."""
+    transpose); 182^2 and 37^3 have offsets that are not multiples of 4 (the
+    generic quad path)."""
     A, b, _ = config_problem(prob, g)
     M = ctx.matrix(A, transpose=True)
     chip = ks.solve(ctx, M, "BICG", b, E=1e-12, L=20000, cluster_solve=0, profile=1)
