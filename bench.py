@@ -339,9 +339,9 @@ def run_ours(args, world, rank, local):
         minfo["offsets"] = [int(o) for o in np.unique(A.col.astype(np.int64) - rows)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # larger than the 126 MB L2
 
-    def time_launches(fn, reps=50, cold=False):
+    def time_launches(fn, reps=50, cold=False, clean=True):
         """CUDA-event time of one launch on the solve's stream: back to back, or
-        each launch after a write of a buffer larger than L2 (cold)."""
+        each launch after an L2 flush (cold; `l2_flush`)."""
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
@@ -357,7 +357,7 @@ def run_ours(args, world, rank, local):
         tot = 0.0
         for _ in range(reps):
             with torch.cuda.stream(stream):
-                flush.fill_(1)
+                l2_flush(flush, clean)
                 e0.record(stream)
                 fn()
                 e1.record(stream)
@@ -375,10 +375,13 @@ def run_ours(args, world, rank, local):
         vcode = {"fp64": ks.FP64, "fp32": ks.FP32, "bf16": ks.BF16}[vals]
         fn = lambda: ks.spmv(M, xs, ys, values=vcode)  # noqa: E731
         warm, cold = time_launches(fn), time_launches(fn, reps=20, cold=True)
+        dirty = time_launches(fn, reps=20, cold=True, clean=False)
         alg = spmv_bytes(nl, nnzl, vals, ib, nd, sym)
         spmv[vals] = {"alg_bytes": alg, "launch_ms": round(warm, 5), "launch_ms_cold": round(cold, 5),
                       "gbs": round(alg / (warm / 1e3) / 1e9, 1), "frac": round(alg / (warm / 1e3) / 1e9 / peak, 4),
-                      "frac_cold": round(alg / (cold / 1e3) / 1e9 / peak, 4)}
+                      "frac_cold": round(alg / (cold / 1e3) / 1e9 / peak, 4),
+                      "launch_ms_cold_dirty": round(dirty, 5),
+                      "frac_cold_dirty": round(alg / (dirty / 1e3) / 1e9 / peak, 4)}
         xs.close()
         ys.close()
 
@@ -428,7 +431,9 @@ def run_ours(args, world, rank, local):
         roofline = {"bound": "hbm", "achieved": w["gbs"], "peak": peak, "unit": "GB/s", "frac": w["frac"],
                     "frac_cold": w["frac_cold"], "traffic": traffic, "kernel": f"spmv_{vals}",
                     "alg_bytes_per_launch": w["alg_bytes"], "launch_ms": w["launch_ms"],
-                    "timed": "alone, back to back (frac) and after an L2 flush (frac_cold)", "peak_kind": peak_kind}
+                    "timed": "alone, back to back (frac) and after an L2 flush that leaves only clean lines "
+                             "(frac_cold; frac_cold_dirty in spmv: after a write-only flush, whose dirty lines "
+                             "the launch writes back)", "peak_kind": peak_kind}
     roofline["layout"] = layout_key(minfo) + ("s" if sym else "")
     roofline["spmv"] = spmv
     roofline["in_solve_seconds"] = {k: round(prof[k], 6) for k in ("t_mv", "t_dot", "t_other", "t_memset",
@@ -627,9 +632,23 @@ def run_reference(args, world, rank):
     print(json.dumps(out))
 
 
+def l2_flush(buf, clean=True):
+    """Evicts the L2: writes `buf` (larger than the 126 MB L2) and, with
+    `clean`, reads it back, so that the L2 then holds clean lines of `buf`
+    only. Without the read ~126 MB of dirty lines stay behind, and the next
+    kernel pays for writing them back to DRAM (about 19 us at HBM speed)."""
+    import torch
+
+    buf.fill_(1)
+    if clean:
+        torch.sum(buf.view(torch.int64))
+
+
 def spmv_only(args):
     """The dominant kernel alone: y = A x with the chosen value precision on
-    the workload's matrix, timed with CUDA events over `steps` launches."""
+    the workload's matrix, timed with CUDA events over `steps` launches back
+    to back and over `steps` launches each after an L2 flush (`l2_flush`,
+    with and without the clean-up read)."""
     import torch
 
     import solver_cpp_b200 as ks
@@ -659,13 +678,35 @@ def spmv_only(args):
         e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
+    # cold: each launch after a write of a buffer larger than the 126 MB L2
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
+
+    def cold_ms(clean):
+        tot = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                l2_flush(flush, clean)
+                e0.record(stream)
+                ks.spmv(M, X, Y, values=vcode)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / args.steps
+
+    ms_cold, ms_dirty = cold_ms(True), cold_ms(False)
     alg = spmv_bytes(A.n, A.nnz, args.spmv_only, ib, nd, sym)
     peak, kind = load_peaks()
     gbs = alg / (ms / 1e3) / 1e9
+    gbs_cold = alg / (ms_cold / 1e3) / 1e9
     print(json.dumps({"kernel": f"spmv_{args.spmv_only}", "workload": args.workload, "n": A.n, "nnz": A.nnz,
                       "layout": layout_key(info), "index_bytes": ib, "diagonals": nd, "alg_bytes": alg,
                       "ms": round(ms, 5), "gbs": round(gbs, 1), "peak": peak,
-                      "frac": round(gbs / peak, 4), "peak_kind": kind}))
+                      "frac": round(gbs / peak, 4), "ms_cold": round(ms_cold, 5), "gbs_cold": round(gbs_cold, 1),
+                      "frac_cold": round(gbs_cold / peak, 4), "ms_cold_dirty": round(ms_dirty, 5),
+                      "frac_cold_dirty": round(alg / (ms_dirty / 1e3) / 1e9 / peak, 4), "peak_kind": kind,
+                      "timed": "back to back (ms, frac; the matrix stays partly in L2), each launch after "
+                               "an L2 flush that leaves clean lines (ms_cold, frac_cold) and after a "
+                               "write-only flush whose dirty lines the launch writes back (ms_cold_dirty)"}))
     M.close()
     ctx.close()
 
@@ -738,8 +779,10 @@ def ortho_only(args):
     length: h = V^T w over k basis vectors (block dot) and w -= V h (block
     AXPY), through ks_block_dot / ks_block_axpy, timed with CUDA events.
     Bytes: the block dot reads k + 1 vectors, the block AXPY reads k + 1 and
-    writes 1. Each call also moves the k coefficients between host and
-    device (block dot: device -> host, block AXPY: host -> device)."""
+    writes 1. Timed twice: with h in device memory (the kernels back to
+    back, as the solvers run them: `block_dot`, `block_axpy`) and with h a
+    host array (each call also moves the k coefficients between host and
+    device and waits for them: `*_host_h`)."""
     import torch
 
     import solver_cpp_b200 as ks
@@ -764,8 +807,17 @@ def ortho_only(args):
         torch.cuda.synchronize()
         out = {"kernel": "gmres_orthogonalisation", "workload": args.workload, "n": n, "k": k, "peak": peak,
                "peak_kind": kind}
-        for name, fn, nbytes in (("block_dot", lambda: ks.block_dot(V, n, k, w), (k + 1) * 8 * n),
-                                 ("block_axpy", lambda: ks.block_axpy(V, n, k, h * 0.0, w), (k + 2) * 8 * n)):
+        hz = h * 0.0
+        hd = torch.zeros(k, dtype=torch.float64, device="cuda:0")
+        hp = hd.data_ptr()
+        torch.cuda.synchronize()
+        for name, fn, nbytes in (("block_dot", lambda: ks.block_dot(V, n, k, w, out_device_ptr=hp), (k + 1) * 8 * n),
+                                 ("block_axpy", lambda: ks.block_axpy(V, n, k, hp, w), (k + 2) * 8 * n),
+                                 ("block_dot_host_h", lambda: ks.block_dot(V, n, k, w), (k + 1) * 8 * n),
+                                 ("block_axpy_host_h", lambda: ks.block_axpy(V, n, k, hz, w), (k + 2) * 8 * n)):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(args.steps):

@@ -96,10 +96,12 @@ inline long long ir_p_pad(const CsrDev &A) {
 
 // Whether a matrix takes the stencil path of the on-chip SpMV: 5 or 7
 // diagonals at offsets 0, -1, +1 and further pairs -o, +o with o a multiple
-// of 4, over the system's own columns (one GPU).
+// of 4, stored diagonals of a multiple of 4 elements (the vector loads of
+// their values aligned), over the system's own columns (one GPU).
 inline bool ir_stencil_ok(const CsrDev &A, long long n) {
   const int nd = A.dia_nd;
   if ((nd != 5 && nd != 7) || A.dia_cmin != 0 || A.dia_cmax != n) return false;
+  if (A.dia_ds % 4 != 0) return false;  // every stored diagonal starts on a 4-element boundary
   const int h = nd / 2;
   if (A.dia_off[h] != 0 || A.dia_off[h - 1] != -1 || A.dia_off[h + 1] != 1) return false;
   for (int k = 0; k < h - 1; k++)

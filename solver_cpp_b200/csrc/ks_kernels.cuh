@@ -353,7 +353,25 @@ inline DiaT<MT> dview(const CsrDev &A) {
   d.cmin = A.dia_cmin;
   d.cmax = A.dia_cmax;
   for (int k = 0; k < kMaxDiag; k++) d.off[k] = A.dia_off[k];
+  d.quad = 0;
   return d;
+}
+
+// Whether a plain SpMV (x read directly, y stored) may take the DIA kernel's
+// quad path: 5 or 7 diagonals at offsets 0, -1, +1 and pairs -o, +o with o a
+// multiple of 4, stored diagonals of a multiple of 4 elements (their vector
+// loads aligned), over the whole x (one GPU), x and y aligned for 4-element
+// vector accesses.
+template <class XT, class YT>
+inline bool dia_quad_ok(const CsrDev &A, const XT *x, const YT *y) {
+  const int nd = A.dia_nd;
+  if ((nd != 5 && nd != 7) || A.dia_cmin != 0 || A.dia_cmax != A.n) return false;
+  if (A.dia_ds % 4 != 0) return false;  // every stored diagonal starts on a 4-element boundary
+  const int h = nd / 2;
+  if (A.dia_off[h] != 0 || A.dia_off[h - 1] != -1 || A.dia_off[h + 1] != 1) return false;
+  for (int k = 0; k < h - 1; k++)
+    if (A.dia_off[k] % 4 != 0 || A.dia_off[k] != -A.dia_off[nd - 1 - k]) return false;
+  return reinterpret_cast<uintptr_t>(x) % (4 * sizeof(XT)) == 0 && reinterpret_cast<uintptr_t>(y) % (4 * sizeof(YT)) == 0;
 }
 
 template <int NV, int NDG, class MT, class GX, class Epi>
@@ -380,8 +398,12 @@ inline void launch_spmv_dn(ks_ctx *ctx, const CsrDev &A, const GX &g0, const GX 
   const long long wave = (long long)ctx->num_sms * spmv_dia_ctas_per_sm<NV, NDG, MT, GX, Epi>(ctx->device);
   const int grid = (int)std::max<long long>(1, std::min(need, wave));
   ctx->next_class = std::is_same<MT, double>::value ? kMv : kMvLow;
-  launch_k(ctx, spmv_dia_kernel<NV, NDG, MT, GX, Epi>, dim3(grid), dim3(kThreads), 0, dview<MT>(A), g0, g1, epi,
-           stop, red_of(ctx, slot));
+  DiaT<MT> dv = dview<MT>(A);
+  if constexpr (NV == 1 && Epi::ND == 0 && (NDG == 5 || NDG == 7) && GX::kPlain && has_row4<Epi>::value &&
+                !std::is_same<MT, double>::value)
+    dv.quad = dia_quad_ok(A, g0.x, epi.y) ? 1 : 0;
+  launch_k(ctx, spmv_dia_kernel<NV, NDG, MT, GX, Epi>, dim3(grid), dim3(kThreads), 0, dv, g0, g1, epi, stop,
+           red_of(ctx, slot));
 }
 
 // SpMV over the diagonal copy: one thread per row, one resident wave of CTAs;

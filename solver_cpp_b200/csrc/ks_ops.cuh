@@ -86,6 +86,15 @@ struct StoreEpi {
   YT *y;
   static constexpr int ND = 0;
   __device__ void row(int r, AT v, double (&)[1]) const { y[r] = (YT)v; }
+  // 4 consecutive rows from r (a multiple of 4; y aligned: dia_quad_ok)
+  __device__ void row4(int r, const AT (&v)[4]) const {
+    if constexpr (sizeof(YT) == 4) {
+      *reinterpret_cast<float4 *>(y + r) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+    } else {
+      reinterpret_cast<double2 *>(y + r)[0] = make_double2((double)v[0], (double)v[1]);
+      reinterpret_cast<double2 *>(y + r)[1] = make_double2((double)v[2], (double)v[3]);
+    }
+  }
   __device__ void finish(const double (&)[1]) const {}
 };
 

@@ -51,6 +51,18 @@ static ks_status fetch(ks_ctx *ctx, int count, double *host) {
 
 static bool same_ctx(const ks_vec *a, const ks_vec *b) { return a && b && a->ctx == b->ctx; }
 
+// True when p is device memory of the context's GPU (cudaMalloc, a torch
+// tensor): the tall-skinny block calls then keep their k values there,
+// ordered on the context's stream, with no copy and no synchronisation.
+static bool on_ctx_device(const ks_ctx *ctx, const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    (void)cudaGetLastError();  // plain host memory on older drivers
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice && a.device == ctx->device;
+}
+
 }  // namespace ks
 
 using namespace ks;
@@ -149,10 +161,11 @@ ks_status ks_block_dot(const ks_vec *V, int64_t ld, int k, const ks_vec *w, doub
   if (k == 0) return KS_OK;
   if (ld < n || (long long)(k - 1) * ld + n > V->n || (size_t)k > ctx->d_result_len)
     return set_error(ctx, KS_BAD_INPUT, "block_dot: basis does not fit");
+  const bool dev = on_ctx_device(ctx, h);
   KS_TRY(launch_block_dot<1, double>(ctx, (const double *)V->d, ld, k, (const double *)w->d, nullptr, n,
-                                     PutArray{ctx->d_result, 0, 1}, Stop{nullptr, nullptr}));
+                                     PutArray{dev ? h : ctx->d_result, 0, 1}, Stop{nullptr, nullptr}));
   KS_CUDA(ctx, cudaGetLastError());
-  return fetch(ctx, k, h);
+  return dev ? KS_OK : fetch(ctx, k, h);
 }
 
 ks_status ks_block_axpy(const ks_vec *V, int64_t ld, int k, const double *h, ks_vec *w) {
@@ -163,11 +176,15 @@ ks_status ks_block_axpy(const ks_vec *V, int64_t ld, int k, const double *h, ks_
   if (k == 0) return KS_OK;
   if (ld < n || (long long)(k - 1) * ld + n > V->n || (size_t)k > ctx->d_result_len)
     return set_error(ctx, KS_BAD_INPUT, "block_axpy: basis does not fit");
-  KS_CUDA(ctx, cudaMemcpyAsync(ctx->d_result, h, sizeof(double) * k, cudaMemcpyHostToDevice, ctx->stream));
-  launch_basis(ctx, n, k, BlockAxpyOp<double>{(const double *)V->d, ld, k, ctx->d_result, 1, (double *)w->d, nullptr},
-             Stop{nullptr, nullptr});
+  const bool dev = on_ctx_device(ctx, h);
+  if (!dev)
+    KS_CUDA(ctx, cudaMemcpyAsync(ctx->d_result, h, sizeof(double) * k, cudaMemcpyHostToDevice, ctx->stream));
+  launch_basis(ctx, n, k,
+               BlockAxpyOp<double>{(const double *)V->d, ld, k, dev ? h : ctx->d_result, 1, (double *)w->d,
+                                   nullptr},
+               Stop{nullptr, nullptr});
   KS_CUDA(ctx, cudaGetLastError());
-  KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // h is a host array
+  if (!dev) KS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // the host array may be reused on return
   return KS_OK;
 }
 

@@ -711,6 +711,7 @@ inline void run_iterations(const Env<VT> &E, bool fixed, F &&body) {
 // read equals the one the update would have stored, bit for bit.
 template <class VT>
 struct GDir {
+  static constexpr bool kPlain = false;
   const VT *__restrict__ pold;
   const VT *__restrict__ r;
   const double *beta;

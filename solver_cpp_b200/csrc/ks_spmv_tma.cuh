@@ -157,6 +157,7 @@ __device__ __forceinline__ bool is_long(int4 info) {
 // get<AT>(column)).
 template <class XT>
 struct GPtr {
+  static constexpr bool kPlain = true;  // x read directly (the DIA kernel's quad path)
   const XT *__restrict__ x;
   __device__ __forceinline__ GPtr prep() const { return *this; }
   template <class AT>

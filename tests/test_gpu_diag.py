@@ -17,8 +17,10 @@ from solver_cpp_b200.matrices import CSR, config_problem
 
 pytestmark = pytest.mark.gpu
 
+# offsets that are multiples of 4 take the SpMV's quad path (4 rows per
+# thread); 37^2 (odd n, offsets +-37) the row path
 STENCILS = [("poisson2d", 40, 5), ("poisson3d", 12, 7), ("convdiff3d", 12, 7), ("varcoef3d", 12, 7),
-            ("varcoef2d", 40, 5), ("convdiff2d", 40, 5)]
+            ("varcoef2d", 40, 5), ("convdiff2d", 40, 5), ("convdiff2d", 37, 5), ("varcoef3d", 20, 7)]
 
 
 def _csr(M):
