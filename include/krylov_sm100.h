@@ -185,7 +185,9 @@ ks_status ks_axpy_dot(double a, const ks_vec *x, ks_vec *y, const ks_vec *w,
                       double *result);
 /* h[i] = (V_i, w) for i < k, V_i = V[i*ld .. i*ld+n). GMRES's H column
  * (gmres.cpp:354-371) and GCR's beta dots (blas.cpp:532-535) as one
- * tall-skinny pass. */
+ * tall-skinny pass. h may be host memory (the call returns with the k
+ * results in it) or device memory of the context's GPU (the results are
+ * written there in stream order and the call returns without waiting). */
 ks_status ks_block_dot(const ks_vec *V, int64_t ld, int k, const ks_vec *w,
                        double *h);
 /* Allocation-free form of ks_block_dot, for callers that cannot allocate
@@ -208,7 +210,9 @@ ks_status ks_block_dot(const ks_vec *V, int64_t ld, int k, const ks_vec *w,
 ks_status ks_block_dot_noalloc(const double *V, int64_t ld, int k, const double *w, int64_t n, double *h,
                                void *stream);
 /* w[j] -= h[i] * V_i[j] for i = 0..k-1 in order (blas::Gmres_sp_1,
- * blas.cpp:477-488). */
+ * blas.cpp:477-488). h in host memory is copied in and the call waits for
+ * the update; h in device memory of the context's GPU is read in stream
+ * order and the call returns without waiting. */
 ks_status ks_block_axpy(const ks_vec *V, int64_t ld, int k, const double *h,
                         ks_vec *w);
 /* Matrix powers Ar[i] = A^{i+1} r (i <= 2k), Ap[i] = A^{i+1} p (i <= 2k+1),

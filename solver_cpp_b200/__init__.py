@@ -235,13 +235,25 @@ def axpy_dot(a: float, x: Vector, y: Vector, w: Vector | None = None) -> float:
     return r.value
 
 
-def block_dot(V: Vector, ld: int, k: int, w: Vector) -> np.ndarray:
+def block_dot(V: Vector, ld: int, k: int, w: Vector, out_device_ptr: int = 0):
+    """h = V^T w over k basis vectors. With out_device_ptr (device memory of
+    the context's GPU, k doubles) the results go there in stream order and
+    nothing is returned; else they come back as a numpy array."""
+    if out_device_ptr:
+        _check(lib().ks_block_dot(V.handle, ld, k, w.handle, C.c_void_p(out_device_ptr)), V.ctx.handle,
+               "block_dot")
+        return None
     h = np.zeros(max(k, 1))
     _check(lib().ks_block_dot(V.handle, ld, k, w.handle, _ptr(h)), V.ctx.handle, "block_dot")
     return h[:k]
 
 
 def block_axpy(V: Vector, ld: int, k: int, h, w: Vector):
+    """w -= V h. h: k coefficients as a host array, or an int device pointer
+    (device memory of the context's GPU, read in stream order)."""
+    if isinstance(h, int):
+        _check(lib().ks_block_axpy(V.handle, ld, k, C.c_void_p(h), w.handle), V.ctx.handle, "block_axpy")
+        return
     h = np.ascontiguousarray(h, dtype=np.float64)
     _check(lib().ks_block_axpy(V.handle, ld, k, _ptr(h), w.handle), V.ctx.handle, "block_axpy")
 

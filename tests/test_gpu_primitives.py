@@ -195,6 +195,24 @@ def test_block_dot_and_axpy_match_gmres_sp(ks, ctx):
     assert np.array_equal(WW.numpy(), ref)
 
 
+def test_block_dot_and_axpy_with_device_coefficients(ks, ctx):
+    """h in device memory: the block dot writes its k results there and the
+    block AXPY reads them there, in stream order; the bits equal the
+    host-array calls'."""
+    n, k = 300_007, 21
+    rng = np.random.default_rng(8)
+    V = rng.standard_normal((k, n))
+    w = rng.standard_normal(n)
+    VV, W1, W2 = ctx.vector(V.ravel()), ctx.vector(w), ctx.vector(w)
+    H = ctx.vector(n=k)
+    h = ks.block_dot(VV, n, k, W1)
+    assert ks.block_dot(VV, n, k, W2, out_device_ptr=H.device_ptr) is None
+    assert np.array_equal(H.numpy(), h)
+    ks.block_axpy(VV, n, k, h, W1)
+    ks.block_axpy(VV, n, k, H.device_ptr, W2)
+    assert np.array_equal(W1.numpy(), W2.numpy())
+
+
 @pytest.mark.parametrize("k", [0, 1, 2, 4])
 def test_matpow_and_gram(ks, ctx, oracle, k):
     A, _, _ = config_problem("convdiff3d", 12)
