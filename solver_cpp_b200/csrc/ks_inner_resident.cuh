@@ -119,6 +119,16 @@ __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned l
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// A reduction with release semantics at GPU scope: the thread's earlier
+// writes, and those of the CTA ordered before it by __syncthreads, are
+// visible to any thread whose acquire load reads this add's result or that
+// of a later add to the same counter. (Cheaper than a sequentially
+// consistent __threadfence followed by a relaxed atomic: C5 BiCG 28.46 ->
+// 28.10 ms, C5 CG 76.3 -> 75.2 ms.)
+__device__ __forceinline__ void red_release_add_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
 // Sums of N values over the CTA's 1024 threads in a fixed order; the result
 // is valid in thread 0.
 template <int N>
@@ -170,8 +180,7 @@ __device__ __forceinline__ void ir_red_post(const IrArgs &a, unsigned long long 
     double *part = a.partials + (size_t)(gen & 1) * kIrMaxSums * G;
 #pragma unroll
     for (int d = 0; d < N; d++) part[(size_t)d * G + blockIdx.x] = v[d];
-    __threadfence();
-    atomicAdd(&a.sync->count, 1ull);
+    red_release_add_u64(&a.sync->count, 1ull);
   }
 }
 
@@ -232,9 +241,8 @@ __device__ __forceinline__ bool ir_allreduce(const IrArgs &a, unsigned long long
 // Returns false when a wait ran out (the timeout flag is then set).
 __device__ __forceinline__ bool ir_publish_sync(const IrArgs &a, unsigned long long gen, int bl, int bh) {
   __shared__ int s_ok;
-  __syncthreads();  // every thread's stores of p are issued
+  __syncthreads();  // every thread's stores of p are ordered before thread 0's release
   if (threadIdx.x == 0) {
-    __threadfence();
     st_release_u64(ir_pub(a.sync, blockIdx.x), gen);
     s_ok = 1;
     const unsigned long long t0 = global_ns();
