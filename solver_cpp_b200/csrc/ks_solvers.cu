@@ -2009,8 +2009,9 @@ struct CgInStartOp {
 };
 
 // Inner end: z = (double) x (ConvertOp of the kernel-per-step loop's x; x
-// is 0 if the inner method stopped before its first update). mode 1 / 2 also
-// fuse VPCG's RzOp (init / beta) over the outer r and z on the outer state.
+// is 0 if the inner method stopped before its first update), not stored
+// when z is null. mode 1 / 2 also fuse VPCG's RzOp (init / beta) over the
+// outer r and z on the outer state.
 template <class VT>
 struct CgInFinalOp {
   const VT *x;
@@ -2027,13 +2028,37 @@ struct CgInFinalOp {
   __device__ Regs load(long long i) const { return {x[i], mode ? r[i] : 0.0}; }
   __device__ void store(long long i, const Regs &g, double (&acc)[1]) const {
     const double zi = __ldg(&ist->k.aux[A_XZERO]) ? 0.0 : (double)g.x;
-    z[i] = zi;
+    if (z) z[i] = zi;
     acc[0] = add_rn(acc[0], mul_rn(g.r, zi));
   }
   __device__ void finish(const double (&s)[1]) const {
     if (mode == 2) ost->k.s[S_BETA] = rdiv(ost, s[0], ost->k.s[S_RR]);
     if (mode) ost->k.s[S_RR] = s[0];
   }
+};
+
+// VPCG's direction update p = beta p + z (XpbyOp) with z read as the fast
+// inner CG's solution in its own precision, widened in the register (0 while
+// the inner solve left it at zero, as CgInFinalOp): the same bits as XpbyOp
+// over the FP64 copy of z, which is then neither written nor read (160^3:
+// 32.8 MB less written and 16.4 MB less read per outer iteration).
+template <class IT>
+struct XpbyInOp {
+  double *p;
+  const IT *x;
+  const DevState *ist;
+  const double *beta;
+  static constexpr int ND = 0;
+  struct Regs {
+    double p;
+    IT x;
+  };
+  __device__ Regs load(long long i) const { return {p[i], x[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&)[1]) const {
+    const double zi = __ldg(&ist->k.aux[A_XZERO]) ? 0.0 : (double)g.x;
+    p[i] = add_rn(mul_rn(rd(beta), g.p), zi);
+  }
+  __device__ void finish(const double (&)[1]) const {}
 };
 
 // VPCG's outer x/r update (XrUpdOp mode 1) fused with the start of the next
@@ -2234,9 +2259,9 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
         I.calls++;
         vec(E, VpXrStartOp<float>{x, r, p, mvv, E.st, I.fb.r, F.st, F.sp.eps, F.sp.maxloop});
         if (I.status == KS_OK) I.status = run_cg_inner_resident(F, I.fb, I.sh);
-        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, F.st, z, r, E.st, 2},
+        launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, F.st, nullptr, r, E.st, 2},
                    Stop{nullptr, F.outer_done});
-        vec(E, XpbyOp<VT>{p, z, &E.st->k.s[S_BETA]});
+        vec(E, XpbyInOp<float>{p, I.fb.x, F.st, &E.st->k.s[S_BETA]});
         return;
       }
     }
