@@ -175,3 +175,40 @@ def test_split_adjoint_gradient(ks, ctx, split3, prob, solver):
     gv = np.concatenate([r[2] for r in res])
     assert np.linalg.norm(gb - gb_ref) <= 1e-8 * np.linalg.norm(gb_ref)
     assert np.linalg.norm(gv - gv_ref) <= 1e-8 * np.linalg.norm(gv_ref)
+
+
+NCCL_CASES = [("poisson3d", "CG", "NONE", {}), ("convdiff3d", "BICG", "NONE", {}),
+              ("convdiff3d", "GMRES", "NONE", {"R": 30}),
+              ("varcoef3d", "VPCG", "CG", {"l": 20, "e": 1e-30, "inner_precision": "fp32"})]
+
+
+@pytest.mark.parametrize("prob,outer,inner,kw", NCCL_CASES)
+def test_nccl_transport_one_rank(ks, ctx, prob, outer, inner, kw):
+    """The NCCL transport (libnccl.so.2 opened at run time, the dots summed
+    by in-place all-reduces queued on the context's stream) as a
+    communicator of one rank on this GPU, where nothing waits on a peer. It
+    runs the split engine that `bench.py --gpus N` runs: the solve must equal
+    the same split solve over the in-process transport bit for bit, and the
+    unsplit solve to rounding."""
+    A, b, _ = config_problem(prob, 20)
+    tr = outer in ("BICG", "KSKIPBICG")
+    lowp = "inner_precision" in kw
+    p = dict(E=1e-10, **kw)
+    ref = ks.solve(ctx, ctx.matrix(A, transpose=tr, fp32=lowp), outer, b, inner=inner, **p)
+    res = []
+    for kind in ("nccl", "local"):
+        c = ks.Context(0)
+        comm = ks.Comm.nccl(c, 1, 0, ks.Comm.unique_id()) if kind == "nccl" else ks.Comm.local([c])[0]
+        try:
+            M = ks.SplitMatrix(c, comm, A, 0, A.n, transpose=tr, fp32=lowp)
+            res.append(ks.solve(c, M, outer, b, inner=inner, **p))
+            M.close()
+        finally:
+            comm.close()
+            c.close()
+    nc, lo = res
+    assert nc.status == lo.status == ref.status == 0
+    assert nc.loop == lo.loop and np.array_equal(nc.hist_err, lo.hist_err) and np.array_equal(nc.x, lo.x)
+    assert abs(nc.loop - ref.loop) <= max(2, 0.02 * ref.loop)
+    assert np.linalg.norm(nc.x - ref.x) <= 1e-8 * np.linalg.norm(ref.x)
+    assert nc.true_rel_res < 2e-10
