@@ -73,6 +73,48 @@ def test_crs_roundtrip_through_library_and_reference_format(ks, tmp_path):
     assert head == [str(A.n), str(A.n), str(A.nnz)]
 
 
+@pytest.mark.parametrize("threads", ["1", "3", "7", "64"])
+def test_crs_parallel_parse_any_whitespace(ks, tmp_path, monkeypatch, threads):
+    """The reader parses chunks of the text in parallel (KS_IO_THREADS forces
+    the chunk count on a small file). Records may be separated by any
+    whitespace, as fscanf reads them: several records on one line, blank
+    lines, tabs, CRLF. Every chunk count gives the written values bit for
+    bit; a file one record short, or with a token that does not parse, is an
+    I/O error."""
+    from solver_cpp_b200.matrices import config_problem
+
+    monkeypatch.setenv("KS_IO_THREADS", threads)
+    A, b, _ = config_problem("varcoef3d", 7)
+    x = np.random.default_rng(1).standard_normal(A.n)
+    d = str(tmp_path / "m")
+    ks.crs_write(d, A, b, x)
+    seps = [" ", "\n", "\t", "\r\n", "\n\n", "  \t "]
+    rng = np.random.default_rng(2)
+
+    def rewrite(name):
+        path = os.path.join(d, name)
+        lines = open(path).read().split("\n")
+        toks = " ".join(lines[1:]).split()
+        out = [lines[0]]
+        body = "".join(t + seps[rng.integers(len(seps))] for t in toks)
+        open(path, "w").write(out[0] + "\n" + body)
+
+    for name in ("ColVal.txt", "Ptr.txt", "bx.txt"):
+        rewrite(name)
+    A2, b2, x2 = ks.crs_read(d)
+    assert np.array_equal(A2.ptr, A.ptr) and np.array_equal(A2.col, A.col)
+    assert np.array_equal(A2.val, A.val) and np.array_equal(b2, b) and np.array_equal(x2, x)
+    # one record short / a token that does not parse
+    path = os.path.join(d, "ColVal.txt")
+    txt = open(path).read()
+    open(path, "w").write(txt.rsplit(None, 2)[0])
+    with pytest.raises(Exception):
+        ks.crs_read(d)
+    open(path, "w").write(txt.replace(txt.split()[10], "x1", 1))
+    with pytest.raises(Exception):
+        ks.crs_read(d)
+
+
 def test_crs_header_mismatch_is_io_error(ks, tmp_path):
     from solver_cpp_b200.matrices import poisson2d
 
