@@ -1049,6 +1049,112 @@ struct BicgMvTEpi {  // r* = -alpha (A^T p*) + r*; rr2 = (r*, r) -> beta
   }
 };
 
+// q = A p with (p*, q) -> alpha (CgMvEpi), and t = A^T p* stored for the
+// A^T epilogue that runs after the r update (spmv_dia_pair_kernel).
+template <class VT>
+struct BicgPairEpi {
+  using acc_t = VT;
+  CgMvEpi<VT> e;
+  VT *t;
+  static constexpr int ND = 1;
+  __device__ void row(int i, VT q, VT tv, double (&acc)[1]) const {
+    t[i] = tv;
+    e.row(i, q, acc);
+  }
+  __device__ void finish(const double (&s)[1]) const { e.finish(s); }
+};
+
+// BiCG after the pair SpMV, in one pass: x += alpha p (unless deferred),
+// r -= alpha q and r* -= alpha t (t = A^T p*), (r,r) for the stopping test and
+// (r*,r) for beta (bicg.cpp:242-262) with the engine's decisions in order: the
+// test (RUpdOp / XrUpdOp mode 1), then beta (BicgMvTEpi) if it did not stop
+// the method. The per-element operations are those two kernels'; (r*,r) adds
+// its terms in this pass's order instead of the A^T SpMV's.
+template <class VT, bool kDefer>
+struct BicgUpd2Op {
+  VT *x;
+  const VT *p;
+  VT *r;
+  const VT *q;
+  VT *rs;
+  const VT *t;
+  DevState *st;
+  double *aslot;  // the ring's alpha slot (deferred x)
+  static constexpr int ND = 2;
+  struct Regs {
+    VT x, p, q, r, t, rs;
+  };
+  __device__ Regs load(long long i) const {
+    if constexpr (kDefer)
+      return {(VT)0, (VT)0, q[i], r[i], t[i], rs[i]};
+    else
+      return {x[i], p[i], q[i], r[i], t[i], rs[i]};
+  }
+  __device__ void store(long long i, const Regs &g, double (&acc)[2]) const {
+    const VT a = (VT)rd(&st->k.s[S_ALPHA]);
+    if constexpr (!kDefer) x[i] = add_rn(mul_rn(a, g.p), g.x);
+    const VT ri = add_rn(mul_rn((VT)(-a), g.q), g.r);
+    r[i] = ri;
+    acc[0] = add_rn(acc[0], mul_rn(widen(ri), widen(ri)));
+    const VT si = add_rn(mul_rn((VT)(-a), g.t), g.rs);
+    rs[i] = si;
+    acc[1] = add_rn(acc[1], mul_rn(widen(si), widen(ri)));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    if constexpr (kDefer) {
+      *aslot = st->k.s[S_ALPHA];
+      st->k.aux[A_PENDING]++;
+    }
+    check_top(st, st->k.loop + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
+    if (st->k.done == kRunning) {
+      st->k.s[S_BETA] = rdiv(st, s[1], st->k.s[S_RR]);
+      st->k.s[S_RR] = s[1];
+    }
+  }
+};
+
+// Whether BiCG's two SpMVs can run as one pass over A's diagonal copy: one
+// GPU, 5 or 7 diagonals in the full layout (nd arrays of n values), and A^T's
+// copy the mirror of A's (its diagonal k at minus A's offset nd-1-k).
+inline bool dia_pair_ok(const CsrDev &A, const CsrDev &T, long long n) {
+  const int nd = A.dia_nd;
+  if ((nd != 5 && nd != 7) || T.dia_nd != nd || A.dia_sym || T.dia_sym || !A.dia_val || !A.dia_mask ||
+      !T.dia_mask)
+    return false;
+  if (A.n != n || T.n != n || A.dia_ds != n || A.dia_cmin != 0 || A.dia_cmax != n || T.dia_cmin != 0 ||
+      T.dia_cmax != n)
+    return false;
+  for (int k = 0; k < nd; k++)
+    if (T.dia_off[k] != -A.dia_off[nd - 1 - k]) return false;
+  return true;
+}
+
+// A^T's diagonals as a view of A's copy: diagonal k (offset o) is A's
+// diagonal nd-1-k (offset -o) read o rows further on; masks are A^T's.
+inline DiaT<double> dview_mirror(const CsrDev &A, const CsrDev &T) {
+  DiaT<double> d = dview<double>(T);
+  const int nd = A.dia_nd;
+  for (int k = 0; k < nd; k++) {
+    d.vb[k] = A.dia_val + (long long)(nd - 1 - k) * A.dia_ds;
+    d.vs[k] = T.dia_off[k];
+  }
+  return d;
+}
+
+// The pair SpMV on the grid of the A SpMV it replaces, so that (p*, q) adds
+// its terms in the same order.
+template <int NDG>
+inline void launch_bicg_pair_n(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, const double *p, const double *ps,
+                               const BicgPairEpi<double> &epi, Stop stop) {
+  const long long need = ((long long)A.n + kThreads - 1) / kThreads;
+  const long long wave =
+      (long long)ctx->num_sms * spmv_dia_ctas_per_sm<1, NDG, double, GPtr<double>, CgMvEpi<double>>(ctx->device);
+  ctx->next_class = kMv;
+  launch_k(ctx, spmv_dia_pair_kernel<NDG, GPtr<double>, BicgPairEpi<double>>,
+           dim3((unsigned)std::max<long long>(1, std::min(need, wave))), dim3(kThreads), 0, dview<double>(A),
+           dview_mirror(A, T), GPtr<double>{p}, GPtr<double>{ps}, epi, stop, red_of(ctx, 0));
+}
+
 // p_next = beta p + r (pn: the next ring slot, or p itself); ps = beta ps + rs.
 template <class VT>
 struct Xpby2PlainOp {
@@ -1196,6 +1302,16 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   const bool fused = E.A->dia_nd > 0 && !E.comm && E.n <= kGraphMaxN && (!defer || dir_ring(E.sp) >= 2);
   const int D = defer ? dir_ring(E.sp) : (fused ? 2 : 1);  // as in run_cg
   DirRing<VT> R{W.take(D), E.ld, D, dws};
+  // q = A p and t = A^T p* in one pass over A's diagonal copy (FP64, one GPU),
+  // where the copy does not fit in L2 (within 60 %, the deferred-x rule):
+  // a copy that fits is read from L2 by the second SpMV, and the separate
+  // SpMVs are as fast (convdiff 104^3, 63 MB: 23.8 against 24.5 ms; 128^3,
+  // 117 MB: 46.8 against 43.9 ms)
+  VT *tv = W.take();
+  bool pair = false;
+  if constexpr (std::is_same<VT, double>::value)
+    pair = !fused && !E.comm && E.mvals == KS_FP64 && dia_pair_ok(*E.A, *E.AT, E.n) &&
+           (double)E.A->dia_nd * (double)E.n * sizeof(double) > 0.6 * (double)E.ctx->l2_bytes;
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   // (r*, r) = (r, r) at the start
@@ -1207,16 +1323,33 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
       const VT *pold = L == 1 ? r : R.slot(L + D - 1);
       mv_g(E, *E.A, GDir<VT>{pold, r, &E.st->k.s[S_BETA], (VT)0},
            BicgMvDirEpi<VT>{pold, r, p, ps, rs, mvv, E.st});
+    } else if (pair) {
+      if constexpr (std::is_same<VT, double>::value) {
+        const BicgPairEpi<double> pe{CgMvEpi<double>{ps, mvv, E.st}, tv};  // alpha = rr/(p*, Ap)
+        if (E.A->dia_nd == 7)
+          launch_bicg_pair_n<7>(E.ctx, *E.A, *E.AT, p, ps, pe, E.stop());
+        else
+          launch_bicg_pair_n<5>(E.ctx, *E.A, *E.AT, p, ps, pe, E.stop());
+      }
     } else {
       mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
     }
-    if (defer) {
-      vec(E, RUpdOp<VT>{r, mvv, E.st, 1, R.aslot(L)});
-      ring_step(E, R, x, L);
+    if (pair) {
+      if (defer) {
+        vec(E, BicgUpd2Op<VT, true>{nullptr, nullptr, r, mvv, rs, tv, E.st, R.aslot(L)});
+        ring_step(E, R, x, L);
+      } else {
+        vec(E, BicgUpd2Op<VT, false>{x, p, r, mvv, rs, tv, E.st, nullptr});
+      }
     } else {
-      vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
+      if (defer) {
+        vec(E, RUpdOp<VT>{r, mvv, E.st, 1, R.aslot(L)});
+        ring_step(E, R, x, L);
+      } else {
+        vec(E, XrUpdOp<VT>{x, r, p, mvv, E.st, 1});
+      }
+      mv(E, *E.AT, (const VT *)ps, BicgMvTEpi<VT>{rs, r, E.st});
     }
-    mv(E, *E.AT, (const VT *)ps, BicgMvTEpi<VT>{rs, r, E.st});
     if (!fused) vec(E, Xpby2PlainOp<VT>{p, r, R.slot(L + 1), ps, rs, &E.st->k.s[S_BETA]});
   });
   if (defer) ring_final(E, R, x);
@@ -1927,7 +2060,7 @@ inline long long vec_count(int method, const Params &sp, long long n, size_t ele
   switch (method) {
     case KS_CG: return 2 + dir_slots(method, sp, n, elem, l2);
     case KS_CR: return 3 + dir_slots(method, sp, n, elem, l2);
-    case KS_BICG: return 4 + dir_slots(method, sp, n, elem, l2);
+    case KS_BICG: return 5 + dir_slots(method, sp, n, elem, l2);  // + A^T p* of the pair SpMV
     case KS_GCR: case KS_VPGCR: return 3 + 2 * m;
     case KS_GMRES: return 3 + (m + 1);
     case KS_VPGMRES: return 3 + (m + 1) + m;

@@ -234,4 +234,56 @@ __global__ void __launch_bounds__(kThreads) spmv_dia_kernel(DiaT<MT> D, GX gx0, 
   }
 }
 
+// BiCG's two products q = A p and t = A^T p* in one pass (FP64, one GPU):
+// thread i sums row i of A against p and row i of A^T against p*, the
+// latter read from A's own diagonal copy through DT, a view in which A^T's
+// diagonal k (offset o) is A's diagonal -o shifted by o rows
+// (A^T[i][i+o] = A[i+o][i]); DT's row masks are A^T's. Both rows add their
+// terms in ascending offset order from +0, so q and t are the bits of the
+// two separate SpMVs. The shifted reads of A's diagonals meet the lines that
+// the CTAs working o rows away load for their own q (|o| is a grid plane at
+// most; plain loads, not evict-first ones, so that those lines stay), so A
+// streams from HBM about once for both products. In the full
+// layout (nd arrays of n values back to back) a shifted read of a lower
+// diagonal runs into the next array and one of an upper diagonal into the
+// previous one: every address stays inside the copy, and those terms are
+// masked out. epi.row(i, q, t, acc).
+template <int NDG, class GX, class Epi>
+__global__ void __launch_bounds__(kThreads)
+    spmv_dia_pair_kernel(DiaT<double> DA, DiaT<double> DT, GX gx0, GX gx1, Epi epi, Stop stop, Red red) {
+  constexpr int ND = Epi::ND > 0 ? Epi::ND : 1;
+  double acc[ND];
+#pragma unroll
+  for (int d = 0; d < ND; d++) acc[d] = 0.0;
+  const int stride = (int)(gridDim.x * blockDim.x);
+  pdl_wait();
+  if (stop()) return;
+  const GX g0 = gx0.prep(), g1 = gx1.prep();
+  for (int i = (int)(blockIdx.x * blockDim.x + threadIdx.x); i < DA.n; i += stride) {
+    const unsigned ma = (unsigned)__ldcs(DA.mask + i), mt = (unsigned)__ldcs(DT.mask + i);
+    double a[NDG], b[NDG], x0[NDG], x1[NDG];
+#pragma unroll
+    for (int d = 0; d < NDG; d++) {
+      a[d] = __ldg(DA.vb[d] + (i + DA.vs[d]));
+      b[d] = __ldg(DT.vb[d] + (i + DT.vs[d]));
+      x0[d] = g0.template get<double>(min(max(i + DA.off[d], DA.cmin), DA.cmax - 1));
+      x1[d] = g1.template get<double>(min(max(i + DT.off[d], DT.cmin), DT.cmax - 1));
+    }
+    double y0 = 0.0, y1 = 0.0;
+#pragma unroll
+    for (int d = 0; d < NDG; d++) {
+      const double t0 = add_rn(y0, mul_rn(a[d], x0[d]));
+      y0 = ((ma >> d) & 1u) ? t0 : y0;
+      const double t1 = add_rn(y1, mul_rn(b[d], x1[d]));
+      y1 = ((mt >> d) & 1u) ? t1 : y1;
+    }
+    epi.row(i, y0, y1, acc);
+  }
+  __syncthreads();
+  pdl_trigger();
+  if constexpr (Epi::ND > 0) {
+    if (grid_sum<ND>(acc, red.partials, red.counter) && threadIdx.x == 0) epi.finish(acc);
+  }
+}
+
 }  // namespace ks

@@ -209,3 +209,40 @@ def test_on_chip_inner_cg_several_quads_per_thread(ks, ctx, prec):
     assert c1.loop == step.loop
     assert np.array_equal(c1.hist_err, step.hist_err)
     assert np.array_equal(c1.x, step.x)
+
+
+@pytest.mark.parametrize("prob,g", [("convdiff3d", 120), ("convdiff3d", 128)])
+def test_bicg_pair_spmv_against_two_spmvs(ks, ctx, prob, g):
+    """Above 2^20 rows, with a diagonal copy larger than 60 % of L2 (120^3:
+    97 MB, 128^3: 117 MB), BiCG computes q = A p and A^T p* in one pass over A's
+    diagonal copy (A^T's diagonals read as A's, mirrored; q and A^T p* are
+    the bits of the separate SpMVs) and updates r and r* in one pass, whose
+    (r*, r) sum adds its terms in another order. A one-rank split solve over
+    the in-process transport still runs the two separate SpMVs: the same
+    verdict, iteration counts within 10 %, solutions within 1e-6 (the upwind
+    residual first grows several-fold, which magnifies the last-bit
+    differences of (r*, r) in the histories to ~1e-6)."""
+    A, b, _ = config_problem(prob, g)
+    assert A.n > 1 << 20
+    M = ctx.matrix(A, transpose=True)
+    assert M.info()["diagonals"] in (5, 7) and M.info()["dia_symmetric"] == 0
+    pair = ks.solve(ctx, M, "BICG", b, E=1e-10, L=6000)
+    c = ks.Context(0)
+    comm = ks.Comm.local([c])[0]
+    try:
+        S = ks.SplitMatrix(c, comm, A, 0, A.n, transpose=True)
+        two = ks.solve(c, S, "BICG", b, E=1e-10, L=6000)
+        S.close()
+    finally:
+        comm.close()
+        c.close()
+    assert pair.status == two.status == 0
+    # BiCG's iteration count moves with the order of the (r*, r) sums: 120^3
+    # takes 517 iterations this way and 490 with the A^T SpMV's order (128^3:
+    # 502 both, the reference's count)
+    assert abs(pair.loop - two.loop) <= max(2, 0.10 * two.loop)
+    assert np.array_equal(pair.hist_err[:2], two.hist_err[:2])  # before the first (r*, r) sum differs
+    assert np.linalg.norm(pair.x - two.x) <= 1e-6 * np.linalg.norm(two.x)
+    # BiCG's recurrence residual can drift from b - A x (upwind systems):
+    # within ten times the two-SpMV solve's own
+    assert pair.true_rel_res <= 10 * two.true_rel_res + 1e-12
