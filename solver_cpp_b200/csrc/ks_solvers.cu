@@ -1141,18 +1141,41 @@ inline DiaT<double> dview_mirror(const CsrDev &A, const CsrDev &T) {
   return d;
 }
 
-// The pair SpMV on the grid of the A SpMV it replaces, so that (p*, q) adds
-// its terms in the same order.
-template <int NDG>
-inline void launch_bicg_pair_n(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, const double *p, const double *ps,
-                               const BicgPairEpi<double> &epi, Stop stop) {
+// The pair SpMV on the grid of the A SpMV (epilogue EpiA) it replaces, so
+// that a sum in its epilogue adds its terms in the same order.
+template <int NDG, class EpiA, class Epi>
+inline void launch_pair_n(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, const double *p, const double *ps,
+                          const Epi &epi, Stop stop) {
   const long long need = ((long long)A.n + kThreads - 1) / kThreads;
-  const long long wave =
-      (long long)ctx->num_sms * spmv_dia_ctas_per_sm<1, NDG, double, GPtr<double>, CgMvEpi<double>>(ctx->device);
+  const long long wave = (long long)ctx->num_sms * spmv_dia_ctas_per_sm<1, NDG, double, GPtr<double>, EpiA>(ctx->device);
   ctx->next_class = kMv;
-  launch_k(ctx, spmv_dia_pair_kernel<NDG, GPtr<double>, BicgPairEpi<double>>,
+  launch_k(ctx, spmv_dia_pair_kernel<NDG, GPtr<double>, Epi>,
            dim3((unsigned)std::max<long long>(1, std::min(need, wave))), dim3(kThreads), 0, dview<double>(A),
            dview_mirror(A, T), GPtr<double>{p}, GPtr<double>{ps}, epi, stop, red_of(ctx, 0));
+}
+
+template <class EpiA, class Epi>
+inline void launch_pair(ks_ctx *ctx, const CsrDev &A, const CsrDev &T, const double *p, const double *ps,
+                        const Epi &epi, Stop stop) {
+  if (A.dia_nd == 7)
+    launch_pair_n<7, EpiA, Epi>(ctx, A, T, p, ps, epi, stop);
+  else
+    launch_pair_n<5, EpiA, Epi>(ctx, A, T, p, ps, epi, stop);
+}
+
+// Whether BiCG-type methods take the pair SpMV: one GPU, FP64, the mirrored
+// diagonal copies, and a copy that does not fit in L2 (within 60 %, the
+// deferred-x rule): a copy that fits is read from L2 by the second SpMV, and
+// the separate SpMVs are as fast (convdiff 104^3, 63 MB: 23.8 against
+// 24.5 ms for BiCG; 128^3, 117 MB: 47.1 against 43.9 ms).
+template <class VT>
+inline bool use_pair(const Env<VT> &E) {
+  if constexpr (!std::is_same<VT, double>::value) {
+    return false;
+  } else {
+    return !E.comm && E.mvals == KS_FP64 && E.AT && dia_pair_ok(*E.A, *E.AT, E.n) &&
+           (double)E.A->dia_nd * (double)E.n * sizeof(double) > 0.6 * (double)E.ctx->l2_bytes;
+  }
 }
 
 // p_next = beta p + r (pn: the next ring slot, or p itself); ps = beta ps + rs.
@@ -1302,16 +1325,9 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   const bool fused = E.A->dia_nd > 0 && !E.comm && E.n <= kGraphMaxN && (!defer || dir_ring(E.sp) >= 2);
   const int D = defer ? dir_ring(E.sp) : (fused ? 2 : 1);  // as in run_cg
   DirRing<VT> R{W.take(D), E.ld, D, dws};
-  // q = A p and t = A^T p* in one pass over A's diagonal copy (FP64, one GPU),
-  // where the copy does not fit in L2 (within 60 %, the deferred-x rule):
-  // a copy that fits is read from L2 by the second SpMV, and the separate
-  // SpMVs are as fast (convdiff 104^3, 63 MB: 23.8 against 24.5 ms; 128^3,
-  // 117 MB: 46.8 against 43.9 ms)
+  // q = A p and t = A^T p* in one pass over A's diagonal copy (use_pair)
   VT *tv = W.take();
-  bool pair = false;
-  if constexpr (std::is_same<VT, double>::value)
-    pair = !fused && !E.comm && E.mvals == KS_FP64 && dia_pair_ok(*E.A, *E.AT, E.n) &&
-           (double)E.A->dia_nd * (double)E.n * sizeof(double) > 0.6 * (double)E.ctx->l2_bytes;
+  const bool pair = !fused && use_pair(E);
   init_state(E, b);
   if (!defer) vec(E, ZeroOp<VT>{x});
   // (r*, r) = (r, r) at the start
@@ -1326,10 +1342,7 @@ ks_status run_bicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
     } else if (pair) {
       if constexpr (std::is_same<VT, double>::value) {
         const BicgPairEpi<double> pe{CgMvEpi<double>{ps, mvv, E.st}, tv};  // alpha = rr/(p*, Ap)
-        if (E.A->dia_nd == 7)
-          launch_bicg_pair_n<7>(E.ctx, *E.A, *E.AT, p, ps, pe, E.stop());
-        else
-          launch_bicg_pair_n<5>(E.ctx, *E.A, *E.AT, p, ps, pe, E.stop());
+        launch_pair<CgMvEpi<double>>(E.ctx, *E.A, *E.AT, p, ps, pe, E.stop());
       }
     } else {
       mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{ps, mvv, E.st});  // alpha = rr/(p*, Ap)
@@ -2019,6 +2032,22 @@ struct KsRsEpi {  // r* = -a (A^T p*) + r*
   __device__ void finish(const double (&)[1]) const {}
 };
 
+// Av = A p and r* = -a (A^T p*) + r* (KsRsEpi) in one pass (the pair SpMV;
+// no sums, so the same bits as the two SpMVs).
+template <class VT>
+struct KsPairEpi {
+  using acc_t = VT;
+  VT *Av;
+  VT *rs;
+  const double *a;
+  static constexpr int ND = 0;
+  __device__ void row(int i, VT q, VT t, double (&)[1]) const {
+    Av[i] = q;
+    rs[i] = add_rn(mul_rn((VT)(-rd(a)), t), rs[i]);
+  }
+  __device__ void finish(const double (&)[1]) const {}
+};
+
 template <class VT>
 ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws) {
   const long long n = E.n, ld = E.ld;
@@ -2028,6 +2057,7 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
   VT *r = W.take(), *p = W.take(), *rs = W.take(), *ps = W.take(), *Av = W.take();
   VT *Ar = W.take(2 * k + 1), *Ap = W.take(2 * k + 2);
   double *G = dws, *coef = dws + 8 * k + 6;
+  const bool pair = use_pair(E);  // A p and A^T p* in one pass
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, p, rs, ps, E.st, START_KSKIP});
@@ -2044,9 +2074,16 @@ ks_status run_kskipbicg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dw
                                    PutArray{G + 4 * k + 2, 2 * k + 2, 1}, E.stop()));
     launch_scalar(E.ctx, KsBicgRecOp{E.st, G, coef, k}, E.stop());
     for (int i = 0; i <= k; i++) {
-      mv(E, *E.A, (const VT *)p, StoreEpi<VT, VT>{Av});
-      vec(E, KsXrOp<VT>{x, r, p, Av, coef + i});
-      mv(E, *E.AT, (const VT *)ps, KsRsEpi<VT>{rs, coef + i});
+      if (pair) {
+        if constexpr (std::is_same<VT, double>::value)
+          launch_pair<StoreEpi<double, double>>(E.ctx, *E.A, *E.AT, p, ps, KsPairEpi<double>{Av, rs, coef + i},
+                                                E.stop());
+        vec(E, KsXrOp<VT>{x, r, p, Av, coef + i});
+      } else {
+        mv(E, *E.A, (const VT *)p, StoreEpi<VT, VT>{Av});
+        vec(E, KsXrOp<VT>{x, r, p, Av, coef + i});
+        mv(E, *E.AT, (const VT *)ps, KsRsEpi<VT>{rs, coef + i});
+      }
       vec(E, Xpby2PlainOp<VT>{p, r, p, ps, rs, coef + k + 1 + i});
     }
     if (E.outer && P.step()) break;

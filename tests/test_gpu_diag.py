@@ -246,3 +246,25 @@ def test_bicg_pair_spmv_against_two_spmvs(ks, ctx, prob, g):
     # BiCG's recurrence residual can drift from b - A x (upwind systems):
     # within ten times the two-SpMV solve's own
     assert pair.true_rel_res <= 10 * two.true_rel_res + 1e-12
+
+
+def test_kskip_bicg_pair_spmv_is_bitwise(ks, ctx):
+    """k-skip BiCG's inner steps take A p and r* -= a A^T p* from one pass
+    over A's diagonal copy above 2^20 rows with a copy larger than 60 % of
+    L2; the epilogue has no sums, so the solve equals the one-rank split
+    solve (two separate SpMVs) bit for bit."""
+    A, b, _ = config_problem("convdiff3d", 128)
+    M = ctx.matrix(A, transpose=True)
+    pair = ks.solve(ctx, M, "KSKIPBICG", b, E=1e-10, L=3000, K=2)
+    c = ks.Context(0)
+    comm = ks.Comm.local([c])[0]
+    try:
+        S = ks.SplitMatrix(c, comm, A, 0, A.n, transpose=True)
+        two = ks.solve(c, S, "KSKIPBICG", b, E=1e-10, L=3000, K=2)
+        S.close()
+    finally:
+        comm.close()
+        c.close()
+    assert pair.status == two.status == 0
+    assert pair.loop == two.loop
+    assert np.array_equal(pair.hist_err, two.hist_err) and np.array_equal(pair.x, two.x)
