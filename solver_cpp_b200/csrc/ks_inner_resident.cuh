@@ -1631,15 +1631,22 @@ struct IrShape {
 
 // False when the system does not fit: r and q of a thread's rows in its 64
 // TMEM words (K <= ir_max_k), p and x of a CTA's rows in shared memory.
+// `fill`: fewer CTAs than SMs where the system is small, so that every
+// thread has at least one quad of rows (fewer arrivals at each grid
+// reduction; FP64 CG whole solves, same box, three rounds: 64^3 4.38 -> 3.79
+// ms, 256^2 30.7 -> 28.8 ms, 512^2 74.8 -> 72.6 ms; CR, which streams x
+// through global memory, got slower: 3.21 -> 4.26 ms).
 template <class VT>
-inline bool ir_shape(const ks_ctx *ctx, long long n, IrShape *s) {
+inline bool ir_shape(const ks_ctx *ctx, long long n, IrShape *s, bool fill = false) {
   if (n < 1) return false;
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess) {
     (void)cudaGetLastError();
     return false;
   }
-  const long long G = ctx->num_sms;
+  const long long G = fill ? std::min<long long>(ctx->num_sms, std::max<long long>(1, (n + kIrQ * kIrThreads - 1) /
+                                                                                         (kIrQ * kIrThreads)))
+                           : ctx->num_sms;
   const long long rpc = ((n + G - 1) / G + 31) / 32 * 32;
   const long long K = (rpc + kIrThreads - 1) / kIrThreads;
   const size_t smem = sizeof(VT) * 2 * (size_t)rpc;

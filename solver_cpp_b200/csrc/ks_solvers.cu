@@ -809,7 +809,7 @@ inline bool run_cg_onchip(const Env<double> &E, const double *b, double *x, doub
   if (E.sp.cluster_solve || !E.outer || E.comm || E.mvals != KS_FP64 || !E.A->dia_nd || !E.A->dia_val) return false;
   ks_ctx *ctx = E.ctx;
   IrShape sh;
-  if (!ir_shape<double>(ctx, E.n, &sh)) return false;
+  if (!ir_shape<double>(ctx, E.n, &sh, true)) return false;
   bool fits = false;
   const IrArgs probe{};
   if (ir_launch<double, double>(ctx, *E.A, probe, sh, true, &fits, 0) != cudaSuccess || !fits) {
