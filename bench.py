@@ -718,7 +718,7 @@ KERNEL_TOUR = [
     ("c2_cg", "CG", "NONE", dict(E=1e-10, L=4)),                      # k_cg_onchip FP64 (the whole solve)
     ("c2_cg", "CG", "NONE", dict(E=1e-10, L=4, cluster_solve=1)),     # the engine: spmv_dia FP64, RUpdOp, XpbyToOp
     ("c2_cr", "CR", "NONE", dict(E=1e-10, L=4)),
-    ("c3_bicg", "BICG", "NONE", dict(E=1e-10, L=4)),                  # A^T SpMV
+    ("c3_bicg", "BICG", "NONE", dict(E=1e-10, L=4)),                  # A p and A^T p* in one pass
     ("c3_gmres30", "GMRES", "NONE", dict(E=1e-10, L=30, R=30)),       # block dot, basis kernel, Givens
     ("c3_gcr30", "GCR", "NONE", dict(E=1e-10, L=30, R=30)),           # block dot, GcrPQOp
     ("c3_kskipbicg2", "KSKIPBICG", "NONE", dict(E=1e-10, L=6, K=2)),  # two-vector matrix powers, Gram
