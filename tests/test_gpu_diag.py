@@ -211,12 +211,13 @@ def test_on_chip_inner_cg_several_quads_per_thread(ks, ctx, prec):
     assert np.array_equal(c1.x, step.x)
 
 
-@pytest.mark.parametrize("prob,g", [("convdiff3d", 120), ("convdiff3d", 128)])
-def test_bicg_pair_spmv_against_two_spmvs(ks, ctx, prob, g):
+@pytest.mark.parametrize("prob,g,xu", [("convdiff3d", 120, 0), ("convdiff3d", 128, 0), ("convdiff3d", 128, 1)])
+def test_bicg_pair_spmv_against_two_spmvs(ks, ctx, prob, g, xu):
     """Above 2^20 rows, with a diagonal copy larger than 60 % of L2 (120^3:
     97 MB, 128^3: 117 MB), BiCG computes q = A p and A^T p* in one pass over A's
     diagonal copy (A^T's diagonals read as A's, mirrored; q and A^T p* are
-    the bits of the separate SpMVs) and updates r and r* in one pass, whose
+    the bits of the separate SpMVs) and updates r and r* (and x, with
+    x_update 1; else x is deferred to the direction ring) in one pass, whose
     (r*, r) sum adds its terms in another order. A one-rank split solve over
     the in-process transport still runs the two separate SpMVs: the same
     verdict, iteration counts within 10 %, solutions within 1e-6 (the upwind
@@ -226,12 +227,12 @@ def test_bicg_pair_spmv_against_two_spmvs(ks, ctx, prob, g):
     assert A.n > 1 << 20
     M = ctx.matrix(A, transpose=True)
     assert M.info()["diagonals"] in (5, 7) and M.info()["dia_symmetric"] == 0
-    pair = ks.solve(ctx, M, "BICG", b, E=1e-10, L=6000)
+    pair = ks.solve(ctx, M, "BICG", b, E=1e-10, L=6000, x_update=xu)
     c = ks.Context(0)
     comm = ks.Comm.local([c])[0]
     try:
         S = ks.SplitMatrix(c, comm, A, 0, A.n, transpose=True)
-        two = ks.solve(c, S, "BICG", b, E=1e-10, L=6000)
+        two = ks.solve(c, S, "BICG", b, E=1e-10, L=6000, x_update=xu)
         S.close()
     finally:
         comm.close()
