@@ -36,7 +36,7 @@ typedef enum {
   KS_BAD_INPUT = 5,       /* invalid argument, shape or handle                  */
   KS_CUDA_ERROR = 6,      /* a CUDA runtime call failed                         */
   KS_TIMEOUT = 7,         /* a bounded device wait gave up                      */
-  KS_OUT_OF_MEMORY = 8,   /* device allocation failed                           */
+  KS_OUT_OF_MEMORY = 8,   /* device (CRS text I/O: host) allocation failed      */
   KS_NO_DEVICE = 9,       /* no usable CUDA device                              */
   KS_IO_ERROR = 10,       /* CRS text files missing or malformed                */
   KS_UNIMPLEMENTED = 99   /* reference's "Not implemented" (KSKIPCR, VPBICG)    */

@@ -8,6 +8,7 @@
 // exactly through the reference's fscanf("%le").
 #include <cerrno>
 #include <cinttypes>
+#include <new>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -73,6 +74,24 @@ int io_threads(size_t bytes) {
   return (int)std::max<size_t>(1, std::min<size_t>((size_t)std::min(hw, 64), bytes >> 22));
 }
 
+// Runs fn(k) for k = 0 .. T-1: chunk 0 here, the others on threads of their
+// own; a chunk whose thread cannot be started runs here too.
+template <class F>
+void run_chunks(int T, const F &fn) {
+  std::vector<std::thread> pool;
+  std::vector<int> here;
+  for (int k = 1; k < T; k++) {
+    try {
+      pool.emplace_back(fn, k);
+    } catch (...) {
+      here.push_back(k);
+    }
+  }
+  fn(0);
+  for (int k : here) fn(k);
+  for (auto &t : pool) t.join();
+}
+
 // The whitespace-separated tokens of [body, end) (end points at the buffer's
 // terminating NUL), the first `want` of them handed to put(t, p) in parallel:
 // put parses token t at p, advances p past it and returns false on a parse
@@ -97,14 +116,7 @@ bool parse_tokens(char *body, char *end, long long want, const Put &put) {
   }
   auto starts_token = [&](const char *q) { return !is_ws(*q) && (q == body || is_ws(q[-1])); };
   std::vector<long long> first(T + 1, 0);
-  std::vector<std::thread> pool;
-  auto run = [&](auto &&fn) {
-    pool.clear();
-    for (int k = 1; k < T; k++) pool.emplace_back(fn, k);
-    fn(0);
-    for (auto &t : pool) t.join();
-  };
-  run([&](int k) {
+  run_chunks(T, [&](int k) {
     long long c = 0;
     for (const char *q = cut[k]; q < cut[k + 1]; q++) c += starts_token(q) ? 1 : 0;
     first[k + 1] = c;
@@ -112,7 +124,7 @@ bool parse_tokens(char *body, char *end, long long want, const Put &put) {
   for (int k = 0; k < T; k++) first[k + 1] += first[k];
   if (first[T] < want) return false;
   std::atomic<bool> ok{true};
-  run([&](int k) {
+  run_chunks(T, [&](int k) {
     char *q = cut[k];
     for (long long t = first[k]; t < std::min(first[k + 1], want); t++) {
       while (is_ws(*q)) q++;
@@ -158,7 +170,6 @@ bool write_records(const std::string &path, const std::string &head, long long c
   if (!f) return false;
   const int T = io_threads((size_t)count * 24);
   std::vector<std::string> part(T);
-  std::vector<std::thread> pool;
   auto work = [&](int k) {
     const long long i0 = count * k / T, i1 = count * (k + 1) / T;
     std::string &o = part[k];
@@ -169,9 +180,7 @@ bool write_records(const std::string &path, const std::string &head, long long c
       if (m > 0) o.append(line, (size_t)m);
     }
   };
-  for (int k = 1; k < T; k++) pool.emplace_back(work, k);
-  work(0);
-  for (auto &t : pool) t.join();
+  run_chunks(T, work);
   bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
   for (int k = 0; k < T && ok; k++) ok = std::fwrite(part[k].data(), 1, part[k].size(), f) == part[k].size();
   return std::fclose(f) == 0 && ok;
@@ -196,8 +205,24 @@ ks_status ks_crs_read_header(const char *dir, int64_t *n, int64_t *nnz) {
   return KS_OK;
 }
 
+static ks_status crs_read(const char *dir, int64_t n, int64_t nnz, int32_t *ptr, int32_t *col, double *val,
+                          double *b, double *x);
+
+// Host memory for the text (and the writer's formatted ranges) can run out;
+// no exception leaves these entry points.
 ks_status ks_crs_read(const char *dir, int64_t n, int64_t nnz, int32_t *ptr, int32_t *col, double *val,
                       double *b, double *x) {
+  try {
+    return crs_read(dir, n, nnz, ptr, col, val, b, x);
+  } catch (const std::bad_alloc &) {
+    return KS_OUT_OF_MEMORY;
+  } catch (...) {
+    return KS_IO_ERROR;
+  }
+}
+
+static ks_status crs_read(const char *dir, int64_t n, int64_t nnz, int32_t *ptr, int32_t *col, double *val,
+                          double *b, double *x) {
   if (!dir || n < 1 || nnz < 0) return KS_BAD_INPUT;
   const std::string d(dir);
   std::vector<char> buf;
@@ -252,8 +277,22 @@ ks_status ks_crs_read(const char *dir, int64_t n, int64_t nnz, int32_t *ptr, int
   return KS_OK;
 }
 
+static ks_status crs_write(const char *dir, int64_t n, int64_t nnz, const int32_t *ptr, const int32_t *col,
+                           const double *val, const double *b, const double *x);
+
 ks_status ks_crs_write(const char *dir, int64_t n, int64_t nnz, const int32_t *ptr, const int32_t *col,
                        const double *val, const double *b, const double *x) {
+  try {
+    return crs_write(dir, n, nnz, ptr, col, val, b, x);
+  } catch (const std::bad_alloc &) {
+    return KS_OUT_OF_MEMORY;
+  } catch (...) {
+    return KS_IO_ERROR;
+  }
+}
+
+static ks_status crs_write(const char *dir, int64_t n, int64_t nnz, const int32_t *ptr, const int32_t *col,
+                           const double *val, const double *b, const double *x) {
   if (!dir || n < 1 || nnz < 0 || !ptr || (nnz > 0 && (!col || !val))) return KS_BAD_INPUT;
   const std::string d(dir);
   char head[96];
