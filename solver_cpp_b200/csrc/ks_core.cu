@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <new>
 
 #include "ks_dist.cuh"
 #include "ks_kernels.cuh"
@@ -600,6 +601,20 @@ __global__ void k_copy_bytes_done(const int *src, int *dst) { *dst = *src; }
 using namespace ks;
 
 // ============================================================= C ABI: context
+// Host containers (std::vector, new) can throw; no exception leaves a C
+// entry point: running out of host memory is KS_OUT_OF_MEMORY, any other
+// exception (a size no container can hold) KS_BAD_INPUT.
+template <class F>
+static ks_status no_throw(F &&f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc &) {
+    return KS_OUT_OF_MEMORY;
+  } catch (...) {
+    return KS_BAD_INPUT;
+  }
+}
+
 extern "C" {
 
 int ks_abi_version(void) { return KS_ABI_VERSION; }
@@ -640,7 +655,8 @@ ks_status ks_ctx_create(int device, ks_ctx **out) {
   int ndev = ks_device_count();
   if (ndev <= 0) return KS_NO_DEVICE;
   if (device < 0 || device >= ndev) return KS_BAD_INPUT;
-  ks_ctx *ctx = new ks_ctx();
+  ks_ctx *ctx = new (std::nothrow) ks_ctx();
+  if (!ctx) return KS_OUT_OF_MEMORY;
   ctx->device = device;
   auto fail = [&](ks_status s) {
     ks_ctx_destroy(ctx);
@@ -791,13 +807,14 @@ static ks_status upload_common(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_
 
 ks_status ks_csr_upload(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_t *ptr, const int32_t *col,
                         const double *val, unsigned flags, ks_mat **out) {
-  return upload_common(ctx, n, nnz, ptr, col, val, flags, out, cudaMemcpyHostToDevice);
+  return no_throw([&] { return upload_common(ctx, n, nnz, ptr, col, val, flags, out, cudaMemcpyHostToDevice); });
 }
 
 ks_status ks_csr_upload_device(ks_ctx *ctx, int64_t n, int64_t nnz, const int32_t *d_ptr,
                                const int32_t *d_col, const double *d_val, unsigned flags,
                                ks_mat **out) {
-  return upload_common(ctx, n, nnz, d_ptr, d_col, d_val, flags, out, cudaMemcpyDeviceToDevice);
+  return no_throw(
+      [&] { return upload_common(ctx, n, nnz, d_ptr, d_col, d_val, flags, out, cudaMemcpyDeviceToDevice); });
 }
 
 ks_status ks_mat_destroy(ks_mat *m) {
@@ -856,9 +873,19 @@ static ks_status plan_of(ks_ctx *ctx, const std::vector<long long> &all, int P, 
   return KS_OK;
 }
 
+static ks_status dist_upload(ks_ctx *ctx, ks_comm *comm, int64_t n_global, int64_t r0, int64_t r1,
+                             const int32_t *ptr, const int32_t *col, const double *val, const int32_t *tptr,
+                             const int32_t *tcol, const double *tval, unsigned flags, ks_mat **out);
+
 ks_status ks_dist_upload(ks_ctx *ctx, ks_comm *comm, int64_t n_global, int64_t r0, int64_t r1, const int32_t *ptr,
                          const int32_t *col, const double *val, const int32_t *tptr, const int32_t *tcol,
                          const double *tval, unsigned flags, ks_mat **out) {
+  return no_throw([&] { return dist_upload(ctx, comm, n_global, r0, r1, ptr, col, val, tptr, tcol, tval, flags, out); });
+}
+
+static ks_status dist_upload(ks_ctx *ctx, ks_comm *comm, int64_t n_global, int64_t r0, int64_t r1,
+                             const int32_t *ptr, const int32_t *col, const double *val, const int32_t *tptr,
+                             const int32_t *tcol, const double *tval, unsigned flags, ks_mat **out) {
   if (!ctx || !comm || !out || !ptr || comm->ctx != ctx) return KS_BAD_INPUT;
   *out = nullptr;
   const bool want_t = (flags & KS_MAT_TRANSPOSE) != 0;
@@ -962,7 +989,8 @@ ks_status ks_vec_create(ks_ctx *ctx, int64_t n, ks_precision type, ks_vec **out)
   if (!ctx || !out || n < 1 || type < KS_FP64 || type > KS_BF16) return KS_BAD_INPUT;
   *out = nullptr;
   KS_CUDA(ctx, cudaSetDevice(ctx->device));
-  ks_vec *v = new ks_vec();
+  ks_vec *v = new (std::nothrow) ks_vec();
+  if (!v) return KS_OUT_OF_MEMORY;
   v->ctx = ctx;
   v->n = n;
   v->type = type;
@@ -986,7 +1014,8 @@ ks_status ks_vec_wrap(ks_ctx *ctx, int64_t n, ks_precision type, void *device_pt
   if (!ctx || !out || !device_ptr || n < 1 || type < KS_FP64 || type > KS_BF16) return KS_BAD_INPUT;
   if (((uintptr_t)device_ptr) % 16 != 0)
     return set_error(ctx, KS_BAD_INPUT, "wrapped device pointer must be 16-byte aligned");
-  ks_vec *v = new ks_vec();
+  ks_vec *v = new (std::nothrow) ks_vec();
+  if (!v) return KS_OUT_OF_MEMORY;
   v->ctx = ctx;
   v->n = n;
   v->type = type;

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -52,8 +53,8 @@ std::string lower(std::string s) {
 }
 
 // Parses the whole file into CSR arrays (ptr has n + 1 entries).
-ks_status parse_mm(const char *file, int64_t &n, std::vector<int32_t> &ptr, std::vector<int32_t> &col,
-                   std::vector<double> &val) {
+ks_status parse_mm_body(const char *file, int64_t &n, std::vector<int32_t> &ptr, std::vector<int32_t> &col,
+                        std::vector<double> &val) {
   if (!file) return KS_BAD_INPUT;
   std::vector<char> buf;
   if (!read_file(file, buf)) return KS_IO_ERROR;
@@ -138,6 +139,19 @@ ks_status parse_mm(const char *file, int64_t &n, std::vector<int32_t> &ptr, std:
   }
   for (int64_t r = 0; r < n; r++) ptr[(size_t)r + 1] += ptr[(size_t)r];
   return KS_OK;
+}
+
+// Running out of host memory for the entries is KS_OUT_OF_MEMORY; no
+// exception leaves the C entry points.
+ks_status parse_mm(const char *file, int64_t &n, std::vector<int32_t> &ptr, std::vector<int32_t> &col,
+                   std::vector<double> &val) {
+  try {
+    return parse_mm_body(file, n, ptr, col, val);
+  } catch (const std::bad_alloc &) {
+    return KS_OUT_OF_MEMORY;
+  } catch (...) {
+    return KS_BAD_INPUT;
+  }
 }
 
 }  // namespace
