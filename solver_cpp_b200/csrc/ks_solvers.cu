@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <new>
 
 #include "ks_ops.cuh"
 #include "ks_state.cuh"
@@ -2892,6 +2893,26 @@ static ks_status solve_impl(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_
   return st_code;
 }
 
+// Host containers (the workspace list, the buffer pool) can throw; no
+// exception leaves a C entry point.
+template <class F>
+static ks_status solve_no_throw(ks_ctx *ctx, F &&f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc &) {
+    return set_error(ctx, KS_OUT_OF_MEMORY, "host allocation failed");
+  } catch (...) {
+    return set_error(ctx, KS_BAD_INPUT, "host container size out of range");
+  }
+}
+
+static ks_status solve_entry(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                             const ks_params *params, const ks_vec *b, ks_vec *x, int64_t *hist_iter,
+                             double *hist_err, int64_t hist_cap, ks_report *report);
+static ks_status solve_host_entry(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                                  const ks_params *params, const double *b, double *x, int64_t *hist_iter,
+                                  double *hist_err, int64_t hist_cap, ks_report *report);
+
 extern "C" {
 
 void ks_params_default(ks_params *p) {
@@ -2916,6 +2937,25 @@ void ks_params_default(ks_params *p) {
 ks_status ks_solve(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
                    const ks_params *params, const ks_vec *b, ks_vec *x, int64_t *hist_iter,
                    double *hist_err, int64_t hist_cap, ks_report *report) {
+  if (!ctx) return KS_BAD_INPUT;
+  return solve_no_throw(
+      ctx, [&] { return solve_entry(ctx, mat, outer, inner, params, b, x, hist_iter, hist_err, hist_cap, report); });
+}
+
+ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                        const ks_params *params, const double *b, double *x, int64_t *hist_iter,
+                        double *hist_err, int64_t hist_cap, ks_report *report) {
+  if (!ctx) return KS_BAD_INPUT;
+  return solve_no_throw(ctx, [&] {
+    return solve_host_entry(ctx, mat, outer, inner, params, b, x, hist_iter, hist_err, hist_cap, report);
+  });
+}
+
+}  // extern "C"
+
+static ks_status solve_entry(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                             const ks_params *params, const ks_vec *b, ks_vec *x, int64_t *hist_iter,
+                             double *hist_err, int64_t hist_cap, ks_report *report) {
   if (!ctx || !mat || !b || !x || mat->ctx != ctx || b->ctx != ctx || x->ctx != ctx) return KS_BAD_INPUT;
   if (b->type != KS_FP64 || x->type != KS_FP64 || b->n != mat->A.n || x->n != mat->A.n)
     return set_error(ctx, KS_BAD_INPUT, "ks_solve: b and x must be FP64 vectors of length n");
@@ -2949,9 +2989,9 @@ ks_status ks_solve(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver in
   return s;
 }
 
-ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
-                        const ks_params *params, const double *b, double *x, int64_t *hist_iter,
-                        double *hist_err, int64_t hist_cap, ks_report *report) {
+static ks_status solve_host_entry(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solver inner,
+                                  const ks_params *params, const double *b, double *x, int64_t *hist_iter,
+                                  double *hist_err, int64_t hist_cap, ks_report *report) {
   if (!ctx || !mat || !b || !x || mat->ctx != ctx) return KS_BAD_INPUT;
   // b and x live in the context's buffer pool between calls: no device
   // allocation (and no synchronising free) per solve
@@ -2992,6 +3032,8 @@ ks_status ks_solve_host(ks_ctx *ctx, const ks_mat *mat, ks_solver outer, ks_solv
   pool_release(ctx, buf);
   return r;
 }
+
+extern "C" {
 
 ks_status ks_adjoint_grad(ks_ctx *ctx, const ks_mat *mat, ks_solver solver, ks_solver inner,
                           const ks_params *params, const ks_vec *x, const ks_vec *g, ks_vec *grad_b,
