@@ -18,6 +18,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <new>
 
 #include "ks_dist.cuh"
 
@@ -274,7 +275,8 @@ ks_status ks_comm_create_nccl(ks_ctx *ctx, int nranks, int rank, const void *id1
   KS_CUDA(ctx, cudaSetDevice(ctx->device));
   ncclUniqueId id;
   std::memcpy(&id, id128, sizeof(id));
-  auto *c = new NcclComm();
+  auto *c = new (std::nothrow) NcclComm();
+  if (!c) return KS_OUT_OF_MEMORY;
   c->ctx = ctx;
   c->nranks = nranks;
   c->rank = rank;
@@ -296,12 +298,25 @@ ks_status ks_comm_create_local(ks_ctx *const *ctxs, int nranks, ks_comm **comms)
     comms[q] = nullptr;
     if (!ctxs[q]) return KS_BAD_INPUT;
   }
-  auto g = std::make_shared<LocalGroup>();
+  // host allocations can throw; no exception leaves this entry point
+  std::shared_ptr<LocalGroup> g;
+  try {
+    g = std::make_shared<LocalGroup>();
+    g->ptr.assign(nranks, nullptr);
+    g->ev.assign(nranks, nullptr);
+  } catch (...) {
+    return KS_OUT_OF_MEMORY;
+  }
   g->P = nranks;
-  g->ptr.assign(nranks, nullptr);
-  g->ev.assign(nranks, nullptr);
   for (int q = 0; q < nranks; q++) {
-    auto *c = new LocalComm();
+    auto *c = new (std::nothrow) LocalComm();
+    if (!c) {
+      for (int p = 0; p < q; p++) {
+        delete comms[p];
+        comms[p] = nullptr;
+      }
+      return KS_OUT_OF_MEMORY;
+    }
     c->ctx = ctxs[q];
     c->nranks = nranks;
     c->rank = q;
