@@ -269,3 +269,29 @@ def test_kskip_bicg_pair_spmv_is_bitwise(ks, ctx):
     assert pair.status == two.status == 0
     assert pair.loop == two.loop
     assert np.array_equal(pair.hist_err, two.hist_err) and np.array_equal(pair.x, two.x)
+
+
+def test_bicg_pair_spmv_on_the_transposed_system(ks, ctx):
+    """A transposed solve (A^T x = b, as the adjoint solve runs it) takes the
+    pair path with the roles of the two copies swapped: it must converge to
+    the same solution as the two-SpMV path (one-rank split) and reach b - A^T x
+    to the tolerance, with iteration counts within 10 %."""
+    A, b, _ = config_problem("convdiff3d", 128)
+    M = ctx.matrix(A, transpose=True)
+    kw = dict(E=1e-10, L=6000, transpose=1)
+    pair = ks.solve(ctx, M, "BICG", b, **kw)
+    c = ks.Context(0)
+    comm = ks.Comm.local([c])[0]
+    try:
+        S = ks.SplitMatrix(c, comm, A, 0, A.n, transpose=True)
+        two = ks.solve(c, S, "BICG", b, **kw)
+        S.close()
+    finally:
+        comm.close()
+        c.close()
+    assert pair.status == two.status == 0
+    assert abs(pair.loop - two.loop) <= max(2, 0.10 * two.loop)
+    assert np.linalg.norm(pair.x - two.x) <= 1e-6 * np.linalg.norm(two.x)
+    AT = A.to_scipy().T.tocsr()
+    true = np.linalg.norm(b - AT @ pair.x) / np.linalg.norm(b)
+    assert true <= 10 * two.true_rel_res + 1e-12 and true < 1e-8
