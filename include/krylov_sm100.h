@@ -252,9 +252,10 @@ typedef struct {
                                 recurrences and GMRES assembly; 0: corrected */
   int32_t transpose;       /* 1: solve A^T x = b (adjoint solves)            */
   int32_t poll_interval;   /* iterations in flight between host polls; 0=auto */
-  int32_t x_update;        /* CG, CR, BiCG: 0 auto, 1 x += alpha p every
-                              iteration, 2 deferred through a ring of 32
-                              directions (same x bit for bit)              */
+  int32_t x_update;        /* CG, CR, BiCG, and VPCG with the on-chip
+                              FP32/BF16 inner CG: 0 auto, 1 x += alpha p
+                              every iteration, 2 deferred through a ring of
+                              32 directions (same x bit for bit)           */
   int32_t cluster_solve;   /* CG, CR, BiCG on at most 32768 rows (one GPU): 0
                               auto, the whole solve in one launch of one
                               thread-block cluster where the device can hold

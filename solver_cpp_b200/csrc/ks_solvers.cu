@@ -2104,7 +2104,7 @@ inline long long vec_count(int method, const Params &sp, long long n, size_t ele
     case KS_VPGMRES: return 3 + (m + 1) + m;
     case KS_KSKIPCG: return 3 + (2 * k + 1) + (2 * k + 2);
     case KS_KSKIPBICG: return 5 + (2 * k + 1) + (2 * k + 2);
-    case KS_VPCG: return 4;
+    case KS_VPCG: return 3 + (defer_x(KS_CG, sp, n, elem, l2) ? dir_ring(sp) : 1);  // r, z, A p, directions
     case KS_VPCR: return 5;
   }
   return 0;
@@ -2117,7 +2117,7 @@ inline long long dws_count(int method, const Params &sp) {
     case KS_GMRES: case KS_VPGMRES: return (m + 1) * m + 4 * m + 4;
     case KS_KSKIPCG: return 6 * k + 4 + 2 * (k + 1) + 4;
     case KS_KSKIPBICG: return 8 * k + 6 + 2 * (k + 1) + 4;
-    case KS_CG: case KS_CR: case KS_BICG: return kDirRing + 4;  // alpha ring
+    case KS_CG: case KS_CR: case KS_BICG: case KS_VPCG: return kDirRing + 4;  // alpha ring
   }
   return 4;
 }
@@ -2215,10 +2215,11 @@ struct CgInFinalOp {
 // 32.8 MB less written and 16.4 MB less read per outer iteration).
 template <class IT>
 struct XpbyInOp {
-  double *p;
+  const double *p;
   const IT *x;
   const DevState *ist;
   const double *beta;
+  double *out;  // p itself, or the next slot of the direction ring
   static constexpr int ND = 0;
   struct Regs {
     double p;
@@ -2227,7 +2228,7 @@ struct XpbyInOp {
   __device__ Regs load(long long i) const { return {p[i], x[i]}; }
   __device__ void store(long long i, const Regs &g, double (&)[1]) const {
     const double zi = __ldg(&ist->k.aux[A_XZERO]) ? 0.0 : (double)g.x;
-    p[i] = add_rn(mul_rn(rd(beta), g.p), zi);
+    out[i] = add_rn(mul_rn(rd(beta), g.p), zi);
   }
   __device__ void finish(const double (&)[1]) const {}
 };
@@ -2262,6 +2263,41 @@ struct VpXrStartOp {
     acc[1] = add_rn(acc[1], mul_rn(widen(r32), widen(r32)));
   }
   __device__ void finish(const double (&s)[2]) const {
+    check_top(st, st->k.loop + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
+    inner_cg_start(ist, ieps, imaxloop, s[1]);
+  }
+};
+
+// VpXrStartOp with x deferred to the direction ring (as RUpdOp for CG):
+// r -= alpha q, the same sums in the same order, alpha recorded beside the
+// ring slot and the iteration counted as pending for x.
+template <class IT>
+struct VpRStartOp {
+  double *r;
+  const double *q;
+  DevState *st;
+  IT *ri;
+  DevState *ist;
+  double ieps;
+  long long imaxloop;
+  double *aslot;
+  static constexpr int ND = 2;
+  struct Regs {
+    double q, r;
+  };
+  __device__ Regs load(long long i) const { return {q[i], r[i]}; }
+  __device__ void store(long long i, const Regs &g, double (&acc)[2]) const {
+    const double a = rd(&st->k.s[S_ALPHA]);
+    const double rn = add_rn(mul_rn(-a, g.q), g.r);
+    r[i] = rn;
+    acc[0] = add_rn(acc[0], mul_rn(rn, rn));
+    const IT r32 = (IT)rn;
+    ri[i] = r32;
+    acc[1] = add_rn(acc[1], mul_rn(widen(r32), widen(r32)));
+  }
+  __device__ void finish(const double (&s)[2]) const {
+    *aslot = st->k.s[S_ALPHA];
+    st->k.aux[A_PENDING]++;
     check_top(st, st->k.loop + 1, sqrt(s[0]) / st->k.s[S_BNORM]);
     inner_cg_start(ist, ieps, imaxloop, s[1]);
   }
@@ -2391,16 +2427,23 @@ struct RzOp {  // rr2 = (r, z); beta = rr2 / rr; rr = rr2   (vpcg.cpp:733-745)
 };
 
 template <class VT>
-ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT> *inner) {
+ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, double *dws, InnerRunner<VT> *inner) {
+  // vpcg.cpp:659-750. With the on-chip inner CG its start is fused into the
+  // outer x/r update and its end into (r, z); where the outer vectors do not
+  // fit in L2 (defer_x, CG's rule) x += alpha p is deferred to a ring of
+  // directions, as in run_cg: the x/r update then reads and writes neither x
+  // nor p, and x gets the same bits.
+  bool fast = false;
+  if constexpr (std::is_same<VT, double>::value) fast = inner->res_cg;
+  const bool defer = fast && defer_x(E, KS_CG);
   Ws<VT> W{ws, E.ld, E.off};
-  VT *r = W.take(), *p = W.take(), *z = W.take(), *mvv = W.take();
+  VT *r = W.take(), *z = W.take(), *mvv = W.take();
+  const int D = defer ? dir_ring(E.sp) : 1;
+  DirRing<VT> R{W.take(D), E.ld, D, dws};
+  long long Lr = 1;  // ring position of the current direction (1 after each start)
   init_state(E, b);
   vec(E, ZeroOp<VT>{x});
   start_from_zero(E, StartEpi<VT>{b, r, nullptr, nullptr, nullptr, E.st, START_CHECK});
-  // vpcg.cpp:659-750. With the on-chip inner CG its start is fused into the
-  // outer x/r update and its end into (r, z).
-  bool fast = false;
-  if constexpr (std::is_same<VT, double>::value) fast = inner->res_cg;
   // z = M r, rr = (r, z), p = z: the method's start, and its restart after a
   // failed true-residual check (r then holds b - A x)
   auto start = [&]() {
@@ -2413,26 +2456,36 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
         launch_vec(E.ctx, E.n, CgInStartOp<float>{r, I.fb.r, F.st, F.sp.eps, F.sp.maxloop}, os);
         if (I.status == KS_OK) I.status = run_cg_inner_resident(F, I.fb, I.sh);
         launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, F.st, z, r, E.st, 1}, os);
-        vec(E, CopyOp<VT>{z, p});
+        Lr = 1;
+        vec(E, CopyOp<VT>{z, R.slot(Lr)});
         return;
       }
     }
     inner->solve(r, z);
-    vec(E, CopyOp<VT>{z, p});
+    Lr = 1;
+    vec(E, CopyOp<VT>{z, R.slot(Lr)});
     vec(E, RzOp<VT>{r, z, E.st, 1});
   };
   auto iteration = [&]() {
+    VT *p = R.slot(Lr);
     mv(E, *E.A, (const VT *)p, CgMvEpi<VT>{p, mvv, E.st});
     if constexpr (std::is_same<VT, double>::value) {
       if (fast) {
         InnerRunner<double> &I = *inner;
         const Env<float> &F = I.E32;
         I.calls++;
-        vec(E, VpXrStartOp<float>{x, r, p, mvv, E.st, I.fb.r, F.st, F.sp.eps, F.sp.maxloop});
+        if (defer) {
+          vec(E, VpRStartOp<float>{r, mvv, E.st, I.fb.r, F.st, F.sp.eps, F.sp.maxloop, R.aslot(Lr)});
+          ring_step(E, R, x, Lr);  // before the next direction overwrites the first slot
+        } else {
+          vec(E, VpXrStartOp<float>{x, r, p, mvv, E.st, I.fb.r, F.st, F.sp.eps, F.sp.maxloop});
+        }
         if (I.status == KS_OK) I.status = run_cg_inner_resident(F, I.fb, I.sh);
         launch_vec(E.ctx, E.n, CgInFinalOp<float>{I.fb.x, F.st, nullptr, r, E.st, 2},
                    Stop{nullptr, F.outer_done});
-        vec(E, XpbyInOp<float>{p, I.fb.x, F.st, &E.st->k.s[S_BETA]});
+        VT *pn = defer ? R.slot(Lr + 1) : p;
+        vec(E, XpbyInOp<float>{p, I.fb.x, F.st, &E.st->k.s[S_BETA], pn});
+        Lr++;
         return;
       }
     }
@@ -2450,6 +2503,7 @@ ks_status run_vpcg(const Env<VT> &E, const VT *b, VT *x, VT *ws, InnerRunner<VT>
       issued++;
       if (P.step()) break;
     }
+    if (defer) ring_final(E, R, x);  // the check reads x
     if (!true_check_continue(E, b, x, r)) break;
     if (issued >= E.sp.maxloop) {
       true_check_exhausted(E);
@@ -2535,7 +2589,7 @@ ks_status run_method(int method, const Env<IT> &E, const IT *b, IT *x, IT *ws, d
   }
   if constexpr (std::is_same<IT, double>::value) {
     switch (method) {
-      case KS_VPCG: return run_vpcg(E, b, x, ws, inner);
+      case KS_VPCG: return run_vpcg(E, b, x, ws, dws, inner);
       case KS_VPCR: return run_vpcr(E, b, x, ws, inner);
       case KS_VPGCR: return run_gcr_core(E, b, x, ws, dws, inner);
       case KS_VPGMRES: return run_gmres_core(E, b, x, ws, dws, inner);

@@ -203,3 +203,19 @@ def test_autograd_binding_gradcheck(ks, ctx, prob, solver):
         return (sparse_solve(ctx, A, v, rhs, solver, E=1e-12, L=20000) * w).sum()
 
     assert torch.autograd.gradcheck(f, (vals, bt), eps=1e-6, atol=1e-5, rtol=1e-4, fast_mode=True)
+
+
+def test_vpcg_direction_ring_is_bitwise(ks, ctx):
+    """160^3 VPCG with the on-chip FP32 inner CG defers x += alpha p to a ring
+    of directions (its outer vectors do not fit in L2); x_update 1 keeps the
+    update in the x/r pass. x is the same bits either way, and so are the
+    history, the iteration count and the true residual."""
+    A, b, _ = config_problem("varcoef3d", 160)
+    M = ctx.matrix(A, fp32=True)
+    kw = dict(E=1e-10, L=20000, l=20, e=1e-30, inner_precision="fp32")
+    ring = ks.solve(ctx, M, "VPCG", b, inner="CG", **kw)
+    flat = ks.solve(ctx, M, "VPCG", b, inner="CG", x_update=1, **kw)
+    assert ring.status == flat.status == 0 and ring.loop == flat.loop
+    assert np.array_equal(ring.hist_err, flat.hist_err)
+    assert np.array_equal(ring.x, flat.x)
+    assert ring.true_rel_res == flat.true_rel_res < 1e-10
